@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: time-to-1e-8 relative residual of the matrix-free hex8 GMG-PCG
+solve, reported as MDOF/s (full-grid DOF / time-to-solution), on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (default): the seeded 256x128x128 noise bracket (Gaussian noise
+blurred sigma=4, 50th-percentile threshold, largest 26-connected component;
+aluminium E=69 GPa nu=0.33, z=0 face clamped, 5 kN in -z on a 16x16 top
+patch), 5-level GMG, e_min=1e-9 voids on the full grid -- 12,830,211 DOF.
+A step is one complete solve from the modulus field and load (coarse-operator
+set-up included) to a true FP64 relative residual below 1e-8.
+
+`value`  device-resident: inputs already in HBM, CUDA events on the solver's
+         stream around K steps, max over ranks.
+`e2e`    the public API (MGSolver.solve with host numpy arrays: modulus and
+         load copied in, displacement copied out every step).
+`impl reference` times the CPU oracle (a numpy restatement of the reference's
+         Jacobi-PCG, the reference path that converges on noise geometry) on a
+         bounded sample of the same generator, on the host cores.
+N > 1 runs independent replicas (one per GPU, no inter-GPU traffic): the
+solve does not shard in this build.
+"""
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "MDOF/s to 1e-8 relative residual (time-to-solution), matrix-free hex8 GMG-PCG"
+UNIT = "MDOF/s"
+TOL = 1e-8
+E_MIN = 1e-9
+
+WORKLOADS = {
+    "bracket_256x128x128": dict(shape=(256, 128, 128), seed=0, sigma=4.0, load=5000.0, patch=16,
+                                levels=5),
+    "bracket_128x64x64": dict(shape=(128, 64, 64), seed=0, sigma=4.0, load=5000.0, patch=16, levels=4),
+    "cantilever_64x16x16": dict(cantilever=True, levels=3),
+}
+CPU_SAMPLE = dict(shape=(64, 32, 32), seed=0, sigma=4.0, load=5000.0, patch=16)
+
+
+def make_problem(w):
+    from voxelsim_fea_b200 import generators
+    if w.get("cantilever"):
+        return generators.cantilever()
+    return generators.bracket(shape=w["shape"], seed=w["seed"], sigma=w["sigma"], load_n=w["load"],
+                              patch=w["patch"])
+
+
+def mg_modulus(p):
+    """VoxelFEA's MG convention: inactive voxels carry e_min * E (fea.py:467-469)."""
+    return np.where(p["active"], p["E_stiff"], p["E_stiff"] * E_MIN)
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- reference arm
+def cpu_sample_solve():
+    """One reference-algorithm solve on the bounded CPU sample; returns (seconds, dof, iters)."""
+    from oracle import fea as ofea
+    from voxelsim_fea_b200 import generators
+    p = generators.bracket(shape=CPU_SAMPLE["shape"], seed=CPU_SAMPLE["seed"], sigma=CPU_SAMPLE["sigma"],
+                           load_n=CPU_SAMPLE["load"], patch=CPU_SAMPLE["patch"])
+    nx, ny, nz = p["dims"]
+    v = ofea.VoxelFEAOracle(nx, ny, nz, nu=p["nu"], active_elems=p["active"], use_multigrid=False)
+    v.set_fixed(p["fixed_dofs"])
+    t0 = time.perf_counter()
+    v.solve(p["E_stiff"], p["f"], tol=TOL)
+    dt = time.perf_counter() - t0
+    return dt, 3 * (nx + 1) * (ny + 1) * (nz + 1), v.last_iters
+
+
+def cpu_cores():
+    try:
+        import threadpoolctl
+        info = threadpoolctl.threadpool_info()
+        if info:
+            return int(max(d.get("num_threads", 1) for d in info))
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def cpu_baseline_record():
+    dt, dof, it = cpu_sample_solve()
+    return {"value": dof / dt / 1e6, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
+            "sample": (f"numpy restatement of the reference's Jacobi-PCG (core/fea.py:497-593) to {TOL:g} "
+                       f"on the seeded bracket generator at {CPU_SAMPLE['shape'][0]}x{CPU_SAMPLE['shape'][1]}x"
+                       f"{CPU_SAMPLE['shape'][2]} ({dof} DOF, {it} iterations, {dt:.1f} s); the reference's "
+                       f"MG path does not converge on this geometry"),
+            "seconds": dt, "iterations": it}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    for _ in range(args.warmup):
+        cpu_sample_solve()
+    times = []
+    dof = it = 0
+    for _ in range(args.steps):
+        dt, dof, it = cpu_sample_solve()
+        times.append(dt)
+    ms = 1e3 * float(np.mean(times))
+    value = dof / (ms / 1e3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": args.workload, "sample": "bracket_64x32x32", "tol": TOL,
+                   "method": "Jacobi-PCG (reference fallback path)", "parallelism": "host cores"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
+                         "sample": f"bracket generator 64x32x32 ({dof} DOF, {it} iterations) per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- B200 arm
+def run_b200(args):
+    import torch
+    from voxelsim_fea_b200 import _lib
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    w = WORKLOADS[args.workload]
+    p = make_problem(w)
+    nx, ny, nz = p["dims"]
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    nelem = nx * ny * nz
+    E_mg = mg_modulus(p)
+    L = _lib.load()
+    DEV = _lib.VF_SOLVE_DEVICE_PTRS
+
+    def solver(opts):
+        return MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=w["levels"], options=opts)
+
+    fast = solver(SolverOptions.fast(device=local, check_every=args.check_every))
+    E_d = torch.from_numpy(np.ascontiguousarray(E_mg)).cuda()
+    f_d = torch.from_numpy(np.ascontiguousarray(p["f"], dtype=np.float64)).cuda()
+    u_d = torch.empty(ndof, dtype=torch.float64, device="cuda")
+    info = _lib.VfSolveInfo()
+
+    def step(sv):
+        _lib.check(L.vf_set_material(sv._h, ctypes.c_void_p(E_d.data_ptr()), None, DEV), sv._h)
+        rc = L.vf_solve(sv._h, ctypes.c_void_p(f_d.data_ptr()), None, TOL, 0, DEV,
+                        ctypes.c_void_p(u_d.data_ptr()), ctypes.byref(info))
+        _lib.check(rc, sv._h)
+        return info.iters, info.true_resid, info.outer_iters
+
+    stream_ptr = ctypes.c_void_p()
+    L.vf_get_stream(fast._h, ctypes.byref(stream_ptr))
+    ext = torch.cuda.ExternalStream(stream_ptr.value)
+
+    def timed(sv, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            step(sv)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        s0 = ctypes.c_uint64()
+        L.vf_launch_count(ctypes.byref(s0))
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.start()
+        ev0.record(ext)
+        res = None
+        for _ in range(steps):
+            res = step(sv)
+        ev1.record(ext)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        if dist:
+            dist.barrier()
+        s1 = ctypes.c_uint64()
+        L.vf_launch_count(ctypes.byref(s1))
+        ms = ev0.elapsed_time(ev1) / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, res, clocks, int(s1.value - s0.value)
+
+    sampler = ClockSampler(local) if rank == 0 else None
+    ms, (iters, true_resid, outer), clocks, launches = timed(fast, args.steps, args.warmup, sampler)
+    value = world * ndof / (ms / 1e3) / 1e6
+
+    # plain FP64 GMG-PCG (same hierarchy, FP64 everywhere) on the same GPU
+    plain = None
+    if not args.no_plain:
+        ps = solver(SolverOptions.robust(device=local, check_every=args.check_every))
+        L.vf_get_stream(ps._h, ctypes.byref(stream_ptr))
+        ext_plain = torch.cuda.ExternalStream(stream_ptr.value)
+        ext_save = ext
+        ext = ext_plain
+        pms, (pit, pres, _), _, _ = timed(ps, max(1, args.steps // 2), 1)
+        ext = ext_save
+        plain = {"ms_per_solve": pms, "iterations": pit, "true_resid": pres,
+                 "mdof_per_s": ndof / (pms / 1e3) / 1e6, "speedup_of_mixed": pms / ms}
+        ps.close()
+
+    # roofline of the dominant kernel: fused FP32 Jacobi sweep on the fine level
+    nodes = (nx + 1) * (ny + 1) * (nz + 1)
+    kms = ctypes.c_double()
+    _lib.check(L.vf_time_kernel(fast._h, 1, _lib.VF_PREC_FP32, 50, ctypes.byref(kms)), fast._h)
+    sweep_bytes = 53 * nodes   # u, b, Minv (12 B each), E 4 B, mask 1 B, u' 12 B per node
+    amv = ctypes.c_double()
+    _lib.check(L.vf_time_kernel(fast._h, 0, _lib.VF_PREC_FP32, 50, ctypes.byref(amv)), fast._h)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = sweep_bytes / (kms.value / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "k_fine_op<float, EPI_SMOOTH> (fused damped-Jacobi sweep, level 0)",
+                "ms_per_launch": kms.value, "algorithmic_bytes_per_launch": sweep_bytes,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650 GB/s",
+                "matvec_ms_per_launch": amv.value,
+                "matvec_gbs": 29 * nodes / (amv.value / 1e3) / 1e9}
+
+    # e2e through the public API (host numpy in/out every step)
+    e2e = None
+    if not args.no_e2e:
+        f_h = np.ascontiguousarray(p["f"], dtype=np.float64)
+        for _ in range(1):
+            fast.solve(E_mg, f_h, tol=TOL)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        ke = max(1, args.steps)
+        for _ in range(ke):
+            u_h = fast.solve(E_mg, f_h, tol=TOL)
+        t1 = time.perf_counter()
+        ems = (t1 - t0) * 1e3 / ke
+        if dist:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * ndof / (ems / 1e3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(8 * nelem + 8 * ndof), "d2h_bytes_per_step": int(8 * ndof),
+               "ms_per_step": ems, "true_resid": float(fast.last_info.true_resid),
+               "u_finite": bool(np.isfinite(u_h).all())}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_record()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 dots, refinement residual, coarsest solve)",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": args.workload, "dof": ndof, "active_voxels": int(p["active"].sum()),
+                       "levels": w["levels"], "solver": "mixed-precision GMG-PCG, Galerkin coarse ops, "
+                                                        "FP64 Cholesky coarsest",
+                       "tol": TOL, "l2": "working set > 126 MB L2 (vectors 54-107 MB each)",
+                       "parallelism": f"replicas x{world}"},
+            "iterations": iters, "outer_iterations": outer, "true_resid": true_resid,
+            "time_to_solution_s": ms / 1e3,
+            "plain_fp64": plain,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    fast.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="bracket_256x128x128")
+    ap.add_argument("--check-every", type=int, default=8)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,228 @@
+/*
+ * voxfea.h -- C-ABI of libvoxfea.so, the B200 (sm_100a) matrix-free voxel
+ * elasticity solve: hex8 element-by-element K*u inside PCG preconditioned by a
+ * geometric-multigrid V-cycle.
+ *
+ * This is the boundary the Python solver layer binds with ctypes
+ * (voxelsim_fea_b200/_lib.py).  Each entry point names the reference
+ * interface it replaces (VoxelSim-FEA, paths relative to that project).
+ *
+ * Conventions (identical to the reference, so host arrays pass through):
+ *   - grid of nx*ny*nz hex8 voxels of unit edge (stiffness scales with the
+ *     modulus the caller passes, E*vsize -- core/solve_worker.py:342-354);
+ *   - node id  ix + (nx+1)*(iy + (ny+1)*iz)       (core/fea.py:129-130);
+ *   - DOF id   3*node + c, c = x,y,z              (core/fea.py:17);
+ *   - element order iz fastest: e = (ix*ny + iy)*nz + iz (core/fea.py:133-148).
+ * All host arrays are caller-owned and only read/written during the call.
+ * Every function returns an int status (VF_OK == 0); nothing aborts the
+ * process.  vf_last_error() gives a message for the last failure on a handle,
+ * vf_global_last_error() for failures before a handle exists.
+ */
+#ifndef VOXFEA_H
+#define VOXFEA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VF_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  VF_OK = 0,
+  VF_ERR_ARG = 1,           /* invalid argument                      -> ValueError */
+  VF_ERR_STATE = 2,         /* wrong call order ("call set_fixed() before solve()",
+                               core/fea.py:427-428)                  -> RuntimeError */
+  VF_ERR_CUDA = 3,          /* CUDA runtime failure                  -> RuntimeError */
+  VF_ERR_NOMEM = 4,         /* device allocation failed              -> MemoryError */
+  VF_ERR_NO_DEVICE = 5,     /* no usable sm_100 device               -> RuntimeError */
+  VF_ERR_STALLED = 6,       /* MG-PCG stall/divergence guard fired
+                               (core/multigrid.py:523-531)           -> RuntimeError */
+  VF_ERR_NONFINITE = 7,     /* NaN/Inf in an input or an iterate     -> FloatingPointError */
+  VF_ERR_UNSUPPORTED = 8,   /* option combination not implemented   -> NotImplementedError */
+  VF_ERR_BREAKDOWN = 9      /* Krylov breakdown / singular coarse factor */
+};
+
+/* ---- options ------------------------------------------------------------ */
+enum { VF_PREC_FP64 = 0,    /* every vector, operator and transfer in FP64 */
+       VF_PREC_MIXED = 1,   /* FP32 PCG + V-cycle inside an FP64 iterative-
+                               refinement loop (FP64 dots, outer residual,
+                               coarsest solve) */
+       VF_PREC_FP32 = 2 };  /* FP32 vectors/operators, FP64 dots (no refinement) */
+
+enum { VF_METHOD_MG = 0,        /* GMG-preconditioned CG on the full grid
+                                   (core/multigrid.py MGSolver.solve) */
+       VF_METHOD_JACOBI = 1 };  /* Jacobi-PCG on the active elements only
+                                   (core/fea.py VoxelFEA._solve_jacobi) */
+
+enum { VF_COARSE_REDISCRETIZE = 0,  /* reference: coarse E = 2x2x2 mean, x 2^level,
+                                       injected Dirichlet mask
+                                       (core/multigrid.py:255-315) */
+       VF_COARSE_GALERKIN = 1 };    /* R A P with the masked trilinear P; robust
+                                       under void/solid contrast */
+
+enum { VF_COARSEST_JACOBI = 0,      /* reference: 30 damped-Jacobi sweeps
+                                       (core/multigrid.py:428-429) */
+       VF_COARSEST_CHOLESKY = 1 };  /* FP64 dense Cholesky direct solve */
+
+typedef struct vf_options {
+  int32_t struct_size;     /* sizeof(vf_options), set by vf_options_default */
+  int32_t method;          /* VF_METHOD_*                                   */
+  int32_t precision;       /* VF_PREC_*                                     */
+  int32_t n_smooth;        /* pre/post sweeps (multigrid.py:86, default 2)  */
+  int32_t min_elems;       /* hierarchy guard (multigrid.py:86, default 4)  */
+  int32_t max_levels;      /* (multigrid.py:86, default 6)                  */
+  int32_t coarse_op;       /* VF_COARSE_*                                   */
+  int32_t coarsest;        /* VF_COARSEST_*                                 */
+  int32_t coarse_sweeps;   /* sweeps of the Jacobi coarsest solve (30)      */
+  int32_t stall_guard;     /* 1: raise VF_ERR_STALLED like multigrid.py:523 */
+  int32_t check_every;     /* PCG iterations per device graph launch        */
+  int32_t use_graphs;      /* capture iteration chunks as CUDA graphs       */
+  int32_t device;          /* CUDA device ordinal                           */
+  int32_t max_outer;       /* VF_PREC_MIXED: refinement steps cap           */
+  double  omega;           /* Jacobi damping (multigrid.py:86, default 0.6) */
+  double  inner_tol;       /* VF_PREC_MIXED: residual reduction per inner solve */
+  int32_t reserved[8];
+} vf_options;
+
+typedef struct vf_solve_info {
+  int32_t iters;           /* PCG iterations (all inner iterations for MIXED);
+                              MGSolver.last_iters (multigrid.py:515)        */
+  int32_t outer_iters;     /* refinement steps (MIXED), else 0              */
+  int32_t converged;       /* MGSolver.last_converged                       */
+  int32_t status;          /* VF_OK, VF_ERR_STALLED, VF_ERR_BREAKDOWN, ...   */
+  double  resid_ratio;     /* MGSolver.last_resid_ratio (recurrence, or the
+                              FP64 true residual for MIXED)                 */
+  double  true_resid;      /* ||mask(f - K u)|| / ||mask f|| in FP64 at exit */
+  double  device_ms;       /* solve time on the solver's stream (events)    */
+  double  setup_ms;        /* of which: density / coarse-operator set-up    */
+} vf_solve_info;
+
+typedef struct vf_solver vf_solver;
+
+/* ---- library / device --------------------------------------------------- */
+int         vf_abi_version(void);
+const char* vf_status_string(int status);
+const char* vf_global_last_error(void);
+/* backend.gpu_device_count (core/backend_gpu.py:110-122) */
+int         vf_device_count(int32_t* count);
+/* backend._self_test (core/backend_gpu.py:40-60): runs the hex8 operator on a
+ * small grid on the device and compares with a host evaluation.  VF_OK if
+ * the device result agrees to 1e-12 (FP64) and 1e-5 (FP32). */
+int         vf_self_test(int32_t device);
+
+/* _hex8_KE / _hex8_B_C (core/fea.py:31-122): KE(E=1, nu) (576), the
+ * nu-independent split KE = lam*K_lam + mu*K_mu (576 each) and the centroid
+ * B0 (6x24).  Host-only; any output pointer may be NULL. */
+int         vf_hex8_tables(double nu, double* KE, double* K_lam, double* K_mu, double* B0);
+
+/* ---- solver lifetime ------------------------------------------------------ */
+void        vf_options_default(vf_options* opts);
+/* MGSolver.__init__ (core/multigrid.py:85-174) / VoxelFEA.__init__
+ * (core/fea.py:244-305): builds the level hierarchy (multigrid.py:141-148)
+ * and the Ke tables.  nu is the Poisson ratio used when vf_set_material gets
+ * no per-voxel ratio. */
+int         vf_create(int32_t nx, int32_t ny, int32_t nz, double nu,
+                      const vf_options* opts, vf_solver** out);
+/* MGSolver.close (core/multigrid.py:245-252) / VoxelFEA.close (fea.py:342-355) */
+int         vf_destroy(vf_solver* s);
+const char* vf_last_error(const vf_solver* s);
+int         vf_num_levels(const vf_solver* s, int32_t* n);
+int         vf_level_dims(const vf_solver* s, int32_t level, int32_t* dims3);
+
+/* ---- problem definition --------------------------------------------------- */
+/* MGSolver._build_free (multigrid.py:255-278) / VoxelFEA.set_fixed
+ * (fea.py:357-369): original (full-grid) DOF ids, any order, duplicates ok. */
+int vf_set_fixed(vf_solver* s, const int64_t* fixed_dofs, int64_t n);
+/* VoxelFEA active_elems (fea.py:266-279): uint8 per element (NULL = all).
+ * Used by VF_METHOD_JACOBI to restrict the system to the active elements'
+ * DOFs; the MG method takes e_min voids through the modulus instead. */
+int vf_set_active(vf_solver* s, const uint8_t* active);
+/* MGSolver.set_density (multigrid.py:281-315): per-element modulus (nelem,
+ * float64, iz-fastest); nu_elem (nelem) is an optional per-voxel Poisson
+ * ratio (NULL = the ratio given to vf_create).  Builds every level's operator,
+ * diagonal and, for VF_COARSEST_CHOLESKY, the coarsest factor.  flags may be
+ * VF_SOLVE_DEVICE_PTRS (E, nu_elem already in device memory). */
+int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32_t flags);
+
+/* ---- solve ---------------------------------------------------------------- */
+#define VF_SOLVE_DEVICE_PTRS 1u   /* array arguments are device pointers      */
+
+/* MGSolver.solve (multigrid.py:439-583) / VoxelFEA._solve_jacobi
+ * (fea.py:497-593): f and u_out are full-grid float64 (3*(nx+1)(ny+1)(nz+1));
+ * x0 may be NULL.  max_it <= 0 selects the reference default (1000 for MG,
+ * 4*n_free for Jacobi).  Returns VF_ERR_STALLED when the stall guard fires
+ * (u_out then holds the last iterate). */
+int vf_solve(vf_solver* s, const double* f, const double* x0, double tol,
+             int32_t max_it, uint32_t flags, double* u_out, vf_solve_info* info);
+/* Same as vf_solve, invoking progress(it, resid_ratio, tol, user) once per
+ * completed iteration, in order, from the calling thread -- the reference's
+ * progress_cb(it, resid, tol) contract (multigrid.py:518-519).  Iterations run
+ * on the device in chunks of vf_options.check_every, so callbacks arrive in
+ * bursts at chunk boundaries.  With a zero (masked) load the solve returns
+ * u = 0 immediately and info->iters = -1 (multigrid.py:471-473). */
+typedef void (*vf_progress_fn)(int32_t it, double resid_ratio, double tol, void* user);
+int vf_solve_cb(vf_solver* s, const double* f, const double* x0, double tol,
+                int32_t max_it, uint32_t flags, double* u_out, vf_solve_info* info,
+                vf_progress_fn progress, void* user);
+/* MGSolver.resid_history (multigrid.py:452, 517): copies up to cap entries. */
+int vf_resid_history(const vf_solver* s, double* out, int32_t cap, int32_t* n_out);
+
+/* ---- post-processing ------------------------------------------------------ */
+/* VoxelFEA.element_von_mises_stress (fea.py:604-626): centroid stress of every
+ * element with active[e] != 0 (active NULL = all), zeros elsewhere.  E_stress
+ * is per element (nelem); nu_elem optional per-voxel ratio. */
+int vf_von_mises(vf_solver* s, const double* u, const double* E_stress,
+                 const double* nu_elem, const uint8_t* active, double* vm_out);
+/* VoxelFEA.element_strain_energy (fea.py:595-602): u_e^T KE u_e, KE at E = 1. */
+int vf_strain_energy(vf_solver* s, const double* u, const uint8_t* active,
+                     double* se_out);
+/* fea.drop_unsupported_islands (fea.py:207-227): 6-connected flood fill of the
+ * active elements from those touching a fixed node (device kernels).
+ * kept_out may alias active.  *n_removed = active - kept (0 and kept = active
+ * when no active element touches a fixed node). */
+int vf_drop_unsupported_islands(int32_t nx, int32_t ny, int32_t nz,
+                                const uint8_t* active, const int64_t* fixed_dofs,
+                                int64_t n_fixed, uint8_t* kept_out,
+                                int64_t* n_removed);
+
+/* ---- level operators (parity tests and tools) ------------------------------
+ * Host float64 arrays in the reference layout of that level.  precision is
+ * VF_PREC_FP64 or VF_PREC_FP32 (the kernel variant that runs).              */
+/* MGSolver._apply (multigrid.py:318-341): y = mask(K_l u) */
+int vf_apply(vf_solver* s, int32_t level, int32_t precision, const double* u, double* y);
+/* MGSolver._smooth (multigrid.py:367-402): `sweeps` damped-Jacobi sweeps */
+int vf_smooth(vf_solver* s, int32_t level, int32_t precision, const double* u0,
+              const double* b, int32_t sweeps, double* out);
+/* MGSolver._restrict (multigrid.py:404-416): fine level -> level+1 */
+int vf_restrict(vf_solver* s, int32_t level, int32_t precision, const double* r_fine,
+                double* r_coarse);
+/* MGSolver._prolongate (multigrid.py:418-424): level+1 -> fine level */
+int vf_prolongate(vf_solver* s, int32_t level, int32_t precision, const double* e_coarse,
+                  double* e_fine);
+/* MGSolver._vcycle(0, r) (multigrid.py:426-436) */
+int vf_vcycle(vf_solver* s, int32_t precision, const double* r, double* z);
+/* MGSolver levels[l]['Minv'] (multigrid.py:300-304): 3 values per node */
+int vf_inv_diagonal(vf_solver* s, int32_t level, double* minv);
+
+/* ---- measurement ------------------------------------------------------------
+ * The solver's CUDA stream (cudaStream_t), for event timing by the caller. */
+int vf_get_stream(const vf_solver* s, void** stream);
+/* Kernels launched by this library since load (graph replays count every
+ * kernel node they contain). */
+int vf_launch_count(uint64_t* count);
+
+/* Times `iters` back-to-back launches of one kernel on the solver's stream with
+ * CUDA events (operands already resident; set_material must have run).
+ * kernel: 0 = fine operator y = K p (+ p.y), 1 = fused Jacobi sweep,
+ *         2 = residual, 3 = restriction, 4 = prolongation+add, 5 = V-cycle.
+ * *ms_per_launch receives the mean duration. */
+int vf_time_kernel(vf_solver* s, int32_t kernel, int32_t precision, int32_t iters,
+                   double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VOXFEA_H */

@@ -1,0 +1,70 @@
+"""Sparse Galerkin coarse operators (oracle, test-only).
+
+Not a reference algorithm: the reference rediscretizes its coarse levels
+(core/multigrid.py:281-315).  The CUDA path can instead build
+
+    A_{l+1} = D_{l+1} P^T D_l A_l D_l P D_{l+1}
+
+with the reference's trilinear P (``mg.prolong_op``, multigrid.py:42-73),
+D_0 the Dirichlet mask and D_{l+1} the DOFs whose Galerkin diagonal is
+non-zero.  This module assembles the same operators with scipy.sparse so the
+device stencils can be checked entry by entry (through their action).
+"""
+
+import numpy as np
+import scipy.sparse as sp
+
+from .hex8 import build_edof, hex8_ke, lame_split
+from .mg import level_dims, node_dims, prolong_op
+
+
+def fine_matrix(nx, ny, nz, E, nu=0.3, lam=None, mu=None):
+    """Assembled K = sum_e E_e Ke (or lam_e K_lam + mu_e K_mu) as CSR."""
+    edof = build_edof(nx, ny, nz)
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    if lam is None:
+        KE = hex8_ke(1.0, nu)
+        vals = (np.asarray(E, float)[:, None, None] * KE[None]).ravel()
+    else:
+        KL, KM = lame_split()
+        vals = (np.asarray(lam, float)[:, None, None] * KL[None]
+                + np.asarray(mu, float)[:, None, None] * KM[None]).ravel()
+    rows = np.repeat(edof, 24, axis=1).ravel()
+    cols = np.tile(edof, (1, 24)).ravel()
+    return sp.csr_matrix((vals, (rows, cols)), shape=(ndof, ndof))
+
+
+def prolong_matrix(fine_dims_el, coarse_dims_el):
+    """(3 Nf) x (3 Nc) trilinear P acting on interleaved DOFs."""
+    idx, w = prolong_op(node_dims(*fine_dims_el), node_dims(*coarse_dims_el))
+    Nf = idx.shape[0]
+    Nc = int(np.prod(node_dims(*coarse_dims_el)))
+    rows, cols, vals = [], [], []
+    for c in range(3):
+        rows.append(np.repeat(3 * np.arange(Nf) + c, 8))
+        cols.append((3 * idx + c).ravel())
+        vals.append(w.ravel())
+    P = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(3 * Nf, 3 * Nc))
+    P.sum_duplicates()
+    return P
+
+
+def galerkin_hierarchy(nx, ny, nz, E, fixed_dofs, nu=0.3, min_elems=4, max_levels=6,
+                       lam=None, mu=None):
+    """[(A_l, free_l)] for every level; A_0 is the masked fine operator."""
+    dims = level_dims(nx, ny, nz, min_elems, max_levels)
+    K = fine_matrix(nx, ny, nz, E, nu, lam, mu)
+    free = np.ones(K.shape[0], dtype=bool)
+    free[np.asarray(fixed_dofs, dtype=np.int64)] = False
+    D = sp.diags(free.astype(float))
+    A = (D @ K @ D).tocsr()
+    out = [(A, free)]
+    for li in range(1, len(dims)):
+        P = prolong_matrix(dims[li - 1], dims[li])
+        Dp = sp.diags(out[-1][1].astype(float))
+        Ac = (P.T @ Dp @ out[-1][0] @ Dp @ P).tocsr()
+        fc = Ac.diagonal() > 0
+        Dc = sp.diags(fc.astype(float))
+        out.append(((Dc @ Ac @ Dc).tocsr(), fc))
+    return out

@@ -1,0 +1,67 @@
+"""libvoxfea loads and exports every symbol include/voxfea.h declares; host-only
+entry points work without a GPU (no device compute is called here)."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+from conftest import REPO, golden
+
+
+def _declared_symbols():
+    text = open(os.path.join(REPO, "include", "voxfea.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"\b(vf_[a-z0-9_]+)\s*\(", text))
+    names.discard("vf_progress_fn")
+    return names
+
+
+def test_exports_match_header(lib):
+    from voxelsim_fea_b200 import _lib
+    declared = _declared_symbols()
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in voxfea.h but not exported"
+    assert declared == set(_lib.EXPORTS)
+
+
+def test_abi_and_options(lib):
+    from voxelsim_fea_b200 import _lib
+    assert lib.vf_abi_version() == 1
+    o = _lib.default_options()
+    assert o.struct_size == ctypes.sizeof(_lib.VfOptions)
+    assert (o.n_smooth, o.min_elems, o.max_levels, o.coarse_sweeps) == (2, 4, 6, 30)
+    assert abs(o.omega - 0.6) < 1e-15
+    assert lib.vf_status_string(_lib.VF_ERR_STALLED) == b"MG-PCG stalled/diverged"
+
+
+def test_host_hex8_tables_match_reference(lib):
+    """The C++ restatement of _hex8_KE / _hex8_B_C (host code of the library)."""
+    g = golden("hex8.npz")
+    for nu in (0.30, 0.33, 0.35):
+        KE = np.empty(576)
+        KL = np.empty(576)
+        KM = np.empty(576)
+        B0 = np.empty(144)
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        assert lib.vf_hex8_tables(nu, p(KE), p(KL), p(KM), p(B0)) == 0
+        tag = int(round(nu * 100))
+        np.testing.assert_allclose(KE.reshape(24, 24), g[f"KE_{tag}"], atol=2e-16)
+        np.testing.assert_allclose(B0.reshape(6, 24), g[f"B0_{tag}"], atol=0)
+        lam = nu / ((1 + nu) * (1 - 2 * nu))
+        mu = 1 / (2 * (1 + nu))
+        np.testing.assert_allclose(lam * KL + mu * KM, KE, atol=1e-15)
+    assert lib.vf_hex8_tables(0.5, None, None, None, None) == 1
+
+
+def test_create_rejects_bad_args(lib):
+    from voxelsim_fea_b200 import _lib
+    h = ctypes.c_void_p()
+    assert lib.vf_create(0, 4, 4, 0.3, None, ctypes.byref(h)) == _lib.VF_ERR_ARG
+    assert lib.vf_create(4, 4, 4, 0.7, None, ctypes.byref(h)) == _lib.VF_ERR_ARG
+    o = _lib.default_options()
+    o.struct_size = 3
+    assert lib.vf_create(4, 4, 4, 0.3, ctypes.byref(o), ctypes.byref(h)) == _lib.VF_ERR_ARG
+    assert not h.value

@@ -1,0 +1,142 @@
+"""End-to-end solves on the device vs the reference's own solves (golden
+vectors) and vs the CPU oracle.
+
+* reference algorithm (rediscretized MG, FP64): same iteration count and
+  residual history as core/multigrid.py, same displacement;
+* robust / mixed-precision B200 solvers: same displacement to the tolerance
+  the solve reaches, true FP64 residual below tol;
+* VoxelFEA facade on a noise part (e_min voids, Jacobi fallback path, von
+  Mises, strain energy, islands) vs the reference's Jacobi-PCG solution.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _cantilever():
+    from voxelsim_fea_b200 import generators
+    return generators.cantilever()
+
+
+def test_cantilever_reference_algorithm(gpu):
+    from voxelsim_fea_b200.multigrid import MGSolver
+    g = golden("cantilever_64x16x16_L3.npz")
+    p = _cantilever()
+    seen = []
+    m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"], max_levels=3)
+    u = m.solve(p["E_stiff"], p["f"], tol=1e-8, progress_cb=lambda it, r, t: seen.append((it, r)))
+    assert len(m.levels) == int(g["n_levels"]) == 3
+    assert m.last_iters == int(g["iters"]) == 19
+    assert m.last_converged
+    np.testing.assert_allclose(m.resid_history, g["resid_history"], rtol=1e-6, atol=1e-14)
+    assert [s[0] for s in seen] == list(range(1, 20))
+    np.testing.assert_allclose([s[1] for s in seen], m.resid_history, rtol=0, atol=0)
+    assert np.abs(u - g["u"]).max() <= 1e-9 * np.abs(g["u"]).max()
+    assert m.last_info.true_resid < 1e-8
+
+
+def test_cantilever_default_levels(gpu):
+    from voxelsim_fea_b200.multigrid import MGSolver
+    g6 = golden("cantilever_64x16x16_L6.npz")
+    p = _cantilever()
+    m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"])
+    u = m.solve(p["E_stiff"], p["f"], tol=1e-8)
+    assert len(m.levels) == int(g6["n_levels"])
+    assert m.last_iters == int(g6["iters"]) == 16
+    np.testing.assert_allclose(m.resid_history, g6["resid_history"], rtol=1e-6, atol=1e-14)
+    assert abs(u[2::3].min() / float(g6["u_tip"]) - 1) < 1e-9
+
+
+@pytest.mark.parametrize("preset", ["robust", "fast", "fp32"])
+def test_cantilever_b200_solvers(gpu, preset):
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    g = golden("cantilever_64x16x16_L3.npz")
+    p = _cantilever()
+    opts = {"robust": SolverOptions.robust(), "fast": SolverOptions.fast(),
+            "fp32": SolverOptions(precision="fp32", coarse="galerkin", coarsest="cholesky")}[preset]
+    tol = 1e-5 if preset == "fp32" else 1e-10
+    m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"], options=opts)
+    u = m.solve(p["E_stiff"], p["f"], tol=tol)
+    assert m.last_converged
+    ref = g["u"]
+    rel = np.abs(u - ref).max() / np.abs(ref).max()
+    assert rel < (1e-3 if preset == "fp32" else 1e-7), rel
+    if preset != "fp32":
+        assert m.last_info.true_resid < tol
+
+
+def test_solve_is_deterministic(gpu):
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    p = _cantilever()
+    m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"], options=SolverOptions.fast())
+    a = m.solve(p["E_stiff"], p["f"], tol=1e-8)
+    b = m.solve(p["E_stiff"], p["f"], tol=1e-8)
+    assert np.array_equal(a, b)
+    assert m.resid_history == list(m.resid_history)
+
+
+def test_warm_start_and_zero_load(gpu):
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    p = _cantilever()
+    m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"], options=SolverOptions.robust())
+    u = m.solve(p["E_stiff"], p["f"], tol=1e-8)
+    it_cold = m.last_iters
+    u2 = m.solve(p["E_stiff"], p["f"], tol=1e-8, x0=u)
+    assert m.last_iters < it_cold
+    assert np.abs(u2 - u).max() < 1e-7 * np.abs(u).max()
+    z = m.solve(p["E_stiff"], np.zeros_like(p["f"]), tol=1e-8)
+    assert not z.any()
+
+
+def test_noise_part_voxelfea(gpu):
+    """VoxelFEA (MG with e_min voids, robust hierarchy) and its Jacobi-PCG
+    path vs the reference's Jacobi-PCG solution on the active system."""
+    from voxelsim_fea_b200.fea import VoxelFEA, drop_unsupported_islands
+    g = golden("noise_32x16x16_jacobi.npz")
+    nx, ny, nz = (int(v) for v in g["dims"])
+    active = g["active"].astype(bool)
+    used = g["u"] != 0
+    ref = g["u"]
+    v = VoxelFEA(nx, ny, nz, nu=float(g["nu"]), active_elems=active)
+    v.set_fixed(g["fixed"])
+    u = v.solve(g["E_stiff"], g["f"], tol=1e-10)
+    assert v.last_converged
+    # e_min voids vs active restriction differ by O(e_min)
+    assert np.abs(u[used] - ref[used]).max() < 1e-6 * np.abs(ref).max()
+    vm = v.element_von_mises_stress(u, g["E_stress"]) / float(g["vsize"])
+    assert np.abs(vm - g["vm"]).max() < 1e-5 * g["vm"].max()
+    # the Jacobi-PCG path itself
+    vj = VoxelFEA(nx, ny, nz, nu=float(g["nu"]), active_elems=active, use_multigrid=False)
+    vj.set_fixed(g["fixed"])
+    uj = vj.solve(g["E_stiff"], g["f"], tol=1e-10)
+    assert vj.last_converged
+    assert abs(vj.last_iters - int(g["iters"])) <= max(3, int(0.02 * int(g["iters"])))
+    assert np.abs(uj - ref).max() < 1e-8 * np.abs(ref).max()
+    np.testing.assert_allclose(vj.element_von_mises_stress(uj, g["E_stress"]) / float(g["vsize"]),
+                               g["vm"], rtol=1e-6, atol=1e-8 * g["vm"].max())
+    np.testing.assert_allclose(vj.element_strain_energy(uj), g["se"], rtol=1e-6,
+                               atol=1e-10 * g["se"].max())
+    kept, n = drop_unsupported_islands(active.reshape(nx, ny, nz), g["fixed"])
+    assert n == 0 and np.array_equal(kept.ravel(), active)
+
+
+def test_islands_device(gpu):
+    from voxelsim_fea_b200.fea import drop_unsupported_islands
+    g = golden("islands_12x10x8.npz")
+    kept, n = drop_unsupported_islands(g["active"], g["fixed"])
+    np.testing.assert_array_equal(kept, g["kept"])
+    assert n == int(g["n_removed"])
+    # nothing reaches a support: input returned unchanged, 0 removed (fea.py:220-225)
+    kept2, n2 = drop_unsupported_islands(g["active"], np.zeros(0, np.int64))
+    assert n2 == 0 and np.array_equal(kept2, g["active"])
+
+
+def test_set_fixed_required(gpu):
+    from voxelsim_fea_b200.fea import VoxelFEA
+    v = VoxelFEA(4, 4, 4)
+    with pytest.raises(RuntimeError, match="set_fixed"):
+        v.solve(np.ones(64), np.zeros(375))

@@ -1,0 +1,95 @@
+"""The CPU oracle reproduces the reference's own outputs (golden vectors made
+by tests/golden/make_golden.py from core/fea.py and core/multigrid.py)."""
+
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import fea as ofea
+from oracle import hex8, islands, mg
+
+
+@pytest.mark.parametrize("nu", [0.30, 0.33, 0.35])
+def test_hex8_tables(nu):
+    g = golden("hex8.npz")
+    tag = int(round(nu * 100))
+    np.testing.assert_allclose(hex8.hex8_ke(1.0, nu), g[f"KE_{tag}"], rtol=0, atol=1e-15)
+    B, C = hex8.hex8_b_c(nu)
+    np.testing.assert_allclose(B, g[f"B0_{tag}"], atol=1e-15)
+    np.testing.assert_allclose(C, g[f"C0_{tag}"], atol=1e-15)
+    lam, mu = hex8.lame(1.0, nu)
+    KL, KM = hex8.lame_split()
+    np.testing.assert_allclose(lam * KL + mu * KM, g[f"KE_{tag}"], atol=1e-14)
+
+
+def test_edof():
+    np.testing.assert_array_equal(hex8.build_edof(3, 2, 4), golden("hex8.npz")["edof_3x2x4"])
+
+
+def test_level_operators():
+    g = golden("mg_ops_16x8x8.npz")
+    nx, ny, nz = (int(v) for v in g["dims"])
+    m = mg.MGOracle(nx, ny, nz, g["fixed"], nu=float(g["nu"]))
+    m.set_density(g["E"])
+    assert len(m.levels) == int(g["n_levels"])
+    for li in range(len(m.levels)):
+        np.testing.assert_array_equal(m.levels[li]["free"], g[f"free{li}"])
+        np.testing.assert_allclose(m.levels[li]["Minv"], g[f"Minv{li}"], rtol=1e-14)
+        np.testing.assert_allclose(m.apply(li, g[f"u{li}"]), g[f"Ku{li}"], rtol=1e-12, atol=1e-12)
+        u0 = g[f"u{li}"] * g[f"free{li}"]
+        np.testing.assert_allclose(m.smooth(li, u0, g[f"b{li}"], 2), g[f"smooth{li}"],
+                                   rtol=1e-12, atol=1e-12)
+        if li + 1 < len(m.levels):
+            np.testing.assert_allclose(m.restrict(li, g[f"u{li}"]), g[f"restrict{li}"], atol=1e-12)
+            np.testing.assert_allclose(m.prolongate(li, g[f"ec{li}"]), g[f"prolong{li}"], atol=1e-12)
+    np.testing.assert_allclose(m.vcycle(0, g["vc_r"]), g["vc_z"], rtol=1e-11, atol=1e-12)
+
+
+def test_cantilever_solve_pins_reference():
+    g = golden("cantilever_64x16x16_L3.npz")
+    from voxelsim_fea_b200 import generators
+    p = generators.cantilever()
+    m = mg.MGOracle(*p["dims"], p["fixed_dofs"], nu=p["nu"], max_levels=3)
+    u = m.solve(p["E_stiff"], p["f"], tol=1e-8)
+    assert m.last_iters == int(g["iters"]) == 19
+    np.testing.assert_allclose(m.resid_history, g["resid_history"], rtol=1e-6, atol=1e-14)
+    np.testing.assert_allclose(u, g["u"], rtol=0, atol=1e-10 * np.abs(g["u"]).max())
+    # known answers of the cantilever (tip deflection ~ -8.22e-5 m, max VM ~ 91.66 MPa)
+    assert abs(u[2::3].min() / -8.36e-5 - 1) < 0.05
+    assert abs(g["vm"].max() / 91.66e6 - 1) < 1e-3
+
+
+def test_noise_jacobi_pins_reference():
+    g = golden("noise_32x16x16_jacobi.npz")
+    nx, ny, nz = (int(v) for v in g["dims"])
+    v = ofea.VoxelFEAOracle(nx, ny, nz, nu=float(g["nu"]), active_elems=g["active"],
+                            use_multigrid=False)
+    v.set_fixed(g["fixed"])
+    u = v.solve(g["E_stiff"], g["f"], tol=1e-10)
+    assert v.last_iters == int(g["iters"])
+    np.testing.assert_allclose(u, g["u"], atol=1e-12 * np.abs(g["u"]).max())
+    vm = v.element_von_mises_stress(u, g["E_stress"]) / float(g["vsize"])
+    np.testing.assert_allclose(vm, g["vm"], rtol=1e-9, atol=1e-6 * g["vm"].max())
+    np.testing.assert_allclose(v.element_strain_energy(u), g["se"], rtol=1e-9,
+                               atol=1e-12 * g["se"].max())
+
+
+def test_islands():
+    g = golden("islands_12x10x8.npz")
+    nx, ny, nz = g["active"].shape
+    np.testing.assert_array_equal(islands.seed_from_fixed_dofs(nx, ny, nz, g["fixed"]), g["seed"])
+    kept, n = islands.drop_unsupported_islands(g["active"], g["fixed"])
+    np.testing.assert_array_equal(kept, g["kept"])
+    assert n == int(g["n_removed"])
+
+
+def test_galerkin_oracle_equals_rediscretization_for_uniform_E():
+    """Sanity of the sparse RAP oracle: with uniform E and no Dirichlet DOFs,
+    Galerkin coarsening of Q1 hex8 equals rediscretization (x 2 per level)."""
+    from oracle import galerkin
+    nx, ny, nz = 8, 4, 4
+    E = np.full(nx * ny * nz, 3.0)
+    hier = galerkin.galerkin_hierarchy(nx, ny, nz, E, np.zeros(0, np.int64), max_levels=2)
+    A1 = hier[1][0]
+    K1 = galerkin.fine_matrix(4, 2, 2, np.full(16, 3.0 * 2.0))
+    assert abs(A1 - K1).max() < 1e-12 * abs(K1).max()

@@ -1,0 +1,270 @@
+// Coarsest-level direct solve in FP64: the assembled coarsest operator (with
+// identity rows on non-free DOFs) is factored A = L L^T by a blocked
+// right-looking Cholesky, inverted as A^{-1} = Y^T Y with Y = L^{-1}, and each
+// V-cycle applies the explicit inverse with one GEMV.  All kernels are plain
+// CUDA-core FP64 (the coarsest level holds a few thousand DOFs at most);
+// the factorization runs once per set_material, outside the iteration.
+// Replaces the reference's 30-sweep Jacobi "coarse solve" (core/multigrid.py:428-429)
+// when VF_COARSEST_CHOLESKY is selected.
+#include "vf_common.cuh"
+
+namespace vf {
+
+namespace {
+
+constexpr int NB = 32;
+
+// Dense row-major A from the coarsest stencil; node order = reference order
+// of the level's nodes, DOF 3*node + c.
+__global__ void k_dense_assemble(Grid c, const double* __restrict__ st, const uint8_t* __restrict__ cm,
+                                 double* __restrict__ A, int n) {
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1, nint = nx1 * ny1 * (c.lz + 1);
+  const long long ns = c.n;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint * 27; t += gridDim.x * blockDim.x) {
+    const int r = t / 27, s = t % 27;
+    const int x = r % nx1, rr = r / nx1, y = rr % ny1, z = rr / ny1;
+    const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+    const int X = x + dx, Y = y + dy, Z = z + dz;
+    if (X < 0 || X > c.lx || Y < 0 || Y > c.ly || Z < 0 || Z > c.lz) continue;
+    const int q = X + nx1 * (Y + ny1 * Z);
+    const int p = c.idx(x, y, z);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        A[(long long)(3 * r + a) * n + 3 * q + b] = st[((long long)s * 9 + a * 3 + b) * ns + p];
+    if (s == 13) {
+      const uint8_t m = cm[p];
+      for (int a = 0; a < 3; ++a)
+        if (!((m >> a) & 1)) A[(long long)(3 * r + a) * n + 3 * r + a] = 1.0;
+    }
+  }
+}
+
+// Factor the nb x nb diagonal block at (k, k) (rows already updated).
+__global__ void k_potrf_diag(double* A, int n, int k, int nb, int* info) {
+  __shared__ double L[NB][NB + 1];
+  const int t = threadIdx.x;
+  for (int j = 0; j < nb; ++j) L[t][j] = (t < nb) ? A[(long long)(k + t) * n + k + j] : 0.0;
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    if (t == j) {
+      const double d = L[j][j];
+      if (!(d > 0.0)) {
+        if (*info == 0) *info = k + j + 1;
+        L[j][j] = 1.0;
+      } else {
+        L[j][j] = sqrt(d);
+      }
+    }
+    __syncthreads();
+    const double piv = L[j][j];
+    if (t > j && t < nb) L[t][j] /= piv;
+    __syncthreads();
+    if (t > j && t < nb)
+      for (int l = j + 1; l <= t; ++l) L[t][l] -= L[t][j] * L[l][j];
+    __syncthreads();
+  }
+  if (t < nb)
+    for (int j = 0; j <= t; ++j) A[(long long)(k + t) * n + k + j] = L[t][j];
+}
+
+// Rows i >= k+nb: A[i, k:k+nb] <- A[i, k:k+nb] L_kk^{-T}.
+__global__ void k_trsm_panel(double* A, int n, int k, int nb) {
+  __shared__ double L[NB][NB + 1];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e / nb, j = e % nb;
+    L[i][j] = (j <= i) ? A[(long long)(k + i) * n + k + j] : 0.0;
+  }
+  __syncthreads();
+  const int i = k + nb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x[NB];
+  for (int j = 0; j < nb; ++j) {
+    double v = A[(long long)i * n + k + j];
+    for (int l = 0; l < j; ++l) v -= x[l] * L[j][l];
+    x[j] = v / L[j][j];
+  }
+  for (int j = 0; j < nb; ++j) A[(long long)i * n + k + j] = x[j];
+}
+
+// Trailing update (lower triangle): A[i][j] -= sum_l A[i][k+l] A[j][k+l].
+__global__ void k_syrk_update(double* A, int n, int k, int nb) {
+  const int t0 = k + nb;
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  if (bj > bi) return;
+  const int i0 = t0 + bi * 32, j0 = t0 + bj * 32;
+  __shared__ double Pi[32][NB + 1], Pj[32][NB + 1];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;   // 256 threads: ty 0..7
+  for (int r = ty; r < 32; r += 8) {
+    Pi[r][tx] = (i0 + r < n && tx < nb) ? A[(long long)(i0 + r) * n + k + tx] : 0.0;
+    Pj[r][tx] = (j0 + r < n && tx < nb) ? A[(long long)(j0 + r) * n + k + tx] : 0.0;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r, j = j0 + tx;
+    if (i >= n || j >= n || j > i) continue;
+    double s = 0.0;
+    for (int l = 0; l < nb; ++l) s += Pi[r][l] * Pj[tx][l];
+    A[(long long)i * n + j] -= s;
+  }
+}
+
+// Forward substitution block: Y[k:k+nb, 0:ncol] <- L_kk^{-1} Y[k:k+nb, 0:ncol].
+__global__ void k_trsv_block_rows(const double* A, double* Y, int n, int k, int nb, int ncol) {
+  __shared__ double L[NB][NB + 1];
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e / nb, j = e % nb;
+    L[i][j] = (j <= i) ? A[(long long)(k + i) * n + k + j] : 0.0;
+  }
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  double x[NB];
+  for (int i = 0; i < nb; ++i) {
+    double v = Y[(long long)(k + i) * n + col];
+    for (int l = 0; l < i; ++l) v -= L[i][l] * x[l];
+    x[i] = v / L[i][i];
+  }
+  for (int i = 0; i < nb; ++i) Y[(long long)(k + i) * n + col] = x[i];
+}
+
+// Y[i, 0:ncol] -= sum_l L[i][k+l] Y[k+l, 0:ncol] for i >= k+nb.
+__global__ void k_trsm_update(const double* A, double* Y, int n, int k, int nb, int ncol) {
+  const int i0 = k + nb + blockIdx.y * 32, c0 = blockIdx.x * 32;
+  __shared__ double Li[32][NB + 1], Yk[NB][33];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  for (int r = ty; r < 32; r += 8) {
+    Li[r][tx] = (i0 + r < n && tx < nb) ? A[(long long)(i0 + r) * n + k + tx] : 0.0;
+    Yk[r][tx] = (r < nb && c0 + tx < ncol) ? Y[(long long)(k + r) * n + c0 + tx] : 0.0;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r, c = c0 + tx;
+    if (i >= n || c >= ncol) continue;
+    double s = 0.0;
+    for (int l = 0; l < nb; ++l) s += Li[r][l] * Yk[l][tx];
+    Y[(long long)i * n + c] -= s;
+  }
+}
+
+// Ainv = Y^T Y (Y lower triangular): Ainv[i][j] = sum_{l >= max(i,j)} Y[l][i] Y[l][j].
+__global__ void k_yty(const double* Y, double* Ainv, int n) {
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  __shared__ double Yi[32][33], Yj[32][33];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  double acc[4] = {0, 0, 0, 0};
+  const int lstart = (i0 > j0 ? i0 : j0);
+  for (int l0 = lstart; l0 < n; l0 += 32) {
+    for (int r = ty; r < 32; r += 8) {
+      const int l = l0 + r;
+      Yi[r][tx] = (l < n && i0 + tx < n) ? Y[(long long)l * n + i0 + tx] : 0.0;
+      Yj[r][tx] = (l < n && j0 + tx < n) ? Y[(long long)l * n + j0 + tx] : 0.0;
+    }
+    __syncthreads();
+    for (int q = 0; q < 4; ++q) {
+      const int r = ty + 8 * q;
+      double s = 0.0;
+      for (int l = 0; l < 32; ++l) s += Yi[l][r] * Yj[l][tx];
+      acc[q] += s;
+    }
+    __syncthreads();
+  }
+  for (int q = 0; q < 4; ++q) {
+    const int i = i0 + ty + 8 * q, j = j0 + tx;
+    if (i < n && j < n) Ainv[(long long)i * n + j] = acc[q];
+  }
+}
+
+__global__ void k_set_identity(double* Y, int n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * n;
+       e += (long long)gridDim.x * blockDim.x)
+    Y[e] = (e / n == e % n) ? 1.0 : 0.0;
+}
+
+// x = Ainv b on the coarsest level; b gathered into shared memory in FP64.
+template <typename T>
+__global__ void k_dense_solve(Grid c, const double* __restrict__ Ainv, int n, const T* __restrict__ b,
+                              T* __restrict__ x, const KrylovState* ks) {
+  if (ks && ks->done) return;
+  extern __shared__ double sb[];
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int r = i / 3, comp = i % 3;
+    const int xx = r % nx1, rr = r / nx1, yy = rr % ny1, zz = rr / ny1;
+    sb[i] = (double)b[3 * (long long)c.idx(xx, yy, zz) + comp];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
+    const double* row = Ainv + (long long)i * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += row[j] * sb[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      const int r = i / 3, comp = i % 3;
+      const int xx = r % nx1, rr = r / nx1, yy = rr % ny1, zz = rr / ny1;
+      x[3 * (long long)c.idx(xx, yy, zz) + comp] = (T)s;
+    }
+  }
+}
+
+}  // namespace
+
+int dense_assemble(const Grid& c, const double* stencil, const uint8_t* cmask, double* A, int n, cudaStream_t st) {
+  cudaMemsetAsync(A, 0, sizeof(double) * (size_t)n * n, st);
+  const long long work = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1) * 27;
+  int blocks = (int)((work + 255) / 256);
+  launch_k(k_dense_assemble, blocks, 256, 0, st, c, stencil, cmask, A, n);
+  return 0;
+}
+
+// A (n x n, lower part) is overwritten by L; work (n x n) receives A^{-1}
+// ... then copied back into A.  d_info > 0 flags a non-positive pivot.
+int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStream_t st) {
+  cudaMemsetAsync(d_info, 0, sizeof(int), st);
+  for (int k = 0; k < n; k += NB) {
+    const int nb = (n - k < NB) ? (n - k) : NB;
+    launch_k(k_potrf_diag, 1, NB, 0, st, A, n, k, nb, d_info);
+    const int rest = n - k - nb;
+    if (rest > 0) {
+      launch_k(k_trsm_panel, (rest + 127) / 128, 128, 0, st, A, n, k, nb);
+      const int tiles = (rest + 31) / 32;
+      launch_k(k_syrk_update, dim3(tiles, tiles), 256, 0, st, A, n, k, nb);
+    }
+  }
+  // Y = L^{-1} into work
+  launch_k(k_set_identity, 148 * 4, 256, 0, st, work, n);
+  for (int k = 0; k < n; k += NB) {
+    const int nb = (n - k < NB) ? (n - k) : NB;
+    const int ncol = k + nb;
+    launch_k(k_trsv_block_rows, (ncol + 127) / 128, 128, 0, st, A, work, n, k, nb, ncol);
+    const int rest = n - k - nb;
+    if (rest > 0) {
+      launch_k(k_trsm_update, dim3((ncol + 31) / 32, (rest + 31) / 32), 256, 0, st, A, work, n, k, nb, ncol);
+    }
+  }
+  // A <- Y^T Y
+  const int tiles = (n + 31) / 32;
+  launch_k(k_yty, dim3(tiles, tiles), 256, 0, st, work, A, n);
+  return 0;
+}
+
+// b is staged in dynamic shared memory (n doubles, n <= 16384).
+void dense_prepare_smem(int n) {
+  const int bytes = (int)sizeof(double) * n;
+  cudaFuncSetAttribute(k_dense_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_dense_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <typename T>
+void launch_dense_solve(const Grid& c, const double* Ainv, int n, const T* b, T* x, const KrylovState* ks,
+                        cudaStream_t st) {
+  int blocks = (n + 7) / 8;
+  if (blocks > 148 * 2) blocks = 148 * 2;
+  launch_k(k_dense_solve<T>, blocks, 256, sizeof(double) * n, st, c, Ainv, n, b, x, ks);
+}
+template void launch_dense_solve<double>(const Grid&, const double*, int, const double*, double*, const KrylovState*, cudaStream_t);
+template void launch_dense_solve<float>(const Grid&, const double*, int, const float*, float*, const KrylovState*, cudaStream_t);
+
+}  // namespace vf

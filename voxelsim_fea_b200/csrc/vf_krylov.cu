@@ -1,0 +1,138 @@
+// PCG vector kernels (core/multigrid.py:497-546): each is one memory pass
+// fused with its FP64 reduction; the scalar recurrences (alpha, beta, ratio,
+// convergence / stall / max_it tests) finalize on the device (vf_reduce.cuh).
+// Vectors are walked over the whole padded array: ghost entries are zero, so
+// they add nothing and the walk stays contiguous.
+#include "vf_common.cuh"
+#include "vf_reduce.cuh"
+
+namespace vf {
+
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_dot(long long n3, const T* __restrict__ a, const T* __restrict__ b,
+                                                     double* partials, KrylovState* ks, int slot) {
+  if (ks->done && slot != SLOT_FNORM && slot != SLOT_RZ_INIT && slot != SLOT_OUTER && slot != SLOT_PLAIN) return;
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    s += (double)a[i] * (double)b[i];
+  reduce_and_finalize(s, partials, ks, slot, nullptr);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_cg_update(long long n3, T* __restrict__ x, const T* __restrict__ p,
+                                                           T* __restrict__ r, const T* __restrict__ Ap,
+                                                           double* partials, KrylovState* ks, double* hist) {
+  if (ks->done) return;
+  const T alpha = (T)ks->alpha;
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    const T ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    s += (double)ri * (double)ri;
+  }
+  reduce_and_finalize(s, partials, ks, SLOT_RR, hist);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_p_update(long long n3, T* __restrict__ p, const T* __restrict__ z,
+                                                          const KrylovState* ks) {
+  if (ks->done) return;
+  const bool restart = ks->restart != 0;
+  const T beta = (T)ks->beta;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    p[i] = restart ? z[i] : z[i] + beta * p[i];
+}
+
+template <typename T>
+__global__ void k_jacobi_precond(int n, const T* __restrict__ r, const T* __restrict__ minv,
+                                 const uint8_t* __restrict__ mask, T* __restrict__ z, const KrylovState* ks) {
+  if (ks && ks->done) return;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const uint8_t m = mask[p];
+    const long long p3 = 3 * (long long)p;
+    z[p3] = (m & 1) ? minv[p3] * r[p3] : (T)0;
+    z[p3 + 1] = (m & 2) ? minv[p3 + 1] * r[p3 + 1] : (T)0;
+    z[p3 + 2] = (m & 4) ? minv[p3 + 2] * r[p3 + 2] : (T)0;
+  }
+}
+
+template <typename T>
+__global__ void k_copy(long long n3, const T* __restrict__ s, T* __restrict__ d, const KrylovState* ks) {
+  if (ks && ks->done) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    d[i] = s[i];
+}
+
+// Mixed precision: r32 = r64 / ||r64|| (inner solves see a unit right-hand
+// side, keeping FP32 far from under/overflow), remember the scale.
+__global__ void k_ir_prepare(long long n3, const double* __restrict__ r64, float* __restrict__ r32, KrylovState* ks) {
+  const double s = sqrt(ks->rr);
+  const double inv = s > 0.0 ? 1.0 / s : 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    r32[i] = (float)(r64[i] * inv);
+  if (blockIdx.x == 0 && threadIdx.x == 0) ks->scale = s;
+}
+
+__global__ void k_ir_accumulate(long long n3, double* __restrict__ x64, const float* __restrict__ d32,
+                                const KrylovState* ks) {
+  const double s = ks->scale;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    x64[i] += s * (double)d32[i];
+}
+
+__global__ void k_sub_from(long long n3, const double* __restrict__ f, double* __restrict__ r) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    r[i] = f[i] - r[i];
+}
+
+}  // namespace
+
+template <typename T>
+void launch_dot(const Grid& g, const T* a, const T* b, double* partials, KrylovState* ks, int slot, cudaStream_t st) {
+  launch_k(k_dot<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, a, b, partials, ks, slot);
+}
+template <typename T>
+void launch_cg_update(const Grid& g, T* x, const T* p, T* r, const T* Ap, double* partials, KrylovState* ks,
+                      double* hist, cudaStream_t st) {
+  launch_k(k_cg_update<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, p, r, Ap, partials, ks, hist);
+}
+template <typename T>
+void launch_p_update(const Grid& g, T* p, const T* z, KrylovState* ks, cudaStream_t st) {
+  launch_k(k_p_update<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, p, z, ks);
+}
+template <typename T>
+void launch_jacobi_precond(const Grid& g, const T* r, const T* minv3, const uint8_t* mask, T* z,
+                           const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_jacobi_precond<T>, kVecBlocks, kVecThreads, 0, st, g.n, r, minv3, mask, z, ks);
+}
+template <typename T>
+void launch_copy_vec(const Grid& g, const T* src, T* dst, const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_copy<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, src, dst, ks);
+}
+void launch_norm2_f64(const Grid& g, const double* v, double* partials, KrylovState* ks, int slot, cudaStream_t st) {
+  launch_k(k_dot<double>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, v, v, partials, ks, slot);
+}
+void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState* ks, cudaStream_t st) {
+  launch_k(k_ir_prepare, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r64, r32, ks);
+}
+void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_ir_accumulate, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x64, d32, ks);
+}
+void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st) {
+  launch_k(k_sub_from, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, f, r);
+}
+
+#define VF_INST(T)                                                                                            \
+  template void launch_dot<T>(const Grid&, const T*, const T*, double*, KrylovState*, int, cudaStream_t);    \
+  template void launch_cg_update<T>(const Grid&, T*, const T*, T*, const T*, double*, KrylovState*, double*, cudaStream_t); \
+  template void launch_p_update<T>(const Grid&, T*, const T*, KrylovState*, cudaStream_t);                   \
+  template void launch_jacobi_precond<T>(const Grid&, const T*, const T*, const uint8_t*, T*, const KrylovState*, cudaStream_t); \
+  template void launch_copy_vec<T>(const Grid&, const T*, T*, const KrylovState*, cudaStream_t);
+VF_INST(double)
+VF_INST(float)
+#undef VF_INST
+
+}  // namespace vf

@@ -1,0 +1,118 @@
+// Deterministic FP64 reductions with a last-block-done finalize, and the
+// scalar logic of the PCG recurrences that runs on the device so that no
+// host round-trip is needed inside an iteration (the reference blocks on a
+// float() per dot: core/multigrid.py:471, 499, 516, 533).
+//
+// Every reduction kernel runs a FIXED grid over a grid-stride loop; each CTA
+// writes one partial, and the last CTA to finish sums the partials in index
+// order.  The result therefore depends only on the problem size, never on
+// scheduling: two runs are bitwise identical.
+#pragma once
+
+#include "vf_common.cuh"
+
+namespace vf {
+
+// Reduction slots: what the finalize does with the sum.
+enum RedSlot {
+  SLOT_PAP = 0,      // p.Ap      -> alpha (or stop on pAp == 0, multigrid.py:500-511)
+  SLOT_RR = 1,       // r.r       -> ratio, history, tol / stall / max_it (multigrid.py:516-531)
+  SLOT_RZ = 2,       // r.z       -> beta or restart (multigrid.py:533-546)
+  SLOT_RZ_INIT = 3,  // r.z before the loop (multigrid.py:476)
+  SLOT_FNORM = 4,    // ||f||^2   -> fnorm (multigrid.py:471)
+  SLOT_OUTER = 5,    // ||r64||^2 -> outer (refinement) residual
+  SLOT_PLAIN = 6     // sum stored in ks->rr only
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum in a fixed order; valid in thread 0.  blockDim.x <= 1024.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double s_warp[32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_warp[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (w == 0) {
+    t = (lane < (int)((blockDim.x + 31) >> 5)) ? s_warp[lane] : 0.0;
+    t = warp_sum(t);
+  }
+  return t;
+}
+
+__device__ inline void finalize_slot(KrylovState* ks, int slot, double total, double* hist) {
+  switch (slot) {
+    case SLOT_PAP: {
+      ks->pAp = total;
+      if (!(total == total) || total == INFINITY || total == -INFINITY) {
+        ks->done = 1; ks->status = KS_NONFINITE;
+      } else if (total == 0.0) {
+        ks->done = 1;
+        ks->status = (ks->resid < ks->tol) ? KS_CONVERGED : KS_BREAKDOWN;
+      } else {
+        ks->alpha = ks->rz / total;
+      }
+      break;
+    }
+    case SLOT_RR: {
+      ks->rr = total;
+      const int it = ks->it + 1;
+      ks->it = it;
+      const double ratio = sqrt(total) / ks->fnorm;
+      ks->resid = ratio;
+      if (hist) hist[ks->it_base + it - 1] = ratio * ks->hist_scale;
+      if (!(ratio == ratio)) { ks->done = 1; ks->status = KS_NONFINITE; break; }
+      if (ratio < ks->tol) { ks->done = 1; ks->status = KS_CONVERGED; break; }
+      if (ratio < ks->best) ks->best = ratio;
+      if (ks->stall_guard && it >= 10 && ratio > 5.0 * ks->best) {
+        ks->done = 1; ks->status = KS_STALLED; break;
+      }
+      if (it >= ks->max_it) { ks->done = 1; ks->status = KS_MAXIT; }
+      break;
+    }
+    case SLOT_RZ: {
+      ks->rz_new = total;
+      if (ks->rz == 0.0) { ks->restart = 1; ks->beta = 0.0; }
+      else { ks->restart = 0; ks->beta = total / ks->rz; }
+      ks->rz = total;
+      break;
+    }
+    case SLOT_RZ_INIT: ks->rz = total; ks->restart = 0; break;
+    case SLOT_FNORM: ks->fnorm = sqrt(total); break;
+    case SLOT_OUTER: ks->rr = total; ks->resid = sqrt(total) / ks->fnorm; break;
+    default: ks->rr = total; break;
+  }
+}
+
+// Called by every thread of every CTA with its own partial `v`.  The CTA sum
+// goes to partials[blockIdx.x]; the last CTA finalizes.
+__device__ inline void reduce_and_finalize(double v, double* partials, KrylovState* ks, int slot,
+                                           double* hist) {
+  __shared__ bool s_last;
+  double bsum = block_sum(v);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = bsum;
+    __threadfence();
+    unsigned int prev = atomicAdd(&ks->counter[slot], 1u);
+    s_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double t = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += ((volatile double*)partials)[i];
+  t = block_sum(t);
+  if (threadIdx.x == 0) {
+    finalize_slot(ks, slot, t, hist);
+    ks->counter[slot] = 0u;
+    __threadfence();
+  }
+}
+
+}  // namespace vf

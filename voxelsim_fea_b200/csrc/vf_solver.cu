@@ -1,0 +1,1307 @@
+// libvoxfea: solver object and C-ABI (include/voxfea.h).
+//
+// One vf_solver = one device, one non-blocking stream, the level hierarchy of
+// core/multigrid.py:141-171 laid out in HBM (vf_common.cuh), and the PCG
+// state.  The iteration loop of core/multigrid.py:497-546 runs entirely on the
+// device: dots finalize into device scalars (vf_reduce.cuh) and every kernel
+// of an iteration turns into a no-op once the device-side `done` flag is set,
+// so CHUNKS of iterations are captured once as a CUDA graph and replayed; the
+// host only reads the state between chunks (progress callbacks, history).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/voxfea.h"
+#include "vf_common.cuh"
+#include "vf_hex8.h"
+#include "vf_reduce.cuh"
+
+namespace vf {
+unsigned long long direct_launches();
+// launchers defined in other translation units without a header entry
+void launch_elem_allfree(const Grid& f, const uint8_t* fmask, uint8_t* allfree, cudaStream_t st);
+void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu, const uint8_t* fmask,
+                               const uint8_t* allfree, const Grid& c, double* stencil_c, const double* Gtab,
+                               const double* Ktab, int lame, cudaStream_t st);
+void launch_stencil_from_elements(const Grid& g, const double* E, const double* mu, const uint8_t* mask,
+                                  double* stencil, const double* Ktab, int lame, cudaStream_t st);
+void launch_galerkin_mask(const Grid& c, double* stencil, uint8_t* cmask, double* minv3, cudaStream_t st);
+void launch_stencil_diag(const Grid& c, double* stencil, const uint8_t* cmask, double* minv3, cudaStream_t st);
+void dense_prepare_smem(int n);
+void launch_strain_energy_tab(const Grid& g, const double* u_pad, const uint8_t* active_ref, const double* KE,
+                              double* se_ref, cudaStream_t st);
+}  // namespace vf
+
+using namespace vf;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<unsigned long long> g_launches{0};
+
+// Kernel nodes of an instantiated chunk graph.
+unsigned long long graph_kernel_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+  unsigned long long k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
+struct Level {
+  Grid g{};
+  uint8_t* mask = nullptr;
+  bool galerkin = false;   // operator is the assembled stencil
+  double* E64 = nullptr; double* mu64 = nullptr; double* minv64 = nullptr; double* st64 = nullptr;
+  float* E32 = nullptr; float* mu32 = nullptr; float* minv32 = nullptr; float* st32 = nullptr;
+  double* w64[4] = {nullptr, nullptr, nullptr, nullptr};   // x, tmp, resid, rhs
+  float* w32[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+template <typename T> struct Sel;
+template <> struct Sel<double> {
+  static double* E(Level& l) { return l.E64; }
+  static double* mu(Level& l) { return l.mu64; }
+  static double* minv(Level& l) { return l.minv64; }
+  static double* st(Level& l) { return l.st64; }
+  static double* w(Level& l, int i) { return l.w64[i]; }
+};
+template <> struct Sel<float> {
+  static float* E(Level& l) { return l.E32; }
+  static float* mu(Level& l) { return l.mu32; }
+  static float* minv(Level& l) { return l.minv32; }
+  static float* st(Level& l) { return l.st32; }
+  static float* w(Level& l, int i) { return l.w32[i]; }
+};
+
+}  // namespace
+
+struct vf_solver {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  vf_options o{};
+  double nu = 0.3;
+  int nx = 0, ny = 0, nz = 0;
+  std::vector<Level> L;
+  double tab[1728];    // KE(nu) | K_lam | K_mu
+  double B0[144];
+  double* d_Gtab = nullptr;   // Galerkin child tables (8 or 16 x 576)
+  double* d_Ktab = nullptr;   // KE or K_lam|K_mu (576 or 1152)
+  double* d_Gtab_lame = nullptr;
+  double* d_Ktab_lame = nullptr;
+  bool have_fixed = false, have_material = false, lame = false;
+  std::vector<uint8_t> h_mask_ref;     // level-0 free bits, reference node order
+  uint8_t* d_active_ref = nullptr;     // per element (reference order)
+  std::vector<uint8_t> h_active;        // host copy (Jacobi default max_it)
+  uint8_t* d_active_pad = nullptr;
+  bool have_active = false;
+  uint8_t* d_allfree = nullptr;
+  // coarsest dense factor
+  double* d_Ainv = nullptr;
+  double* d_dense_work = nullptr;
+  int dense_n = 0;
+  int* d_info = nullptr;
+  // Krylov vectors on level 0: x, r, z, p, Ap
+  double* k64[5] = {};
+  float* k32[5] = {};
+  double* f64 = nullptr;      // padded masked rhs
+  double* r64 = nullptr;      // outer residual (mixed)
+  KrylovState* ks = nullptr;
+  KrylovState* h_ks = nullptr;   // pinned
+  double* d_partials = nullptr;
+  double* d_hist = nullptr;
+  int hist_cap = 0;
+  std::vector<double> history;
+  std::string err;
+  double* d_ref_a = nullptr;   // staging, reference layout (max(ndof, nelem) doubles)
+  double* d_ref_b = nullptr;
+  double* d_ref_c = nullptr;
+  uint8_t* d_ref_u8 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  cudaGraphExec_t chunk[3] = {nullptr, nullptr, nullptr};   // FP64 MG / FP32 MG / Jacobi
+  unsigned long long chunk_kernels[3] = {0, 0, 0};
+  std::vector<void*> allocs;
+  double last_setup_ms = 0.0;
+};
+
+namespace {
+
+#define VF_TRY(expr)                                                                  \
+  do {                                                                                \
+    cudaError_t _e = (expr);                                                          \
+    if (_e != cudaSuccess) {                                                          \
+      s->err = std::string(#expr) + ": " + cudaGetErrorString(_e);                    \
+      return (_e == cudaErrorMemoryAllocation) ? VF_ERR_NOMEM : VF_ERR_CUDA;          \
+    }                                                                                 \
+  } while (0)
+
+#define VF_CHECK_LAUNCH()                                                             \
+  do {                                                                                \
+    cudaError_t _e = cudaGetLastError();                                              \
+    if (_e != cudaSuccess) {                                                          \
+      s->err = std::string("kernel launch: ") + cudaGetErrorString(_e);               \
+      return VF_ERR_CUDA;                                                             \
+    }                                                                                 \
+  } while (0)
+
+template <typename T>
+int dalloc(vf_solver* s, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    s->err = std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) + " B): " + cudaGetErrorString(e);
+    return VF_ERR_NOMEM;
+  }
+  e = cudaMemset(q, 0, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) { s->err = cudaGetErrorString(e); return VF_ERR_CUDA; }
+  s->allocs.push_back(q);
+  *p = (T*)q;
+  return VF_OK;
+}
+
+#define VF_ALLOC(ptr, count)                              \
+  do {                                                    \
+    int _rc = dalloc(s, &(ptr), (size_t)(count));         \
+    if (_rc) return _rc;                                  \
+  } while (0)
+
+std::vector<std::array<int, 3>> level_dims(int nx, int ny, int nz, int min_elems, int max_levels) {
+  std::vector<std::array<int, 3>> d{{nx, ny, nz}};
+  while ((int)d.size() < max_levels && d.back()[0] % 2 == 0 && d.back()[1] % 2 == 0 && d.back()[2] % 2 == 0 &&
+         std::min({d.back()[0], d.back()[1], d.back()[2]}) / 2 >= min_elems / 2 &&
+         std::min({d.back()[0], d.back()[1], d.back()[2]}) >= 2) {
+    auto b = d.back();
+    d.push_back({b[0] / 2, b[1] / 2, b[2] / 2});
+  }
+  return d;
+}
+
+bool use_mg(const vf_solver* s) { return s->o.method == VF_METHOD_MG; }
+int nlev(const vf_solver* s) { return use_mg(s) ? (int)s->L.size() : 1; }
+
+// ---------------------------------------------------------------------------
+// operator dispatch on one level
+// ---------------------------------------------------------------------------
+template <typename T>
+void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, KrylovState* ks, double* partials,
+              int slot) {
+  Level& l = s->L[li];
+  OpArgs a{};
+  a.u = u; a.out = out; a.b = b;
+  a.minv = Sel<T>::minv(l);
+  a.E = Sel<T>::E(l);
+  a.mu = s->lame ? Sel<T>::mu(l) : nullptr;
+  a.mask = l.mask;
+  a.omega = s->o.omega;
+  a.dot_partials = partials;
+  a.ks = ks;
+  a.dot_slot = slot;
+  a.ke_tab = s->tab;
+  if (l.galerkin) launch_stencil_op<T>(l.g, epi, a, Sel<T>::st(l), s->st);
+  else launch_fine_op<T>(l.g, epi, a, s->st);
+}
+
+// `sweeps` damped-Jacobi sweeps on x (in place, through tmp); from_zero uses
+// the exact first sweep x = w*Minv*b.
+template <typename T>
+void smooth(vf_solver* s, int li, T* x, T* tmp, const T* b, int sweeps, bool from_zero, KrylovState* ks) {
+  Level& l = s->L[li];
+  if (sweeps <= 0) {
+    if (from_zero) cudaMemsetAsync(x, 0, sizeof(T) * 3 * (size_t)l.g.n, s->st);
+    return;
+  }
+  T* cur;
+  int rest;
+  if (from_zero) {
+    T* first = (sweeps % 2 == 1) ? x : tmp;
+    launch_jacobi_from_zero<T>(l.g, b, Sel<T>::minv(l), l.mask, s->o.omega, first, ks, s->st);
+    cur = first;
+    rest = sweeps - 1;
+  } else {
+    cur = x;
+    rest = sweeps;
+  }
+  for (int k = 0; k < rest; ++k) {
+    T* nxt = (cur == x) ? tmp : x;
+    level_op<T>(s, li, EPI_SMOOTH, cur, nxt, b, ks, nullptr, 0);
+    cur = nxt;
+  }
+  if (cur != x) launch_copy_vec<T>(l.g, cur, x, ks, s->st);
+}
+
+template <typename T>
+void coarse_solve(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
+  Level& l = s->L[li];
+  if (s->o.coarsest == VF_COARSEST_CHOLESKY && s->d_Ainv) {
+    launch_dense_solve<T>(l.g, s->d_Ainv, s->dense_n, b, x, ks, s->st);
+  } else {
+    smooth<T>(s, li, x, Sel<T>::w(l, 1), b, s->o.coarse_sweeps, true, ks);
+  }
+}
+
+// x = V-cycle(b) on level li (core/multigrid.py:426-436).
+template <typename T>
+void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
+  Level& l = s->L[li];
+  if (li == (int)s->L.size() - 1) {
+    coarse_solve<T>(s, li, b, x, ks);
+    return;
+  }
+  Level& c = s->L[li + 1];
+  T* tmp = Sel<T>::w(l, 1);
+  T* res = Sel<T>::w(l, 2);
+  smooth<T>(s, li, x, tmp, b, s->o.n_smooth, true, ks);
+  level_op<T>(s, li, EPI_RESID, x, res, b, ks, nullptr, 0);
+  launch_restrict<T>(l.g, res, c.g, c.mask, Sel<T>::w(c, 3), ks, s->st);
+  vcycle<T>(s, li + 1, Sel<T>::w(c, 3), Sel<T>::w(c, 0), ks);
+  launch_prolong_add<T>(c.g, Sel<T>::w(c, 0), l.g, l.mask, x, ks, s->st);
+  smooth<T>(s, li, x, tmp, b, s->o.n_smooth, false, ks);
+}
+
+template <typename T> T** kvec(vf_solver* s);
+template <> double** kvec<double>(vf_solver* s) { return s->k64; }
+template <> float** kvec<float>(vf_solver* s) { return s->k32; }
+
+template <typename T>
+void precondition(vf_solver* s, const T* r, T* z, KrylovState* ks) {
+  if (use_mg(s)) vcycle<T>(s, 0, r, z, ks);
+  else launch_jacobi_precond<T>(s->L[0].g, r, Sel<T>::minv(s->L[0]), s->L[0].mask, z, ks, s->st);
+}
+
+// One PCG iteration (core/multigrid.py:497-546 / core/fea.py:548-580).
+template <typename T>
+void pcg_iteration(vf_solver* s) {
+  T** v = kvec<T>(s);
+  T *x = v[0], *r = v[1], *z = v[2], *p = v[3], *Ap = v[4];
+  const Grid& g = s->L[0].g;
+  // the fine operator (level 0), masked, fused with p.Ap -> alpha
+  level_op<T>(s, 0, EPI_APPLY, p, Ap, nullptr, s->ks, s->d_partials, SLOT_PAP);
+  launch_cg_update<T>(g, x, p, r, Ap, s->d_partials, s->ks, s->d_hist, s->st);
+  precondition<T>(s, r, z, s->ks);
+  launch_dot<T>(g, r, z, s->d_partials, s->ks, SLOT_RZ, s->st);
+  launch_p_update<T>(g, p, z, s->ks, s->st);
+}
+
+int graph_slot(const vf_solver* s, bool fp32) { return use_mg(s) ? (fp32 ? 1 : 0) : 2; }
+
+// Run PCG chunks until the device says done.  Host callbacks see each new
+// history entry.
+template <typename T>
+int run_chunks(vf_solver* s, void (*progress)(int, double, double, void*), void* user, double tol) {
+  const int K = std::max(1, s->o.check_every);
+  const int gslot = graph_slot(s, sizeof(T) == 4);
+  if (s->o.use_graphs && !s->chunk[gslot]) {
+    cudaGraph_t graph = nullptr;
+    VF_TRY(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < K; ++k) pcg_iteration<T>(s);
+    cudaError_t e = cudaStreamEndCapture(s->st, &graph);
+    if (e != cudaSuccess) { s->err = std::string("graph capture: ") + cudaGetErrorString(e); return VF_ERR_CUDA; }
+    e = cudaGraphInstantiate(&s->chunk[gslot], graph, 0);
+    s->chunk_kernels[gslot] = graph_kernel_nodes(graph);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { s->err = std::string("graph instantiate: ") + cudaGetErrorString(e); return VF_ERR_CUDA; }
+  }
+  int seen = s->h_ks->it;
+  // Host-side bound: the device stops at max_it by itself; if the state
+  // ever fails to advance, report an error instead of polling forever.
+  const long long max_chunks = (long long)(s->h_ks->max_it + K - 1) / K + 4;
+  long long chunks = 0;
+  for (;;) {
+    if (++chunks > max_chunks) {
+      s->err = "PCG state did not reach max_it/convergence within the expected number of chunks";
+      return VF_ERR_CUDA;
+    }
+    if (s->o.use_graphs) {
+      VF_TRY(cudaGraphLaunch(s->chunk[gslot], s->st));
+      g_launches += s->chunk_kernels[gslot];
+    } else {
+      for (int k = 0; k < K; ++k) pcg_iteration<T>(s);
+      VF_CHECK_LAUNCH();
+    }
+    VF_TRY(cudaMemcpyAsync(s->h_ks, s->ks, sizeof(KrylovState), cudaMemcpyDeviceToHost, s->st));
+    VF_TRY(cudaStreamSynchronize(s->st));
+    const int it = s->h_ks->it;
+    if (it > seen) {
+      const int base = s->h_ks->it_base;
+      const size_t old = s->history.size();
+      s->history.resize(base + it);
+      VF_TRY(cudaMemcpy(s->history.data() + base + seen, s->d_hist + base + seen, sizeof(double) * (it - seen),
+                        cudaMemcpyDeviceToHost));
+      (void)old;
+      if (progress)
+        for (int k = seen; k < it; ++k) progress(base + k + 1, s->history[base + k], tol, user);
+      seen = it;
+    }
+    if (s->h_ks->done) break;
+  }
+  return VF_OK;
+}
+
+void init_ks(KrylovState& h, double tol, int max_it, int stall_guard, int it_base, double hist_scale) {
+  memset(&h, 0, sizeof(h));
+  h.tol = tol;
+  h.max_it = max_it;
+  h.stall_guard = stall_guard;
+  h.it_base = it_base;
+  h.hist_scale = hist_scale;
+  h.best = std::numeric_limits<double>::infinity();
+  h.resid = std::numeric_limits<double>::quiet_NaN();
+  h.fnorm = 1.0;
+}
+
+int ensure_hist(vf_solver* s, int need) {
+  if (need <= s->hist_cap) return VF_OK;
+  int cap = std::max(need, 2 * s->hist_cap);
+  double* nh = nullptr;
+  VF_ALLOC(nh, cap);
+  s->d_hist = nh;   // old buffer stays in allocs until destroy
+  s->hist_cap = cap;
+  // captured graphs hold the old pointer
+  for (auto& gexe : s->chunk)
+    if (gexe) { cudaGraphExecDestroy(gexe); gexe = nullptr; }
+  return VF_OK;
+}
+
+// Inner PCG on the already-prepared r (level-0 vectors of precision T), x = 0.
+template <typename T>
+int pcg_solve(vf_solver* s, double tol, int max_it, int stall_guard, int it_base, double hist_scale, double fnorm,
+              void (*progress)(int, double, double, void*), void* user, double tol_report) {
+  T** v = kvec<T>(s);
+  const Grid& g = s->L[0].g;
+  init_ks(*s->h_ks, tol, max_it, stall_guard, it_base, hist_scale);
+  s->h_ks->fnorm = fnorm;
+  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  precondition<T>(s, v[1], v[2], nullptr);
+  launch_dot<T>(g, v[1], v[2], s->d_partials, s->ks, SLOT_RZ_INIT, s->st);
+  launch_copy_vec<T>(g, v[2], v[3], nullptr, s->st);
+  VF_CHECK_LAUNCH();
+  if (max_it <= 0) return VF_OK;
+  return run_chunks<T>(s, progress, user, tol_report);
+}
+
+int map_status(int ks) {
+  switch (ks) {
+    case KS_STALLED: return VF_ERR_STALLED;
+    case KS_NONFINITE: return VF_ERR_NONFINITE;
+    default: return VF_OK;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// set-up
+// ---------------------------------------------------------------------------
+int build_levels(vf_solver* s) {
+  auto dims = level_dims(s->nx, s->ny, s->nz, s->o.min_elems, s->o.max_levels);
+  if (s->o.method != VF_METHOD_MG) dims.resize(1);
+  s->L.resize(dims.size());
+  for (size_t i = 0; i < dims.size(); ++i) {
+    Level& l = s->L[i];
+    l.g = make_grid(dims[i][0], dims[i][1], dims[i][2]);
+    if ((long long)l.g.px * l.g.py * l.g.pz * 3 >= (1LL << 31)) {
+      s->err = "grid too large for 32-bit indexing";
+      return VF_ERR_ARG;
+    }
+    l.galerkin = (i > 0 && s->o.coarse_op == VF_COARSE_GALERKIN);
+    const size_t n = l.g.n;
+    VF_ALLOC(l.mask, n);
+    VF_ALLOC(l.minv64, 3 * n);
+    VF_ALLOC(l.minv32, 3 * n);
+    if (!l.galerkin) {
+      VF_ALLOC(l.E64, n);
+      VF_ALLOC(l.E32, n);
+    } else {
+      VF_ALLOC(l.st64, 243 * n);
+      VF_ALLOC(l.st32, 243 * n);
+    }
+    for (int k = 0; k < 4; ++k) {
+      VF_ALLOC(l.w64[k], 3 * n);
+      VF_ALLOC(l.w32[k], 3 * n);
+    }
+  }
+  const Grid& g0 = s->L[0].g;
+  for (int k = 0; k < 5; ++k) {
+    VF_ALLOC(s->k64[k], 3 * (size_t)g0.n);
+    VF_ALLOC(s->k32[k], 3 * (size_t)g0.n);
+  }
+  VF_ALLOC(s->f64, 3 * (size_t)g0.n);
+  VF_ALLOC(s->r64, 3 * (size_t)g0.n);
+  const size_t nref = std::max<size_t>(3 * (size_t)g0.nodes_ref(), (size_t)g0.elems_ref());
+  VF_ALLOC(s->d_ref_a, nref);
+  VF_ALLOC(s->d_ref_b, nref);
+  VF_ALLOC(s->d_ref_c, nref);
+  VF_ALLOC(s->d_ref_u8, nref);
+  VF_ALLOC(s->d_active_ref, (size_t)g0.elems_ref());
+  VF_ALLOC(s->d_active_pad, (size_t)g0.n);
+  VF_ALLOC(s->d_allfree, (size_t)g0.n);
+  VF_ALLOC(s->ks, 1);
+  VF_ALLOC(s->d_partials, 148 * 64);
+  VF_ALLOC(s->d_info, 1);
+  VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
+  memset(s->h_ks, 0, sizeof(KrylovState));
+  return ensure_hist(s, 4096);
+}
+
+int upload_tables(vf_solver* s) {
+  hex8_tables(s->nu, s->tab, s->B0);
+  std::vector<double> G(8 * 576), GL(16 * 576);
+  galerkin_child_tables(s->tab, G.data());
+  galerkin_child_tables(s->tab + 576, GL.data());
+  galerkin_child_tables(s->tab + 1152, GL.data() + 8 * 576);
+  VF_ALLOC(s->d_Gtab, 8 * 576);
+  VF_ALLOC(s->d_Ktab, 576);
+  VF_ALLOC(s->d_Gtab_lame, 16 * 576);
+  VF_ALLOC(s->d_Ktab_lame, 1152);
+  VF_TRY(cudaMemcpy(s->d_Gtab, G.data(), sizeof(double) * 8 * 576, cudaMemcpyHostToDevice));
+  VF_TRY(cudaMemcpy(s->d_Ktab, s->tab, sizeof(double) * 576, cudaMemcpyHostToDevice));
+  VF_TRY(cudaMemcpy(s->d_Gtab_lame, GL.data(), sizeof(double) * 16 * 576, cudaMemcpyHostToDevice));
+  VF_TRY(cudaMemcpy(s->d_Ktab_lame, s->tab + 576, sizeof(double) * 1152, cudaMemcpyHostToDevice));
+  return VF_OK;
+}
+
+// Level masks: level 0 from the fixed DOFs (and the used-node restriction of
+// the Jacobi method); rediscretized levels by injection.
+int build_masks(vf_solver* s) {
+  Level& l0 = s->L[0];
+  const int nref = l0.g.nodes_ref();
+  VF_TRY(cudaMemcpyAsync(s->d_ref_u8, s->h_mask_ref.data(), nref, cudaMemcpyHostToDevice, s->st));
+  launch_pack_mask(l0.g, s->d_ref_u8, l0.mask, s->st);
+  if (!use_mg(s) && s->have_active) launch_used_mask(l0.g, s->d_active_pad, l0.mask, s->st);
+  for (size_t i = 1; i < s->L.size(); ++i)
+    if (!s->L[i].galerkin) launch_inject_mask(s->L[i - 1].g, s->L[i - 1].mask, s->L[i].g, s->L[i].mask, s->st);
+  VF_CHECK_LAUNCH();
+  return VF_OK;
+}
+
+int build_dense_coarsest(vf_solver* s) {
+  Level& lc = s->L.back();
+  const int n = 3 * lc.g.nodes_ref();
+  if (n > 16384) {
+    s->err = "coarsest level has " + std::to_string(n) + " DOFs; the dense coarsest solve supports <= 16384 "
+             "(use more levels or VF_COARSEST_JACOBI)";
+    return VF_ERR_UNSUPPORTED;
+  }
+  if (s->dense_n != n) {
+    VF_ALLOC(s->d_Ainv, (size_t)n * n);
+    VF_ALLOC(s->d_dense_work, (size_t)n * n);
+    s->dense_n = n;
+    dense_prepare_smem(n);
+  }
+  double* st = lc.st64;
+  if (!lc.galerkin) {
+    // stencil of the rediscretized element operator on the coarsest level
+    if (!lc.st64) VF_ALLOC(lc.st64, 243 * (size_t)lc.g.n);
+    st = lc.st64;
+    launch_stencil_from_elements(lc.g, lc.E64, s->lame ? lc.mu64 : nullptr, lc.mask, st,
+                                 s->lame ? s->d_Ktab_lame : s->d_Ktab, s->lame ? 1 : 0, s->st);
+  }
+  dense_assemble(lc.g, st, lc.mask, s->d_Ainv, n, s->st);
+  dense_cholesky_inverse(s->d_Ainv, s->d_dense_work, n, s->d_info, s->st);
+  VF_CHECK_LAUNCH();
+  int info = 0;
+  VF_TRY(cudaMemcpyAsync(&info, s->d_info, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  if (info != 0) {
+    s->err = "coarsest-level Cholesky: non-positive pivot at row " + std::to_string(info - 1) +
+             " (singular coarse operator: is the part supported?)";
+    return VF_ERR_BREAKDOWN;
+  }
+  return VF_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+extern "C" {
+
+int vf_abi_version(void) { return VF_ABI_VERSION; }
+
+int vf_get_stream(const vf_solver* s, void** stream) {
+  if (!s || !stream) return VF_ERR_ARG;
+  *stream = (void*)s->st;
+  return VF_OK;
+}
+
+int vf_launch_count(uint64_t* count) {
+  if (!count) return VF_ERR_ARG;
+  *count = (uint64_t)(g_launches.load() + vf::direct_launches());
+  return VF_OK;
+}
+
+const char* vf_status_string(int status) {
+  switch (status) {
+    case VF_OK: return "ok";
+    case VF_ERR_ARG: return "invalid argument";
+    case VF_ERR_STATE: return "invalid call order";
+    case VF_ERR_CUDA: return "CUDA error";
+    case VF_ERR_NOMEM: return "out of device memory";
+    case VF_ERR_NO_DEVICE: return "no usable CUDA device";
+    case VF_ERR_STALLED: return "MG-PCG stalled/diverged";
+    case VF_ERR_NONFINITE: return "non-finite value";
+    case VF_ERR_UNSUPPORTED: return "unsupported option";
+    case VF_ERR_BREAKDOWN: return "breakdown";
+    default: return "unknown status";
+  }
+}
+
+const char* vf_global_last_error(void) { return g_last_error.c_str(); }
+
+int vf_hex8_tables(double nu, double* KE, double* KL, double* KM, double* B0) {
+  if (!(nu > -1.0 && nu < 0.5)) { g_last_error = "Poisson ratio must lie in (-1, 0.5)"; return VF_ERR_ARG; }
+  double tab[1728], b0[144];
+  hex8_tables(nu, tab, b0);
+  if (KE) memcpy(KE, tab, sizeof(double) * 576);
+  if (KL) memcpy(KL, tab + 576, sizeof(double) * 576);
+  if (KM) memcpy(KM, tab + 1152, sizeof(double) * 576);
+  if (B0) memcpy(B0, b0, sizeof(double) * 144);
+  return VF_OK;
+}
+
+int vf_device_count(int32_t* count) {
+  if (!count) return VF_ERR_ARG;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) { *count = 0; g_last_error = cudaGetErrorString(e); return VF_ERR_NO_DEVICE; }
+  *count = n;
+  return VF_OK;
+}
+
+void vf_options_default(vf_options* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->struct_size = (int32_t)sizeof(vf_options);
+  o->method = VF_METHOD_MG;
+  o->precision = VF_PREC_FP64;
+  o->n_smooth = 2;
+  o->min_elems = 4;
+  o->max_levels = 6;
+  o->coarse_op = VF_COARSE_REDISCRETIZE;
+  o->coarsest = VF_COARSEST_JACOBI;
+  o->coarse_sweeps = 30;
+  o->stall_guard = 1;
+  o->check_every = 8;
+  o->use_graphs = 1;
+  o->device = 0;
+  o->max_outer = 20;
+  o->omega = 0.6;
+  o->inner_tol = 1e-4;
+}
+
+int vf_destroy(vf_solver* s) {
+  if (!s) return VF_OK;
+  cudaSetDevice(s->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  for (auto& gexe : s->chunk)
+    if (gexe) cudaGraphExecDestroy(gexe);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->h_ks) cudaFreeHost(s->h_ks);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->ev2) cudaEventDestroy(s->ev2);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+  return VF_OK;
+}
+
+int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* opts, vf_solver** out) {
+  if (!out) { g_last_error = "out is NULL"; return VF_ERR_ARG; }
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1) { g_last_error = "grid dimensions must be >= 1"; return VF_ERR_ARG; }
+  if (!(nu > -1.0 && nu < 0.5)) { g_last_error = "Poisson ratio must lie in (-1, 0.5)"; return VF_ERR_ARG; }
+  vf_options o;
+  vf_options_default(&o);
+  if (opts) {
+    if (opts->struct_size != (int32_t)sizeof(vf_options)) { g_last_error = "vf_options.struct_size mismatch"; return VF_ERR_ARG; }
+    o = *opts;
+  }
+  if (o.precision < 0 || o.precision > 2 || o.method < 0 || o.method > 1 || o.coarse_op < 0 || o.coarse_op > 1 ||
+      o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0) {
+    g_last_error = "invalid vf_options field";
+    return VF_ERR_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) { g_last_error = "no CUDA device"; return VF_ERR_NO_DEVICE; }
+  if (o.device < 0 || o.device >= ndev) { g_last_error = "device ordinal out of range"; return VF_ERR_ARG; }
+  vf_solver* s = new vf_solver();
+  s->o = o;
+  s->nu = nu;
+  s->nx = nx; s->ny = ny; s->nz = nz;
+  s->device = o.device;
+  int rc = VF_OK;
+  auto fail = [&](int code) {
+    g_last_error = s->err;
+    vf_destroy(s);
+    return code;
+  };
+  if (cudaSetDevice(s->device) != cudaSuccess) { s->err = "cudaSetDevice failed"; return fail(VF_ERR_CUDA); }
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) { s->err = "stream"; return fail(VF_ERR_CUDA); }
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  cudaEventCreate(&s->ev2);
+  if ((rc = build_levels(s))) return fail(rc);
+  if ((rc = upload_tables(s))) return fail(rc);
+  s->h_mask_ref.assign((size_t)s->L[0].g.nodes_ref(), kFreeAll);
+  *out = s;
+  return VF_OK;
+}
+
+const char* vf_last_error(const vf_solver* s) { return s ? s->err.c_str() : g_last_error.c_str(); }
+
+int vf_num_levels(const vf_solver* s, int32_t* n) {
+  if (!s || !n) return VF_ERR_ARG;
+  *n = (int32_t)s->L.size();
+  return VF_OK;
+}
+
+int vf_level_dims(const vf_solver* s, int32_t level, int32_t* dims3) {
+  if (!s || !dims3 || level < 0 || level >= (int)s->L.size()) return VF_ERR_ARG;
+  dims3[0] = s->L[level].g.lx; dims3[1] = s->L[level].g.ly; dims3[2] = s->L[level].g.lz;
+  return VF_OK;
+}
+
+int vf_set_fixed(vf_solver* s, const int64_t* fixed, int64_t n) {
+  if (!s || (n > 0 && !fixed) || n < 0) return VF_ERR_ARG;
+  cudaSetDevice(s->device);
+  const long long ndof = 3LL * s->L[0].g.nodes_ref();
+  std::fill(s->h_mask_ref.begin(), s->h_mask_ref.end(), kFreeAll);
+  for (int64_t i = 0; i < n; ++i) {
+    const long long d = fixed[i];
+    if (d < 0 || d >= ndof) {
+      s->err = "fixed DOF " + std::to_string(d) + " out of range [0, " + std::to_string(ndof) + ")";
+      return VF_ERR_ARG;
+    }
+    s->h_mask_ref[d / 3] &= (uint8_t)~(1u << (d % 3));
+  }
+  s->have_fixed = true;
+  s->have_material = false;   // masks feed the coarse operators
+  return build_masks(s);
+}
+
+int vf_set_active(vf_solver* s, const uint8_t* active) {
+  if (!s) return VF_ERR_ARG;
+  cudaSetDevice(s->device);
+  const Grid& g0 = s->L[0].g;
+  if (active) {
+    s->h_active.assign(active, active + (size_t)g0.elems_ref());
+    VF_TRY(cudaMemcpyAsync(s->d_active_ref, s->h_active.data(), (size_t)g0.elems_ref(), cudaMemcpyHostToDevice, s->st));
+    launch_pack_active(g0, s->d_active_ref, s->d_active_pad, s->st);
+    s->have_active = true;
+  } else {
+    launch_pack_active(g0, nullptr, s->d_active_pad, s->st);
+    s->have_active = false;
+  }
+  VF_CHECK_LAUNCH();
+  s->have_material = false;
+  return s->have_fixed ? build_masks(s) : VF_OK;
+}
+
+int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32_t flags) {
+  if (!s || !E) return VF_ERR_ARG;
+  const cudaMemcpyKind kind = (flags & VF_SOLVE_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (!s->have_fixed) { s->err = "call set_fixed() before solve()"; return VF_ERR_STATE; }
+  cudaSetDevice(s->device);
+  VF_TRY(cudaEventRecord(s->ev0, s->st));
+  const Grid& g0 = s->L[0].g;
+  const size_t ne = (size_t)g0.elems_ref();
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, E, sizeof(double) * ne, kind, s->st));
+  const bool lame = nu_elem != nullptr;
+  if (lame) VF_TRY(cudaMemcpyAsync(s->d_ref_b, nu_elem, sizeof(double) * ne, kind, s->st));
+  if (lame != s->lame) {
+    // per-voxel mu arrays on the element-operator levels
+    for (auto& l : s->L)
+      if (!l.galerkin && !l.mu64) {
+        VF_ALLOC(l.mu64, l.g.n);
+        VF_ALLOC(l.mu32, l.g.n);
+      }
+    for (auto& gexe : s->chunk)
+      if (gexe) { cudaGraphExecDestroy(gexe); gexe = nullptr; }
+    s->lame = lame;
+  }
+  const uint8_t* act = (!use_mg(s) && s->have_active) ? s->d_active_ref : nullptr;
+  Level& l0 = s->L[0];
+  if (lame) launch_pack_lame<double>(g0, s->d_ref_a, s->d_ref_b, s->nu, act, 1.0, l0.E64, l0.mu64, s->st);
+  else launch_pack_elem<double>(g0, s->d_ref_a, l0.E64, act, 1.0, s->st);
+  const double dL = lame ? s->tab[576] : s->tab[0];
+  const double dM = lame ? s->tab[1152] : 0.0;
+  launch_inv_diag_fine<double>(g0, l0.E64, lame ? l0.mu64 : nullptr, dL, dM, l0.minv64, s->st);
+  if (use_mg(s)) {
+    for (size_t i = 1; i < s->L.size(); ++i) {
+      Level& f = s->L[i - 1];
+      Level& c = s->L[i];
+      if (!c.galerkin) {
+        launch_coarsen_E<double>(f.g, f.E64, c.g, c.E64, s->st);
+        if (lame) launch_coarsen_E<double>(f.g, f.mu64, c.g, c.mu64, s->st);
+        launch_inv_diag_fine<double>(c.g, c.E64, lame ? c.mu64 : nullptr, dL, dM, c.minv64, s->st);
+      } else if (i == 1) {
+        launch_elem_allfree(f.g, f.mask, s->d_allfree, s->st);
+        launch_galerkin_from_fine(f.g, f.E64, lame ? f.mu64 : nullptr, f.mask, s->d_allfree, c.g, c.st64,
+                                  lame ? s->d_Gtab_lame : s->d_Gtab, lame ? s->d_Ktab_lame : s->d_Ktab,
+                                  lame ? 1 : 0, s->st);
+        launch_galerkin_mask(c.g, c.st64, c.mask, c.minv64, s->st);
+      } else {
+        launch_galerkin_from_stencil(f.g, f.st64, c.g, c.st64, s->st);
+        launch_galerkin_mask(c.g, c.st64, c.mask, c.minv64, s->st);
+      }
+    }
+  }
+  // FP32 copies
+  for (size_t i = 0; i < (size_t)nlev(s); ++i) {
+    Level& l = s->L[i];
+    const long long n = l.g.n;
+    if (!l.galerkin) {
+      launch_convert<double, float>(l.E64, l.E32, n, s->st);
+      if (lame) launch_convert<double, float>(l.mu64, l.mu32, n, s->st);
+    } else {
+      launch_convert<double, float>(l.st64, l.st32, 243 * n, s->st);
+    }
+    launch_convert<double, float>(l.minv64, l.minv32, 3 * n, s->st);
+  }
+  VF_CHECK_LAUNCH();
+  if (use_mg(s) && s->o.coarsest == VF_COARSEST_CHOLESKY) {
+    int rc = build_dense_coarsest(s);
+    if (rc) return rc;
+  }
+  VF_TRY(cudaEventRecord(s->ev1, s->st));
+  VF_TRY(cudaEventSynchronize(s->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  s->last_setup_ms = ms;
+  s->have_material = true;
+  return VF_OK;
+}
+
+int vf_solve(vf_solver* s, const double* f, const double* x0, double tol, int32_t max_it, uint32_t flags,
+             double* u_out, vf_solve_info* info) {
+  return vf_solve_cb(s, f, x0, tol, max_it, flags, u_out, info, nullptr, nullptr);
+}
+
+}  // extern "C"
+
+extern "C" int vf_solve_cb(vf_solver* s, const double* f, const double* x0, double tol, int32_t max_it,
+                           uint32_t flags, double* u_out, vf_solve_info* info,
+                           vf_progress_fn progress, void* user) {
+  if (!s || !f || !u_out) return VF_ERR_ARG;
+  if (!s->have_fixed) { s->err = "call set_fixed() before solve()"; return VF_ERR_STATE; }
+  if (!s->have_material) { s->err = "call set_material() before solve()"; return VF_ERR_STATE; }
+  if (!(tol > 0.0)) { s->err = "tol must be > 0"; return VF_ERR_ARG; }
+  cudaSetDevice(s->device);
+  const bool dev = (flags & VF_SOLVE_DEVICE_PTRS) != 0;
+  Level& l0 = s->L[0];
+  const Grid& g = l0.g;
+  const size_t nref = 3 * (size_t)g.nodes_ref();
+  const cudaMemcpyKind h2d = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  VF_TRY(cudaEventRecord(s->ev0, s->st));
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, f, sizeof(double) * nref, h2d, s->st));
+  launch_pack_vec<double>(g, s->d_ref_a, s->f64, l0.mask, s->st);   // f = where(free, f, 0)
+  if (x0) {
+    VF_TRY(cudaMemcpyAsync(s->d_ref_b, x0, sizeof(double) * nref, h2d, s->st));
+  }
+  VF_CHECK_LAUNCH();
+  s->history.clear();
+  int n_free = 0;
+  if (max_it <= 0) {
+    if (use_mg(s)) max_it = 1000;   // multigrid.py:481
+    else {
+      // fea.py:546: 4 x the free DOFs of the active-restricted system
+      const int nx1 = s->nx + 1, ny1 = s->ny + 1;
+      std::vector<uint8_t> used(s->h_mask_ref.size(), s->have_active ? 0 : 1);
+      if (s->have_active)
+        for (int ix = 0; ix < s->nx; ++ix)
+          for (int iy = 0; iy < s->ny; ++iy)
+            for (int iz = 0; iz < s->nz; ++iz) {
+              if (!s->h_active[((size_t)ix * s->ny + iy) * s->nz + iz]) continue;
+              for (int k = 0; k < 8; ++k)
+                used[(ix + kCorner[k][0]) + (size_t)nx1 * ((iy + kCorner[k][1]) + (size_t)ny1 * (iz + kCorner[k][2]))] = 1;
+            }
+      for (size_t i = 0; i < s->h_mask_ref.size(); ++i)
+        if (used[i]) n_free += __builtin_popcount(s->h_mask_ref[i]);
+      max_it = std::max(1, 4 * n_free);
+    }
+  }
+  {
+    int rc = ensure_hist(s, max_it + 8);
+    if (rc) return rc;
+  }
+  const bool mixed = s->o.precision == VF_PREC_MIXED;
+  const bool fp32 = s->o.precision == VF_PREC_FP32;
+  // fnorm = ||mask f|| (multigrid.py:471)
+  init_ks(*s->h_ks, tol, max_it, s->o.stall_guard, 0, 1.0);
+  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  launch_norm2_f64(g, s->f64, s->d_partials, s->ks, SLOT_FNORM, s->st);
+  VF_TRY(cudaMemcpyAsync(s->h_ks, s->ks, sizeof(KrylovState), cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  const double fnorm = s->h_ks->fnorm;
+  vf_solve_info inf{};
+  inf.resid_ratio = std::numeric_limits<double>::quiet_NaN();
+  int status = VF_OK;
+  double* x64 = s->k64[0];
+  if (fnorm == 0.0) {
+    // multigrid.py:472-473 / fea.py:543-545: zero load -> zero displacement
+    cudaMemsetAsync(x64, 0, sizeof(double) * 3 * (size_t)g.n, s->st);
+    inf.converged = use_mg(s) ? 0 : 1;
+    inf.iters = -1;
+  } else if (!mixed && !fp32) {
+    // ---- FP64 PCG (reference algorithm) ----
+    double** v = s->k64;
+    if (x0) {
+      launch_pack_vec<double>(g, s->d_ref_b, v[0], l0.mask, s->st);   // u = where(free, x0, 0)
+      level_op<double>(s, 0, EPI_APPLY, v[0], v[1], nullptr, nullptr, nullptr, 0);
+      launch_sub_from(g, s->f64, v[1], s->st);                           // r = f - A u
+    } else {
+      cudaMemsetAsync(v[0], 0, sizeof(double) * 3 * (size_t)g.n, s->st);
+      launch_copy_vec<double>(g, s->f64, v[1], nullptr, s->st);
+    }
+    VF_CHECK_LAUNCH();
+    int rc = pcg_solve<double>(s, tol, max_it, use_mg(s) ? s->o.stall_guard : 0, 0, 1.0, fnorm, progress, user, tol);
+    if (rc) return rc;
+    inf.iters = s->h_ks->it;
+    inf.converged = s->h_ks->status == KS_CONVERGED;
+    inf.resid_ratio = s->h_ks->it > 0 ? s->h_ks->resid : std::numeric_limits<double>::quiet_NaN();
+    status = map_status(s->h_ks->status);
+  } else if (fp32) {
+    // ---- FP32 vectors/operators, FP64 dots, no refinement ----
+    float** v = s->k32;
+    launch_convert<double, float>(s->f64, v[1], 3LL * g.n, s->st);
+    cudaMemsetAsync(v[0], 0, sizeof(float) * 3 * (size_t)g.n, s->st);
+    if (x0) {
+      launch_pack_vec<double>(g, s->d_ref_b, s->r64, l0.mask, s->st);
+      launch_convert<double, float>(s->r64, v[0], 3LL * g.n, s->st);
+      level_op<float>(s, 0, EPI_RESID, v[0], v[2], v[1], nullptr, nullptr, 0);
+      launch_copy_vec<float>(g, v[2], v[1], nullptr, s->st);
+    }
+    VF_CHECK_LAUNCH();
+    int rc = pcg_solve<float>(s, tol, max_it, use_mg(s) ? s->o.stall_guard : 0, 0, 1.0, fnorm, progress, user, tol);
+    if (rc) return rc;
+    launch_convert<float, double>(v[0], x64, 3LL * g.n, s->st);
+    inf.iters = s->h_ks->it;
+    inf.converged = s->h_ks->status == KS_CONVERGED;
+    inf.resid_ratio = s->h_ks->it > 0 ? s->h_ks->resid : std::numeric_limits<double>::quiet_NaN();
+    status = map_status(s->h_ks->status);
+  } else {
+    // ---- mixed precision iterative refinement ----
+    if (x0) launch_pack_vec<double>(g, s->d_ref_b, x64, l0.mask, s->st);
+    else cudaMemsetAsync(x64, 0, sizeof(double) * 3 * (size_t)g.n, s->st);
+    int total = 0, outer = 0;
+    double resid = 0.0;
+    for (;;) {
+      // r64 = f - A64 x64 (true residual in FP64)
+      level_op<double>(s, 0, EPI_APPLY, x64, s->r64, nullptr, nullptr, nullptr, 0);
+      launch_sub_from(g, s->f64, s->r64, s->st);
+      init_ks(*s->h_ks, tol, max_it, 0, total, 1.0);
+      s->h_ks->fnorm = fnorm;
+      VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+      launch_norm2_f64(g, s->r64, s->d_partials, s->ks, SLOT_OUTER, s->st);
+      VF_CHECK_LAUNCH();
+      VF_TRY(cudaMemcpyAsync(s->h_ks, s->ks, sizeof(KrylovState), cudaMemcpyDeviceToHost, s->st));
+      VF_TRY(cudaStreamSynchronize(s->st));
+      resid = s->h_ks->resid;
+      if (!(resid == resid)) { status = VF_ERR_NONFINITE; break; }
+      if (resid < tol) { inf.converged = 1; break; }
+      if (outer >= s->o.max_outer || total >= max_it) break;
+      // inner FP32 solve of A d = r64 / ||r64||
+      launch_ir_prepare(g, s->r64, s->k32[1], s->ks, s->st);
+      cudaMemsetAsync(s->k32[0], 0, sizeof(float) * 3 * (size_t)g.n, s->st);
+      const double itol = std::max(s->o.inner_tol, 0.5 * tol / resid);
+      const double scale = std::sqrt(s->h_ks->rr);
+      int rc = pcg_solve<float>(s, itol, max_it - total, 0, total, scale / fnorm, 1.0, progress, user, tol);
+      if (rc) return rc;
+      const int it = s->h_ks->it;
+      const int kst = s->h_ks->status;
+      // ks->scale was set by ir_prepare before pcg_solve reset the state: restore it
+      s->h_ks->scale = scale;
+      VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+      launch_ir_accumulate(g, x64, s->k32[0], s->ks, s->st);
+      VF_CHECK_LAUNCH();
+      total += it;
+      ++outer;
+      if (kst == KS_NONFINITE) { status = VF_ERR_NONFINITE; break; }
+      if (it == 0) break;
+    }
+    inf.iters = total;
+    inf.outer_iters = outer;
+    inf.resid_ratio = resid;
+    s->history.resize(total);
+  }
+  // u = where(free, u, 0) and the FP64 true residual
+  level_op<double>(s, 0, EPI_APPLY, x64, s->r64, nullptr, nullptr, nullptr, 0);
+  launch_sub_from(g, s->f64, s->r64, s->st);
+  init_ks(*s->h_ks, tol, 0, 0, 0, 1.0);
+  s->h_ks->fnorm = fnorm > 0.0 ? fnorm : 1.0;
+  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  launch_norm2_f64(g, s->r64, s->d_partials, s->ks, SLOT_OUTER, s->st);
+  launch_unpack_vec<double>(g, x64, s->d_ref_c, s->st);
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaMemcpyAsync(u_out, s->d_ref_c, sizeof(double) * nref, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                         s->st));
+  VF_TRY(cudaMemcpyAsync(s->h_ks, s->ks, sizeof(KrylovState), cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaEventRecord(s->ev1, s->st));
+  VF_TRY(cudaEventSynchronize(s->ev1));
+  inf.true_resid = fnorm > 0.0 ? s->h_ks->resid : 0.0;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  inf.device_ms = ms;
+  inf.setup_ms = s->last_setup_ms;
+  inf.status = status;
+  if (info) *info = inf;
+  if (status == VF_ERR_STALLED) {
+    char buf[256];
+    snprintf(buf, sizeof(buf),
+             "MG-PCG stalled/diverged at iter %d (resid ratio %.3e, best seen %.3e) -- likely a small/thin "
+             "essential-BC patch the coarse grid can't represent well",
+             inf.iters, inf.resid_ratio, s->h_ks->best);
+    s->err = buf;
+  }
+  return status;
+}
+
+extern "C" {
+
+int vf_resid_history(const vf_solver* s, double* out, int32_t cap, int32_t* n_out) {
+  if (!s || !n_out) return VF_ERR_ARG;
+  const int n = (int)s->history.size();
+  *n_out = n;
+  if (out) memcpy(out, s->history.data(), sizeof(double) * std::min(n, (int)cap));
+  return VF_OK;
+}
+
+int vf_von_mises(vf_solver* s, const double* u, const double* E_stress, const double* nu_elem,
+                 const uint8_t* active, double* vm_out) {
+  if (!s || !u || !E_stress || !vm_out) return VF_ERR_ARG;
+  cudaSetDevice(s->device);
+  const Grid& g = s->L[0].g;
+  const size_t nref = 3 * (size_t)g.nodes_ref(), ne = (size_t)g.elems_ref();
+  double* upad = s->k64[4];
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, u, sizeof(double) * nref, cudaMemcpyHostToDevice, s->st));
+  launch_pack_vec<double>(g, s->d_ref_a, upad, nullptr, s->st);
+  VF_TRY(cudaMemcpyAsync(s->d_ref_b, E_stress, sizeof(double) * ne, cudaMemcpyHostToDevice, s->st));
+  double* nud = nullptr;
+  if (nu_elem) {
+    VF_TRY(cudaMemcpyAsync(s->d_ref_c, nu_elem, sizeof(double) * ne, cudaMemcpyHostToDevice, s->st));
+    nud = s->d_ref_c;
+  }
+  uint8_t* act = nullptr;
+  if (active) {
+    VF_TRY(cudaMemcpyAsync(s->d_ref_u8, active, ne, cudaMemcpyHostToDevice, s->st));
+    act = s->d_ref_u8;
+  }
+  launch_von_mises(g, upad, s->d_ref_b, nud, s->nu, act, s->B0, s->d_ref_a, s->st);
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaMemcpyAsync(vm_out, s->d_ref_a, sizeof(double) * ne, cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  return VF_OK;
+}
+
+int vf_strain_energy(vf_solver* s, const double* u, const uint8_t* active, double* se_out) {
+  if (!s || !u || !se_out) return VF_ERR_ARG;
+  cudaSetDevice(s->device);
+  const Grid& g = s->L[0].g;
+  const size_t nref = 3 * (size_t)g.nodes_ref(), ne = (size_t)g.elems_ref();
+  double* upad = s->k64[4];
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, u, sizeof(double) * nref, cudaMemcpyHostToDevice, s->st));
+  launch_pack_vec<double>(g, s->d_ref_a, upad, nullptr, s->st);
+  uint8_t* act = nullptr;
+  if (active) {
+    VF_TRY(cudaMemcpyAsync(s->d_ref_u8, active, ne, cudaMemcpyHostToDevice, s->st));
+    act = s->d_ref_u8;
+  }
+  launch_strain_energy_tab(g, upad, act, s->tab, s->d_ref_b, s->st);
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaMemcpyAsync(se_out, s->d_ref_b, sizeof(double) * ne, cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  return VF_OK;
+}
+
+int vf_drop_unsupported_islands(int32_t nx, int32_t ny, int32_t nz, const uint8_t* active, const int64_t* fixed,
+                                int64_t n_fixed, uint8_t* kept_out, int64_t* n_removed) {
+  if (nx < 1 || ny < 1 || nz < 1 || !active || !kept_out || !n_removed || (n_fixed > 0 && !fixed)) {
+    g_last_error = "invalid argument";
+    return VF_ERR_ARG;
+  }
+  const size_t ne = (size_t)nx * ny * nz;
+  const size_t nn = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+  std::vector<uint8_t> fixed_node(nn, 0);
+  for (int64_t i = 0; i < n_fixed; ++i) {
+    if (fixed[i] < 0 || (size_t)fixed[i] >= 3 * nn) { g_last_error = "fixed DOF out of range"; return VF_ERR_ARG; }
+    fixed_node[fixed[i] / 3] = 1;
+  }
+  uint8_t *d_act = nullptr, *d_fix = nullptr, *d_kept = nullptr;
+  int* d_changed = nullptr;
+  cudaStream_t st = nullptr;
+  int rc = VF_OK;
+  auto cleanup = [&]() {
+    if (d_act) cudaFree(d_act);
+    if (d_fix) cudaFree(d_fix);
+    if (d_kept) cudaFree(d_kept);
+    if (d_changed) cudaFree(d_changed);
+    if (st) cudaStreamDestroy(st);
+  };
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess || cudaMalloc(&d_act, ne) != cudaSuccess ||
+      cudaMalloc(&d_fix, nn) != cudaSuccess || cudaMalloc(&d_kept, ne) != cudaSuccess ||
+      cudaMalloc(&d_changed, sizeof(int)) != cudaSuccess) {
+    g_last_error = "device allocation failed";
+    cleanup();
+    return VF_ERR_NOMEM;
+  }
+  std::vector<uint8_t> act01(ne);
+  long long n_active = 0;
+  for (size_t e = 0; e < ne; ++e) { act01[e] = active[e] ? 1 : 0; n_active += act01[e]; }
+  cudaMemcpyAsync(d_act, act01.data(), ne, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_fix, fixed_node.data(), nn, cudaMemcpyHostToDevice, st);
+  if (flood_fill_islands(nx, ny, nz, d_act, d_fix, d_kept, d_changed, st) < 0) rc = VF_ERR_CUDA;
+  std::vector<uint8_t> kept(ne);
+  if (!rc && cudaMemcpyAsync(kept.data(), d_kept, ne, cudaMemcpyDeviceToHost, st) != cudaSuccess) rc = VF_ERR_CUDA;
+  if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = VF_ERR_CUDA;
+  cleanup();
+  if (rc) { g_last_error = "CUDA error in flood fill"; return rc; }
+  long long n_kept = 0;
+  for (size_t e = 0; e < ne; ++e) n_kept += kept[e];
+  if (n_kept == 0) {   // fea.py:220-225: nothing reached -> unchanged
+    for (size_t e = 0; e < ne; ++e) kept_out[e] = act01[e];
+    *n_removed = 0;
+    return VF_OK;
+  }
+  for (size_t e = 0; e < ne; ++e) kept_out[e] = kept[e];
+  *n_removed = n_active - n_kept;
+  return VF_OK;
+}
+
+}  // extern "C"
+
+// ---- level operators ------------------------------------------------------
+
+static int level_check(vf_solver* s, int level, int precision) {
+  if (!s) return VF_ERR_ARG;
+  if (level < 0 || level >= nlev(s)) { s->err = "level out of range"; return VF_ERR_ARG; }
+  if (precision != VF_PREC_FP64 && precision != VF_PREC_FP32) { s->err = "precision must be FP64 or FP32"; return VF_ERR_ARG; }
+  if (!s->have_fixed || !s->have_material) { s->err = "call set_fixed() and set_material() first"; return VF_ERR_STATE; }
+  cudaSetDevice(s->device);
+  return VF_OK;
+}
+
+template <typename T>
+static int op_in(vf_solver* s, int level, const double* h, T* pad, const uint8_t* mask) {
+  const Grid& g = s->L[level].g;
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, h, sizeof(double) * 3 * (size_t)g.nodes_ref(), cudaMemcpyHostToDevice, s->st));
+  launch_pack_vec<T>(g, s->d_ref_a, pad, mask, s->st);
+  return VF_OK;
+}
+
+template <typename T>
+static int op_out(vf_solver* s, int level, const T* pad, double* h) {
+  const Grid& g = s->L[level].g;
+  launch_unpack_vec<T>(g, pad, s->d_ref_c, s->st);
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaMemcpyAsync(h, s->d_ref_c, sizeof(double) * 3 * (size_t)g.nodes_ref(), cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  return VF_OK;
+}
+
+template <typename T>
+static int apply_t(vf_solver* s, int level, const double* u, double* y) {
+  Level& l = s->L[level];
+  T* a = Sel<T>::w(l, 0);
+  T* b = Sel<T>::w(l, 1);
+  int rc = op_in<T>(s, level, u, a, nullptr);
+  if (rc) return rc;
+  level_op<T>(s, level, EPI_APPLY, a, b, nullptr, nullptr, nullptr, 0);
+  return op_out<T>(s, level, b, y);
+}
+
+template <typename T>
+static int smooth_t(vf_solver* s, int level, const double* u0, const double* b, int sweeps, double* out) {
+  Level& l = s->L[level];
+  T* x = Sel<T>::w(l, 0);
+  T* t = Sel<T>::w(l, 1);
+  T* rhs = Sel<T>::w(l, 3);
+  int rc = op_in<T>(s, level, u0, x, nullptr);
+  if (!rc) rc = op_in<T>(s, level, b, rhs, nullptr);
+  if (rc) return rc;
+  smooth<T>(s, level, x, t, rhs, sweeps, false, nullptr);
+  return op_out<T>(s, level, x, out);
+}
+
+template <typename T>
+static int restrict_t(vf_solver* s, int level, const double* rf, double* rc_out) {
+  Level& l = s->L[level];
+  Level& c = s->L[level + 1];
+  T* a = Sel<T>::w(l, 2);
+  int rc = op_in<T>(s, level, rf, a, nullptr);
+  if (rc) return rc;
+  launch_restrict<T>(l.g, a, c.g, c.mask, Sel<T>::w(c, 3), nullptr, s->st);
+  return op_out<T>(s, level + 1, Sel<T>::w(c, 3), rc_out);
+}
+
+template <typename T>
+static int prolong_t(vf_solver* s, int level, const double* ec, double* ef) {
+  Level& l = s->L[level];
+  Level& c = s->L[level + 1];
+  int rc = op_in<T>(s, level + 1, ec, Sel<T>::w(c, 0), nullptr);
+  if (rc) return rc;
+  cudaMemsetAsync(Sel<T>::w(l, 0), 0, sizeof(T) * 3 * (size_t)l.g.n, s->st);
+  launch_prolong_add<T>(c.g, Sel<T>::w(c, 0), l.g, l.mask, Sel<T>::w(l, 0), nullptr, s->st);
+  return op_out<T>(s, level, Sel<T>::w(l, 0), ef);
+}
+
+template <typename T>
+static int vcycle_t(vf_solver* s, const double* r, double* z) {
+  T** v = kvec<T>(s);
+  int rc = op_in<T>(s, 0, r, v[1], nullptr);
+  if (rc) return rc;
+  precondition<T>(s, v[1], v[2], nullptr);
+  return op_out<T>(s, 0, v[2], z);
+}
+
+extern "C" {
+
+int vf_apply(vf_solver* s, int32_t level, int32_t precision, const double* u, double* y) {
+  int rc = level_check(s, level, precision);
+  if (rc) return rc;
+  if (!u || !y) return VF_ERR_ARG;
+  return precision == VF_PREC_FP64 ? apply_t<double>(s, level, u, y) : apply_t<float>(s, level, u, y);
+}
+
+int vf_smooth(vf_solver* s, int32_t level, int32_t precision, const double* u0, const double* b, int32_t sweeps,
+              double* out) {
+  int rc = level_check(s, level, precision);
+  if (rc) return rc;
+  if (!u0 || !b || !out || sweeps < 0) return VF_ERR_ARG;
+  return precision == VF_PREC_FP64 ? smooth_t<double>(s, level, u0, b, sweeps, out)
+                                   : smooth_t<float>(s, level, u0, b, sweeps, out);
+}
+
+int vf_restrict(vf_solver* s, int32_t level, int32_t precision, const double* rf, double* rc_out) {
+  int rc = level_check(s, level, precision);
+  if (rc) return rc;
+  if (level + 1 >= nlev(s) || !rf || !rc_out) { s->err = "no coarser level"; return VF_ERR_ARG; }
+  return precision == VF_PREC_FP64 ? restrict_t<double>(s, level, rf, rc_out) : restrict_t<float>(s, level, rf, rc_out);
+}
+
+int vf_prolongate(vf_solver* s, int32_t level, int32_t precision, const double* ec, double* ef) {
+  int rc = level_check(s, level, precision);
+  if (rc) return rc;
+  if (level + 1 >= nlev(s) || !ec || !ef) { s->err = "no coarser level"; return VF_ERR_ARG; }
+  return precision == VF_PREC_FP64 ? prolong_t<double>(s, level, ec, ef) : prolong_t<float>(s, level, ec, ef);
+}
+
+int vf_vcycle(vf_solver* s, int32_t precision, const double* r, double* z) {
+  int rc = level_check(s, 0, precision);
+  if (rc) return rc;
+  if (!r || !z) return VF_ERR_ARG;
+  return precision == VF_PREC_FP64 ? vcycle_t<double>(s, r, z) : vcycle_t<float>(s, r, z);
+}
+
+int vf_inv_diagonal(vf_solver* s, int32_t level, double* minv) {
+  int rc = level_check(s, level, VF_PREC_FP64);
+  if (rc) return rc;
+  if (!minv) return VF_ERR_ARG;
+  return op_out<double>(s, level, s->L[level].minv64, minv);
+}
+
+int vf_time_kernel(vf_solver* s, int32_t kernel, int32_t precision, int32_t iters, double* ms) {
+  int rc = level_check(s, 0, precision);
+  if (rc) return rc;
+  if (!ms || iters < 1 || kernel < 0 || kernel > 5) return VF_ERR_ARG;
+  const bool f32 = precision == VF_PREC_FP32;
+  Level& l0 = s->L[0];
+  init_ks(*s->h_ks, 1.0, 1, 0, 0, 1.0);
+  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  auto one = [&]() {
+    if (f32) {
+      float** v = s->k32;
+      switch (kernel) {
+        case 0: level_op<float>(s, 0, EPI_APPLY, v[3], v[4], nullptr, s->ks, s->d_partials, SLOT_PLAIN); break;
+        case 1: level_op<float>(s, 0, EPI_SMOOTH, v[3], v[4], v[1], nullptr, nullptr, 0); break;
+        case 2: level_op<float>(s, 0, EPI_RESID, v[3], v[4], v[1], nullptr, nullptr, 0); break;
+        case 3: if (s->L.size() > 1) launch_restrict<float>(l0.g, v[3], s->L[1].g, s->L[1].mask, s->L[1].w32[3], nullptr, s->st); break;
+        case 4: if (s->L.size() > 1) launch_prolong_add<float>(s->L[1].g, s->L[1].w32[0], l0.g, l0.mask, v[4], nullptr, s->st); break;
+        default: precondition<float>(s, v[1], v[2], nullptr); break;
+      }
+    } else {
+      double** v = s->k64;
+      switch (kernel) {
+        case 0: level_op<double>(s, 0, EPI_APPLY, v[3], v[4], nullptr, s->ks, s->d_partials, SLOT_PLAIN); break;
+        case 1: level_op<double>(s, 0, EPI_SMOOTH, v[3], v[4], v[1], nullptr, nullptr, 0); break;
+        case 2: level_op<double>(s, 0, EPI_RESID, v[3], v[4], v[1], nullptr, nullptr, 0); break;
+        case 3: if (s->L.size() > 1) launch_restrict<double>(l0.g, v[3], s->L[1].g, s->L[1].mask, s->L[1].w64[3], nullptr, s->st); break;
+        case 4: if (s->L.size() > 1) launch_prolong_add<double>(s->L[1].g, s->L[1].w64[0], l0.g, l0.mask, v[4], nullptr, s->st); break;
+        default: precondition<double>(s, v[1], v[2], nullptr); break;
+      }
+    }
+  };
+  one();   // warm-up
+  VF_TRY(cudaEventRecord(s->ev0, s->st));
+  for (int i = 0; i < iters; ++i) one();
+  VF_TRY(cudaEventRecord(s->ev1, s->st));
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaEventSynchronize(s->ev1));
+  float t = 0.f;
+  cudaEventElapsedTime(&t, s->ev0, s->ev1);
+  *ms = t / iters;
+  return VF_OK;
+}
+
+// Host evaluation of sum_e E_e Ke u_e on a small grid vs the device (FP64 and
+// FP32 element kernels): the library's analogue of backend._self_test.
+int vf_self_test(int32_t device) {
+  const int nx = 4, ny = 3, nz = 5;
+  vf_options o;
+  vf_options_default(&o);
+  o.device = device;
+  vf_solver* s = nullptr;
+  int rc = vf_create(nx, ny, nz, 0.3, &o, &s);
+  if (rc) return rc;
+  const int ne = nx * ny * nz, nn = (nx + 1) * (ny + 1) * (nz + 1);
+  std::vector<double> E(ne), u(3 * nn), y(3 * nn), ref(3 * nn, 0.0);
+  unsigned long long st = 88172645463325252ULL;
+  auto rnd = [&]() { st ^= st << 13; st ^= st >> 7; st ^= st << 17; return (double)(st % 1000003) / 1000003.0; };
+  for (auto& e : E) e = 0.5 + rnd();
+  for (auto& v : u) v = rnd() - 0.5;
+  rc = vf_set_fixed(s, nullptr, 0);
+  if (!rc) rc = vf_set_material(s, E.data(), nullptr, 0);
+  for (int ix = 0; ix < nx; ++ix)
+    for (int iy = 0; iy < ny; ++iy)
+      for (int iz = 0; iz < nz; ++iz) {
+        const int e = (ix * ny + iy) * nz + iz;
+        int dofs[24];
+        for (int k = 0; k < 8; ++k) {
+          const int nid = (ix + kCorner[k][0]) + (nx + 1) * ((iy + kCorner[k][1]) + (ny + 1) * (iz + kCorner[k][2]));
+          for (int c = 0; c < 3; ++c) dofs[3 * k + c] = 3 * nid + c;
+        }
+        for (int i = 0; i < 24; ++i) {
+          double acc = 0.0;
+          for (int j = 0; j < 24; ++j) acc += s->tab[i * 24 + j] * u[dofs[j]];
+          ref[dofs[i]] += E[e] * acc;
+        }
+      }
+  double scale = 0.0;
+  for (double v : ref) scale = std::max(scale, std::fabs(v));
+  for (int prec = 0; prec < 2 && !rc; ++prec) {
+    rc = vf_apply(s, 0, prec == 0 ? VF_PREC_FP64 : VF_PREC_FP32, u.data(), y.data());
+    if (rc) break;
+    double err = 0.0;
+    for (int i = 0; i < 3 * nn; ++i) err = std::max(err, std::fabs(y[i] - ref[i]));
+    if (err > (prec == 0 ? 1e-12 : 1e-5) * scale) {
+      g_last_error = "self-test mismatch";
+      rc = VF_ERR_CUDA;
+    }
+  }
+  if (rc && s) g_last_error = s->err.empty() ? g_last_error : s->err;
+  vf_destroy(s);
+  return rc;
+}
+
+}  // extern "C"

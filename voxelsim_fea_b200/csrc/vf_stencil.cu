@@ -1,0 +1,418 @@
+// Assembled coarse operators of the robust (Galerkin) hierarchy.
+//
+// The reference rediscretizes coarse levels (2x2x2 mean modulus, injected
+// Dirichlet mask; core/multigrid.py:255-315).  Under the void/solid contrast
+// of noise geometry that hierarchy stops converging, so this library can build
+// instead the Galerkin operators
+//
+//     A_{l+1} = D_{l+1} P^T D_l A_l D_l P D_{l+1}
+//
+// with P the reference's trilinear prolongation (multigrid.py:42-73).  They are
+// stored as node-centric 27-point stencils of 3x3 blocks, SoA:
+//     st[(s*9 + r*3 + c) * n + p],  s = (dz+1)*9 + (dy+1)*3 + (dx+1)
+// = coupling of DOF r of node p with DOF c of node p + (dx,dy,dz).  Applying
+// one is a deterministic gather (one thread per output node).
+//
+// Build kernels (FP64, once per set_material):
+//   * galerkin_from_fine: level 0 (matrix-free hex8) -> level 1.  A coarse
+//     element E with 8 fine children e contributes sum_e P_e^T D_e K_e D_e P_e.
+//     For a child whose 24 DOFs are all free this is E_e * G[child] with G a
+//     fixed 24x24 table (P^T Ke P, precomputed on the host); children that
+//     touch a Dirichlet DOF take the masked general path.
+//   * galerkin_from_stencil: level l -> l+1 for l >= 1 (stencil RAP).
+//   * stencil_mask_and_diag: D_{l+1} = {DOFs with a non-zero Galerkin
+//     diagonal}; zero their rows/columns; Jacobi inverse diagonal.
+#include "vf_common.cuh"
+#include "vf_reduce.cuh"
+
+namespace vf {
+
+namespace {
+
+constexpr int kThreads = 128;
+
+__device__ __forceinline__ int sidx(int dx, int dy, int dz) { return (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1); }
+
+__device__ __forceinline__ void decode(const Grid& g, int p, int& x, int& y, int& z) {
+  x = p % g.px - 1;
+  int t = p / g.px;
+  y = t % g.py - 1;
+  z = t / g.py - 1;
+}
+
+template <typename T, int EPI>
+__global__ void __launch_bounds__(256) k_stencil_op(Grid g, OpArgs a, const T* __restrict__ st) {
+  KrylovState* ks = a.ks;
+  if (ks && ks->done) return;
+  const T* __restrict__ u = (const T*)a.u;
+  T* __restrict__ out = (T*)a.out;
+  const T* __restrict__ b = (const T*)a.b;
+  const T* __restrict__ minv = (const T*)a.minv;
+  const uint8_t* __restrict__ mask = a.mask;
+  const T w = (T)a.omega;
+  const int nx1 = g.lx + 1, ny1 = g.ly + 1;
+  const int nint = nx1 * ny1 * (g.lz + 1);
+  const long long n = g.n;
+  double dot = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int x = t % nx1;
+    const int rr = t / nx1;
+    const int y = rr % ny1;
+    const int z = rr / ny1;
+    const int p = g.idx(x, y, z);
+    T k0 = 0, k1 = 0, k2 = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int s = sidx(dx, dy, dz);
+          const int q = g.idx(x + dx, y + dy, z + dz);
+          const T u0 = __ldg(u + 3 * q), u1 = __ldg(u + 3 * q + 1), u2 = __ldg(u + 3 * q + 2);
+          const T* B = st + (long long)s * 9 * n + p;
+          k0 += __ldg(B) * u0 + __ldg(B + n) * u1 + __ldg(B + 2 * n) * u2;
+          k1 += __ldg(B + 3 * n) * u0 + __ldg(B + 4 * n) * u1 + __ldg(B + 5 * n) * u2;
+          k2 += __ldg(B + 6 * n) * u0 + __ldg(B + 7 * n) * u1 + __ldg(B + 8 * n) * u2;
+        }
+    const uint8_t m = mask[p];
+    k0 = (m & 1) ? k0 : (T)0;
+    k1 = (m & 2) ? k1 : (T)0;
+    k2 = (m & 4) ? k2 : (T)0;
+    const long long p3 = 3 * (long long)p;
+    if (EPI == EPI_APPLY) {
+      out[p3] = k0; out[p3 + 1] = k1; out[p3 + 2] = k2;
+      if (a.dot_partials)
+        dot += (double)u[p3] * (double)k0 + (double)u[p3 + 1] * (double)k1 + (double)u[p3 + 2] * (double)k2;
+    } else if (EPI == EPI_SMOOTH) {
+      const T r0 = b[p3] - k0, r1 = b[p3 + 1] - k1, r2 = b[p3 + 2] - k2;
+      out[p3] = u[p3] + ((m & 1) ? w * (minv[p3] * r0) : (T)0);
+      out[p3 + 1] = u[p3 + 1] + ((m & 2) ? w * (minv[p3 + 1] * r1) : (T)0);
+      out[p3 + 2] = u[p3 + 2] + ((m & 4) ? w * (minv[p3 + 2] * r2) : (T)0);
+    } else {
+      out[p3] = b[p3] - k0; out[p3 + 1] = b[p3 + 1] - k1; out[p3 + 2] = b[p3 + 2] - k2;
+    }
+  }
+  if (EPI == EPI_APPLY && a.dot_partials && ks) reduce_and_finalize(dot, a.dot_partials, ks, a.dot_slot, nullptr);
+}
+
+// 1-D trilinear weight of a coarse node at fine offset d (in fine spacings).
+__device__ __forceinline__ double w1(int d) { return d == 0 ? 1.0 : ((d == 1 || d == -1) ? 0.5 : 0.0); }
+
+// Per fine element: 1 if all 8 of its nodes have all 3 DOFs free.
+__global__ void k_elem_allfree(Grid f, const uint8_t* __restrict__ m, uint8_t* __restrict__ out) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < f.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(f, p, x, y, z);
+    uint8_t v = 0;
+    if (x >= 0 && x < f.lx && y >= 0 && y < f.ly && z >= 0 && z < f.lz) {
+      uint8_t a = 7;
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) a &= m[f.idx(x + i, y + j, z + k)];
+      v = (a == 7);
+    }
+    out[p] = v;
+  }
+}
+
+// Level 0 -> 1.  One thread per coarse interior node N; loops over the 27
+// output blocks.  Gtab: [8 child positions][24][24] of P_c^T K P_c for K =
+// Ke(nu) (and, with lame, a second table for K_mu after K_lam).  Ktab: the
+// plain 24x24 (or K_lam, K_mu) for the masked path.
+__global__ void __launch_bounds__(kThreads) k_galerkin_from_fine(Grid f, const double* __restrict__ E,
+                                                                 const double* __restrict__ MU,
+                                                                 const uint8_t* __restrict__ fmask,
+                                                                 const uint8_t* __restrict__ allfree,
+                                                                 Grid c, double* __restrict__ stc,
+                                                                 const double* __restrict__ Gtab,
+                                                                 const double* __restrict__ Ktab, int lame) {
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1;
+  const int nint = nx1 * ny1 * (c.lz + 1);
+  const long long n = c.n;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int X = t % nx1;
+    const int rr = t / nx1;
+    const int Y = rr % ny1;
+    const int Z = rr / ny1;
+    const int p = c.idx(X, Y, Z);
+    for (int s = 0; s < 27; ++s) {
+      const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+      double acc[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+      const int MX = X + dx, MY = Y + dy, MZ = Z + dz;
+      if (MX >= 0 && MX <= c.lx && MY >= 0 && MY <= c.ly && MZ >= 0 && MZ <= c.lz) {
+        // coarse elements (lower corner L) containing both N and M
+        for (int lz = Z - 1; lz <= Z; ++lz) {
+          if (lz < 0 || lz >= c.lz || MZ - lz < 0 || MZ - lz > 1) continue;
+          for (int ly = Y - 1; ly <= Y; ++ly) {
+            if (ly < 0 || ly >= c.ly || MY - ly < 0 || MY - ly > 1) continue;
+            for (int lx = X - 1; lx <= X; ++lx) {
+              if (lx < 0 || lx >= c.lx || MX - lx < 0 || MX - lx > 1) continue;
+              const int aNx = X - lx, aNy = Y - ly, aNz = Z - lz;
+              const int aMx = MX - lx, aMy = MY - ly, aMz = MZ - lz;
+              const int aN = corner_k(aNx, aNy, aNz), aM = corner_k(aMx, aMy, aMz);
+              for (int ch = 0; ch < 8; ++ch) {
+                const int ci = ch & 1, cj = (ch >> 1) & 1, ck = ch >> 2;
+                const int q = f.idx(2 * lx + ci, 2 * ly + cj, 2 * lz + ck);
+                const double Ee = E[q];
+                const double Me = lame ? MU[q] : 0.0;
+                if (Ee == 0.0 && Me == 0.0) continue;
+                if (allfree[q]) {
+                  const double* G = Gtab + (size_t)ch * 576;
+#pragma unroll
+                  for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                      double v = Ee * G[(3 * aN + r) * 24 + 3 * aM + cc];
+                      if (lame) v += Me * G[8 * 576 + (3 * aN + r) * 24 + 3 * aM + cc];
+                      acc[r * 3 + cc] += v;
+                    }
+                } else {
+                  // masked general path: sum_{i,i'} wN(i) wM(i') m(i,r) m(i',c) K[(i,r),(i',c)]
+                  uint8_t mi[8];
+                  double wN[8], wM[8];
+                  for (int i = 0; i < 8; ++i) {
+                    const int ox = (i == 1 || i == 2 || i == 5 || i == 6);
+                    const int oy = (i == 2 || i == 3 || i == 6 || i == 7);
+                    const int oz = (i >= 4);
+                    const int fx = ci + ox, fy = cj + oy, fz = ck + oz;   // fine offset within E, 0..2
+                    mi[i] = fmask[f.idx(2 * lx + fx, 2 * ly + fy, 2 * lz + fz)];
+                    wN[i] = w1(fx - 2 * aNx) * w1(fy - 2 * aNy) * w1(fz - 2 * aNz);
+                    wM[i] = w1(fx - 2 * aMx) * w1(fy - 2 * aMy) * w1(fz - 2 * aMz);
+                  }
+                  for (int i = 0; i < 8; ++i) {
+                    if (wN[i] == 0.0) continue;
+                    for (int j = 0; j < 8; ++j) {
+                      if (wM[j] == 0.0) continue;
+                      const double ww = wN[i] * wM[j];
+                      for (int r = 0; r < 3; ++r) {
+                        if (!((mi[i] >> r) & 1)) continue;
+                        for (int cc = 0; cc < 3; ++cc) {
+                          if (!((mi[j] >> cc) & 1)) continue;
+                          const int kk = (3 * i + r) * 24 + 3 * j + cc;
+                          double kv = Ee * Ktab[kk];
+                          if (lame) kv += Me * Ktab[576 + kk];
+                          acc[r * 3 + cc] += ww * kv;
+                        }
+                      }
+                    }
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * n + p] = acc[k];
+    }
+  }
+}
+
+// Level l -> l+1 by stencil RAP (fine stencil already masked).
+__global__ void __launch_bounds__(kThreads) k_galerkin_from_stencil(Grid f, const double* __restrict__ stf,
+                                                                    Grid c, double* __restrict__ stc) {
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1;
+  const int nint = nx1 * ny1 * (c.lz + 1);
+  const long long nf = f.n, nc = c.n;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int X = t % nx1;
+    const int rr = t / nx1;
+    const int Y = rr % ny1;
+    const int Z = rr / ny1;
+    const int p = c.idx(X, Y, Z);
+    for (int s = 0; s < 27; ++s) {
+      const int Dx = s % 3 - 1, Dy = (s / 3) % 3 - 1, Dz = s / 9 - 1;
+      double acc[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+      const int MX = X + Dx, MY = Y + Dy, MZ = Z + Dz;
+      if (MX >= 0 && MX <= c.lx && MY >= 0 && MY <= c.ly && MZ >= 0 && MZ <= c.lz) {
+        for (int iz = -1; iz <= 1; ++iz)
+          for (int iy = -1; iy <= 1; ++iy)
+            for (int ix = -1; ix <= 1; ++ix) {
+              const int fx = 2 * X + ix, fy = 2 * Y + iy, fz = 2 * Z + iz;
+              const double wi = w1(ix) * w1(iy) * w1(iz);
+              const int fp = f.idx(fx, fy, fz);
+              for (int jz = -1; jz <= 1; ++jz) {
+                const int sz = 2 * MZ + jz - fz;
+                if (sz < -1 || sz > 1) continue;
+                for (int jy = -1; jy <= 1; ++jy) {
+                  const int sy = 2 * MY + jy - fy;
+                  if (sy < -1 || sy > 1) continue;
+                  for (int jx = -1; jx <= 1; ++jx) {
+                    const int sx = 2 * MX + jx - fx;
+                    if (sx < -1 || sx > 1) continue;
+                    const double ww = wi * w1(jx) * w1(jy) * w1(jz);
+                    const double* B = stf + (long long)sidx(sx, sy, sz) * 9 * nf + fp;
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) acc[k] += ww * B[k * nf];
+                  }
+                }
+              }
+            }
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * nc + p] = acc[k];
+    }
+  }
+}
+
+// Stencil of the element operator itself (sum_e E_e Ke, masked by D): used for
+// a direct coarsest solve on a rediscretized level.
+__global__ void __launch_bounds__(kThreads) k_stencil_from_elements(Grid g, const double* __restrict__ E,
+                                                                    const double* __restrict__ MU,
+                                                                    const uint8_t* __restrict__ mask,
+                                                                    double* __restrict__ st,
+                                                                    const double* __restrict__ Ktab, int lame) {
+  const int nx1 = g.lx + 1, ny1 = g.ly + 1;
+  const int nint = nx1 * ny1 * (g.lz + 1);
+  const long long n = g.n;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int X = t % nx1;
+    const int rr = t / nx1;
+    const int Y = rr % ny1;
+    const int Z = rr / ny1;
+    const int p = g.idx(X, Y, Z);
+    const uint8_t mp = mask[p];
+    for (int s = 0; s < 27; ++s) {
+      const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+      double acc[9];
+      for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+      const int MX = X + dx, MY = Y + dy, MZ = Z + dz;
+      const uint8_t mq = mask[g.idx(MX, MY, MZ)];
+      for (int lz = Z - 1; lz <= Z; ++lz) {
+        if (MZ - lz < 0 || MZ - lz > 1) continue;
+        for (int ly = Y - 1; ly <= Y; ++ly) {
+          if (MY - ly < 0 || MY - ly > 1) continue;
+          for (int lx = X - 1; lx <= X; ++lx) {
+            if (MX - lx < 0 || MX - lx > 1) continue;
+            const int q = g.idx(lx, ly, lz);
+            const double Ee = E[q], Me = lame ? MU[q] : 0.0;
+            const int aN = corner_k(X - lx, Y - ly, Z - lz), aM = corner_k(MX - lx, MY - ly, MZ - lz);
+            for (int r = 0; r < 3; ++r)
+              for (int cc = 0; cc < 3; ++cc) {
+                const int kk = (3 * aN + r) * 24 + 3 * aM + cc;
+                acc[r * 3 + cc] += Ee * Ktab[kk] + (lame ? Me * Ktab[576 + kk] : 0.0);
+              }
+          }
+        }
+      }
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc) {
+          const bool keep = ((mp >> r) & 1) && ((mq >> cc) & 1);
+          st[((long long)s * 9 + r * 3 + cc) * n + p] = keep ? acc[r * 3 + cc] : 0.0;
+        }
+    }
+  }
+}
+
+// Coarse free mask from the Galerkin diagonal (D_{l+1}).
+__global__ void k_mask_from_diag(Grid c, const double* __restrict__ st, uint8_t* __restrict__ cmask) {
+  const long long n = c.n;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < c.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(c, p, x, y, z);
+    uint8_t m = 0;
+    if (x >= 0 && x <= c.lx && y >= 0 && y <= c.ly && z >= 0 && z <= c.lz) {
+      const int s0 = 13;   // (0,0,0)
+      for (int r = 0; r < 3; ++r)
+        if (st[((long long)s0 * 9 + r * 4) * n + p] > 0.0) m |= (uint8_t)(1 << r);
+    }
+    cmask[p] = m;
+  }
+}
+
+// Zero rows/columns of non-free DOFs; Minv = 1/diag (0 for non-free).
+__global__ void k_apply_mask_diag(Grid c, double* __restrict__ st, const uint8_t* __restrict__ cmask,
+                                  double* __restrict__ minv3) {
+  const long long n = c.n;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < c.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(c, p, x, y, z);
+    const bool inside = (x >= 0 && x <= c.lx && y >= 0 && y <= c.ly && z >= 0 && z <= c.lz);
+    const uint8_t mp = cmask[p];
+    for (int s = 0; s < 27; ++s) {
+      const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+      uint8_t mq = 0;
+      if (inside) mq = cmask[c.idx(x + dx, y + dy, z + dz)];
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc) {
+          const bool keep = inside && ((mp >> r) & 1) && ((mq >> cc) & 1);
+          if (!keep) st[((long long)s * 9 + r * 3 + cc) * n + p] = 0.0;
+        }
+    }
+    for (int r = 0; r < 3; ++r) {
+      const double d = st[((long long)13 * 9 + r * 4) * n + p];
+      minv3[3 * (long long)p + r] = ((mp >> r) & 1) && d != 0.0 ? 1.0 / d : 0.0;
+    }
+  }
+}
+
+inline int blocks_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b > 148 * 32) b = 148 * 32;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+template <typename T>
+int stencil_op_grid_blocks(const Grid& g) {
+  long long nint = (long long)(g.lx + 1) * (g.ly + 1) * (g.lz + 1);
+  long long b = (nint + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+template <typename T>
+void launch_stencil_op(const Grid& g, int epi, const OpArgs& a, const T* stencil, cudaStream_t st) {
+  const int blocks = stencil_op_grid_blocks<T>(g);
+  if (epi == EPI_APPLY) launch_k(k_stencil_op<T, EPI_APPLY>, blocks, 256, 0, st, g, a, stencil);
+  else if (epi == EPI_SMOOTH) launch_k(k_stencil_op<T, EPI_SMOOTH>, blocks, 256, 0, st, g, a, stencil);
+  else launch_k(k_stencil_op<T, EPI_RESID>, blocks, 256, 0, st, g, a, stencil);
+}
+template void launch_stencil_op<double>(const Grid&, int, const OpArgs&, const double*, cudaStream_t);
+template void launch_stencil_op<float>(const Grid&, int, const OpArgs&, const float*, cudaStream_t);
+template int stencil_op_grid_blocks<double>(const Grid&);
+template int stencil_op_grid_blocks<float>(const Grid&);
+
+void launch_elem_allfree(const Grid& f, const uint8_t* fmask, uint8_t* allfree, cudaStream_t st) {
+  launch_k(k_elem_allfree, blocks_for(f.n, 256), 256, 0, st, f, fmask, allfree);
+}
+
+void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu, const uint8_t* fmask,
+                               const uint8_t* allfree, const Grid& c, double* stencil_c, const double* Gtab,
+                               const double* Ktab, int lame, cudaStream_t st) {
+  long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
+  launch_k(k_galerkin_from_fine, blocks_for(nint, kThreads), kThreads, 0, st, f, E, mu, fmask, allfree, c, stencil_c,
+                                                                        Gtab, Ktab, lame);
+}
+
+void launch_galerkin_from_stencil(const Grid& f, const double* stencil_f, const Grid& c, double* stencil_c,
+                                  cudaStream_t st) {
+  long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
+  launch_k(k_galerkin_from_stencil, blocks_for(nint, kThreads), kThreads, 0, st, f, stencil_f, c, stencil_c);
+}
+
+void launch_stencil_from_elements(const Grid& g, const double* E, const double* mu, const uint8_t* mask,
+                                  double* stencil, const double* Ktab, int lame, cudaStream_t st) {
+  long long nint = (long long)(g.lx + 1) * (g.ly + 1) * (g.lz + 1);
+  launch_k(k_stencil_from_elements, blocks_for(nint, kThreads), kThreads, 0, st, g, E, mu, mask, stencil, Ktab, lame);
+}
+
+void launch_galerkin_mask(const Grid& c, double* stencil, uint8_t* cmask, double* minv3, cudaStream_t st) {
+  launch_k(k_mask_from_diag, blocks_for(c.n, 256), 256, 0, st, c, stencil, cmask);
+  launch_k(k_apply_mask_diag, blocks_for(c.n, 256), 256, 0, st, c, stencil, cmask, minv3);
+}
+
+void launch_stencil_diag(const Grid& c, double* stencil, const uint8_t* cmask, double* minv3, cudaStream_t st) {
+  launch_k(k_apply_mask_diag, blocks_for(c.n, 256), 256, 0, st, c, stencil, cmask, minv3);
+}
+
+}  // namespace vf

@@ -1,0 +1,148 @@
+// Grid transfers of the V-cycle, in gather form (no atomics, deterministic):
+//
+//   restriction  r_c[J] = D_c sum_{d in {-1,0,1}^3} w(d) r_f[2J + d]
+//                w(d) = prod_k (d_k == 0 ? 1 : 1/2)
+//     == R = P^T of the reference's trilinear P, scattered there with
+//        bincount (core/multigrid.py:404-416); the reference's clipped
+//        corners carry weight 0 (multigrid.py:62-72), so the gather is exact.
+//   prolongation u_f[i] += D_f sum_J w(i - 2J) e_c[J]     (multigrid.py:418-424, 434)
+//   first sweep  u = w * D (Minv b)   -- the first damped-Jacobi sweep of a
+//     V-cycle starts from u = 0, where b - A u = b exactly (multigrid.py:430).
+#include "vf_common.cuh"
+
+namespace vf {
+
+namespace {
+
+__global__ void __launch_bounds__(256) k_restrict_d(Grid f, const double* __restrict__ rf, Grid c,
+                                                    const uint8_t* __restrict__ cm, double* __restrict__ rc,
+                                                    const KrylovState* ks) {
+  if (ks && ks->done) return;
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1, nint = nx1 * ny1 * (c.lz + 1);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int X = t % nx1, rr = t / nx1, Y = rr % ny1, Z = rr / ny1;
+    double a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          const double w = (dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0);
+          const long long q = 3 * (long long)f.idx(2 * X + dx, 2 * Y + dy, 2 * Z + dz);
+          a0 += w * rf[q]; a1 += w * rf[q + 1]; a2 += w * rf[q + 2];
+        }
+    const int p = c.idx(X, Y, Z);
+    const uint8_t m = cm[p];
+    rc[3 * (long long)p] = (m & 1) ? a0 : 0.0;
+    rc[3 * (long long)p + 1] = (m & 2) ? a1 : 0.0;
+    rc[3 * (long long)p + 2] = (m & 4) ? a2 : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_restrict_f(Grid f, const float* __restrict__ rf, Grid c,
+                                                    const uint8_t* __restrict__ cm, float* __restrict__ rc,
+                                                    const KrylovState* ks) {
+  if (ks && ks->done) return;
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1, nint = nx1 * ny1 * (c.lz + 1);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int X = t % nx1, rr = t / nx1, Y = rr % ny1, Z = rr / ny1;
+    float a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          const float w = (dx ? 0.5f : 1.0f) * (dy ? 0.5f : 1.0f) * (dz ? 0.5f : 1.0f);
+          const long long q = 3 * (long long)f.idx(2 * X + dx, 2 * Y + dy, 2 * Z + dz);
+          a0 += w * rf[q]; a1 += w * rf[q + 1]; a2 += w * rf[q + 2];
+        }
+    const int p = c.idx(X, Y, Z);
+    const uint8_t m = cm[p];
+    rc[3 * (long long)p] = (m & 1) ? a0 : 0.0f;
+    rc[3 * (long long)p + 1] = (m & 2) ? a1 : 0.0f;
+    rc[3 * (long long)p + 2] = (m & 4) ? a2 : 0.0f;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_add(Grid c, const T* __restrict__ ec, Grid f,
+                                                     const uint8_t* __restrict__ fm, T* __restrict__ uf,
+                                                     const KrylovState* ks) {
+  if (ks && ks->done) return;
+  const int nx1 = f.lx + 1, ny1 = f.ly + 1, nint = nx1 * ny1 * (f.lz + 1);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int x = t % nx1, rr = t / nx1, y = rr % ny1, z = rr / ny1;
+    const int p = f.idx(x, y, z);
+    const uint8_t m = fm[p];
+    if (!m) continue;
+    const int x0 = x >> 1, y0 = y >> 1, z0 = z >> 1;
+    const int nxs = (x & 1) + 1, nys = (y & 1) + 1, nzs = (z & 1) + 1;
+    const T wx = (x & 1) ? (T)0.5 : (T)1, wy = (y & 1) ? (T)0.5 : (T)1, wz = (z & 1) ? (T)0.5 : (T)1;
+    T e0 = 0, e1 = 0, e2 = 0;
+    for (int kz = 0; kz < nzs; ++kz)
+      for (int ky = 0; ky < nys; ++ky)
+        for (int kx = 0; kx < nxs; ++kx) {
+          const T w = wx * wy * wz;
+          const long long q = 3 * (long long)c.idx(x0 + kx, y0 + ky, z0 + kz);
+          e0 += w * ec[q]; e1 += w * ec[q + 1]; e2 += w * ec[q + 2];
+        }
+    const long long p3 = 3 * (long long)p;
+    if (m & 1) uf[p3] += e0;
+    if (m & 2) uf[p3 + 1] += e1;
+    if (m & 4) uf[p3 + 2] += e2;
+  }
+}
+
+template <typename T>
+__global__ void k_jacobi_from_zero(Grid g, const T* __restrict__ b, const T* __restrict__ minv,
+                                   const uint8_t* __restrict__ mask, T w, T* __restrict__ u,
+                                   const KrylovState* ks) {
+  if (ks && ks->done) return;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
+    const uint8_t m = mask[p];
+    const long long p3 = 3 * (long long)p;
+    u[p3] = (m & 1) ? w * (minv[p3] * b[p3]) : (T)0;
+    u[p3 + 1] = (m & 2) ? w * (minv[p3 + 1] * b[p3 + 1]) : (T)0;
+    u[p3 + 2] = (m & 4) ? w * (minv[p3 + 2] * b[p3 + 2]) : (T)0;
+  }
+}
+
+inline int blocks_for(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+template <>
+void launch_restrict<double>(const Grid& f, const double* rf, const Grid& c, const uint8_t* cmask, double* rc,
+                             const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_restrict_d, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c, cmask, rc, ks);
+}
+template <>
+void launch_restrict<float>(const Grid& f, const float* rf, const Grid& c, const uint8_t* cmask, float* rc,
+                            const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_restrict_f, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c, cmask, rc, ks);
+}
+
+template <typename T>
+void launch_prolong_add(const Grid& c, const T* ec, const Grid& f, const uint8_t* fmask, T* uf,
+                        const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_prolong_add<T>, blocks_for((long long)(f.lx + 1) * (f.ly + 1) * (f.lz + 1)), 256, 0, st, c, ec, f, fmask, uf, ks);
+}
+
+template <typename T>
+void launch_jacobi_from_zero(const Grid& g, const T* b, const T* minv3, const uint8_t* mask, double omega, T* u,
+                             const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_jacobi_from_zero<T>, blocks_for(g.n), 256, 0, st, g, b, minv3, mask, (T)omega, u, ks);
+}
+
+template void launch_prolong_add<double>(const Grid&, const double*, const Grid&, const uint8_t*, double*, const KrylovState*, cudaStream_t);
+template void launch_prolong_add<float>(const Grid&, const float*, const Grid&, const uint8_t*, float*, const KrylovState*, cudaStream_t);
+template void launch_jacobi_from_zero<double>(const Grid&, const double*, const double*, const uint8_t*, double, double*, const KrylovState*, cudaStream_t);
+template void launch_jacobi_from_zero<float>(const Grid&, const float*, const float*, const uint8_t*, double, float*, const KrylovState*, cudaStream_t);
+
+}  // namespace vf

@@ -1,0 +1,304 @@
+"""Geometric-multigrid PCG solver on the B200 -- drop-in for
+VoxelSim-FEA's ``core/multigrid.py`` ``MGSolver``.
+
+Same constructor signature, ``solve`` contract, attributes (``last_iters``,
+``last_converged``, ``last_resid_ratio``, ``resid_history``, ``levels``,
+``plan``) and error behaviour (stall guard raises ``RuntimeError``, always
+printed non-convergence warning) as the reference (core/multigrid.py:85-583).
+Every operator, smoother sweep, transfer and PCG update runs in libvoxfea on
+the device; the host only supplies numpy inputs and receives numpy ``u``.
+
+Default settings reproduce the reference algorithm exactly (FP64,
+rediscretized coarse levels, injected Dirichlet masks, 30-sweep Jacobi coarse
+"solve").  ``SolverOptions`` selects the B200 extensions:
+
+* ``coarse="galerkin"``  R A P coarse operators (robust on void/solid noise
+  geometry, where the rediscretized hierarchy stops converging);
+* ``coarsest="cholesky"`` FP64 dense direct solve on the coarsest level;
+* ``precision="mixed"`` FP32 PCG + V-cycle inside FP64 iterative refinement
+  (FP64 dots, outer residual and coarsest solve); ``"fp32"`` without refinement.
+"""
+
+import ctypes
+import dataclasses
+import time
+
+import numpy as np
+
+from . import _lib, compute_plan
+
+
+@dataclasses.dataclass
+class SolverOptions:
+    """B200 solver options beyond the reference's keyword arguments."""
+    precision: str = "fp64"          # "fp64" | "mixed" | "fp32"
+    coarse: str = "rediscretize"     # "rediscretize" (reference) | "galerkin"
+    coarsest: str = "jacobi"         # "jacobi" (reference, 30 sweeps) | "cholesky"
+    coarse_sweeps: int = 30
+    stall_guard: bool = True
+    check_every: int = 8             # PCG iterations per device graph launch
+    use_graphs: bool = True
+    device: int = 0
+    inner_tol: float = 1e-4          # mixed: residual reduction per inner solve
+    max_outer: int = 20
+
+    @classmethod
+    def reference(cls, **kw):
+        """The reference algorithm, FP64 (core/multigrid.py)."""
+        return cls(**kw)
+
+    @classmethod
+    def robust(cls, **kw):
+        """FP64 Galerkin hierarchy with a direct coarsest solve ("plain GMG-PCG")."""
+        base = dict(coarse="galerkin", coarsest="cholesky")
+        base.update(kw)
+        return cls(**base)
+
+    @classmethod
+    def fast(cls, **kw):
+        """Galerkin hierarchy, mixed precision with FP64 refinement."""
+        base = dict(coarse="galerkin", coarsest="cholesky", precision="mixed")
+        base.update(kw)
+        return cls(**base)
+
+
+def _node_dims(nx, ny, nz):
+    return (nx + 1, ny + 1, nz + 1)
+
+
+def _injected_free(levels, fixed_dofs):
+    """Per-level free masks by injection (core/multigrid.py:255-278); host
+    bookkeeping only, for the ``levels[li]['free']`` attribute."""
+    free0 = np.ones(levels[0]["ndof"], dtype=bool)
+    fd = np.asarray(fixed_dofs, dtype=np.int64)
+    if fd.size:
+        free0[fd] = False
+    levels[0]["free"] = free0
+    prev, prev_dims = free0, _node_dims(*levels[0]["dims"])
+    for li in range(1, len(levels)):
+        Lcx, Lcy, Lcz = _node_dims(*levels[li]["dims"])
+        Lfx, Lfy, _ = prev_dims
+        n = np.arange(Lcx * Lcy * Lcz)
+        fid = 2 * (n % Lcx) + Lfx * (2 * ((n // Lcx) % Lcy) + Lfy * (2 * (n // (Lcx * Lcy))))
+        free = np.ones(3 * n.size, dtype=bool)
+        for c in range(3):
+            free[3 * n + c] = prev[3 * fid + c]
+        levels[li]["free"] = free
+        prev, prev_dims = free, (Lcx, Lcy, Lcz)
+
+
+class MGSolver:
+    """Multigrid-preconditioned CG on the full voxel grid, on the B200."""
+
+    _TRY_POOLED_SMOOTH = False   # reference class switch (multigrid.py:83); no pools here
+
+    def __init__(self, nx, ny, nz, fixed_dofs, nu=0.3, xp=None, n_smooth=2, omega=0.6,
+                 min_elems=4, max_levels=6, compute_mode="AUTO", cpu_threads=0,
+                 verbose=False, options=None, method=_lib.VF_METHOD_MG):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.nelem = nx * ny * nz
+        self.ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+        self.n_smooth = n_smooth
+        self.omega = omega
+        self.nu = nu
+        self.verbose = verbose
+        self.options = options if options is not None else SolverOptions()
+        self.xp = np
+        self.plan = compute_plan.choose(self.ndof, mode=compute_mode, cpu_threads=cpu_threads,
+                                        verbose=verbose)
+        self._h = None
+        L = _lib.load()
+        o = _lib.default_options()
+        o.method = method
+        o.precision = _lib.PRECISIONS[self.options.precision]
+        o.n_smooth = int(n_smooth)
+        o.omega = float(omega)
+        o.min_elems = int(min_elems)
+        o.max_levels = int(max_levels)
+        o.coarse_op = _lib.COARSE_OPS[self.options.coarse]
+        o.coarsest = _lib.COARSEST[self.options.coarsest]
+        o.coarse_sweeps = int(self.options.coarse_sweeps)
+        o.stall_guard = int(bool(self.options.stall_guard))
+        o.check_every = int(self.options.check_every)
+        o.use_graphs = int(bool(self.options.use_graphs))
+        o.device = int(self.options.device)
+        o.inner_tol = float(self.options.inner_tol)
+        o.max_outer = int(self.options.max_outer)
+        h = ctypes.c_void_p()
+        _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
+                   None, "vf_create")
+        self._h = h
+        n = ctypes.c_int32()
+        L.vf_num_levels(h, ctypes.byref(n))
+        self.levels = []
+        d3 = (ctypes.c_int32 * 3)()
+        for li in range(n.value):
+            L.vf_level_dims(h, li, d3)
+            lx, ly, lz = int(d3[0]), int(d3[1]), int(d3[2])
+            self.levels.append({"dims": (lx, ly, lz), "ndof": 3 * (lx + 1) * (ly + 1) * (lz + 1),
+                                "g": float(2 ** li), "free": None})
+        self.last_iters = 0
+        self.last_converged = None
+        self.last_resid_ratio = float("nan")
+        self.resid_history = []
+        self.last_info = None
+        self._density_set = False
+        self._build_free(fixed_dofs)
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self):
+        """Release the device state (core/multigrid.py:245-252)."""
+        if self._h is not None:
+            _lib.load().vf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _handle(self):
+        if self._h is None:
+            raise RuntimeError("solver is closed")
+        return self._h
+
+    # -- boundary conditions / density -----------------------------------------
+    def _build_free(self, fixed_dofs):
+        fd = np.ascontiguousarray(np.asarray(fixed_dofs, dtype=np.int64).ravel())
+        self._fixed = fd
+        _lib.check(_lib.load().vf_set_fixed(self._handle(), _lib.ptr(fd), fd.size), self._h,
+                   "set_fixed")
+        if self.options.coarse == "rediscretize":
+            _injected_free(self.levels, fd)
+        else:
+            _injected_free(self.levels[:1], fd)
+        self._density_set = False
+
+    def set_density(self, Evec_full, nu_elem=None):
+        """Per-element modulus (core/multigrid.py:281-315): builds every
+        level's operator and diagonal on the device.  ``nu_elem`` optionally
+        gives a per-voxel Poisson ratio (B200 extension)."""
+        E = _lib.f64(np.asarray(Evec_full, dtype=float).ravel())
+        if E.size != self.nelem:
+            raise ValueError(f"Evec has {E.size} entries, expected {self.nelem}")
+        nu_e = None if nu_elem is None else _lib.f64(np.asarray(nu_elem, dtype=float).ravel())
+        _lib.check(_lib.load().vf_set_material(self._handle(), _lib.ptr(E), _lib.ptr(nu_e), 0), self._h,
+                   "set_density")
+        self._density_set = True
+
+    # -- level operators (reference private API, routed to the device) ------
+    def _need_density(self):
+        if not self._density_set:
+            raise RuntimeError("call set_density() first")
+
+    def _level_call(self, fn, li, *arrays, out_level=None, precision="fp64", extra=()):
+        self._need_density()
+        out_level = li if out_level is None else out_level
+        out = np.empty(self.levels[out_level]["ndof"])
+        args = [_lib.ptr(_lib.f64(a)) for a in arrays]
+        prec = _lib.PRECISIONS[precision]
+        _lib.check(fn(self._handle(), li, prec, *args, *extra, _lib.ptr(out)), self._h)
+        return out
+
+    def _apply(self, li, u, precision="fp64"):
+        """y = where(free, K_li u, 0) (core/multigrid.py:318-341)."""
+        return self._level_call(_lib.load().vf_apply, li, u, precision=precision)
+
+    _apply_pooled = None   # set below: level-0 apply (multigrid.py:343-365)
+
+    def _smooth(self, li, u, b, iters, precision="fp64"):
+        """``iters`` damped-Jacobi sweeps (core/multigrid.py:367-402)."""
+        self._need_density()
+        out = np.empty(self.levels[li]["ndof"])
+        u = _lib.f64(u)
+        b = _lib.f64(b)
+        _lib.check(_lib.load().vf_smooth(self._handle(), li, _lib.PRECISIONS[precision], _lib.ptr(u),
+                                         _lib.ptr(b), int(iters), _lib.ptr(out)), self._h)
+        return out
+
+    def _restrict(self, li, r_fine, precision="fp64"):
+        """R = P^T then coarse mask (core/multigrid.py:404-416)."""
+        return self._level_call(_lib.load().vf_restrict, li, r_fine, out_level=li + 1,
+                                precision=precision)
+
+    def _prolongate(self, li, e_coarse, precision="fp64"):
+        """where(free_f, P e_c) (core/multigrid.py:418-424)."""
+        return self._level_call(_lib.load().vf_prolongate, li, e_coarse, precision=precision)
+
+    def _vcycle(self, li, b, precision="fp64"):
+        """One V-cycle from level 0 (core/multigrid.py:426-436)."""
+        if li != 0:
+            raise ValueError("the device V-cycle starts at level 0")
+        self._need_density()
+        out = np.empty(self.ndof)
+        b = _lib.f64(b)
+        _lib.check(_lib.load().vf_vcycle(self._handle(), _lib.PRECISIONS[precision], _lib.ptr(b),
+                                         _lib.ptr(out)), self._h)
+        return out
+
+    def inv_diagonal(self, li):
+        """levels[li]['Minv'] (core/multigrid.py:300-304), 3 values per node."""
+        self._need_density()
+        out = np.empty(self.levels[li]["ndof"])
+        _lib.check(_lib.load().vf_inv_diagonal(self._handle(), li, _lib.ptr(out)), self._h)
+        return out
+
+    # -- public solve ------------------------------------------------------------
+    def solve(self, Evec_full, f, tol=1e-4, max_cg=None, x0=None, progress_cb=None, nu_elem=None):
+        """PCG with the V-cycle preconditioner; returns a fresh numpy u
+        (core/multigrid.py:439-583).  ``progress_cb(it, resid_ratio, tol)`` is
+        called once per iteration, in order (bursts at graph-chunk ends)."""
+        self.resid_history = []
+        t0 = time.perf_counter()
+        self.set_density(Evec_full, nu_elem=nu_elem)
+        f = _lib.f64(np.asarray(f, dtype=float).ravel())
+        if f.size != self.ndof:
+            raise ValueError(f"f has {f.size} entries, expected {self.ndof}")
+        x0a = None if x0 is None else _lib.f64(np.asarray(x0, dtype=float).ravel())
+        u = np.empty(self.ndof)
+        info = _lib.VfSolveInfo()
+        cb_error = []
+
+        def _tramp(it, resid, tl, _user):
+            if progress_cb is None or cb_error:
+                return
+            try:
+                progress_cb(int(it), float(resid), float(tl))
+            except BaseException as exc:  # noqa: BLE001  re-raised after the call
+                cb_error.append(exc)
+
+        cfun = _lib.PROGRESS_FN(_tramp)
+        L = _lib.load()
+        rc = L.vf_solve_cb(self._handle(), _lib.ptr(f), _lib.ptr(x0a), float(tol),
+                           int(max_cg or 0), 0, _lib.ptr(u), ctypes.byref(info), cfun, None)
+        self.last_info = info
+        if rc not in (_lib.VF_OK, _lib.VF_ERR_STALLED):
+            _lib.check(rc, self._h, "solve")
+        if info.iters < 0:
+            return np.zeros(self.ndof)   # zero load (multigrid.py:471-473)
+        n = ctypes.c_int32()
+        L.vf_resid_history(self._h, None, 0, ctypes.byref(n))
+        hist = np.empty(n.value)
+        L.vf_resid_history(self._h, _lib.ptr(hist), n.value, ctypes.byref(n))
+        self.resid_history = [float(v) for v in hist]
+        self.last_iters = int(info.iters)
+        self.last_converged = bool(info.converged)
+        self.last_resid_ratio = float(info.resid_ratio)
+        if cb_error:
+            raise cb_error[0]
+        if rc == _lib.VF_ERR_STALLED:
+            _lib.check(rc, self._h)
+        if not self.last_converged:
+            print(f"[VoxelSim FEA] WARNING: MG-PCG did not converge in {max_cg or 1000} "
+                  f"iterations (tol={tol:g}, final residual ratio={self.last_resid_ratio:.3e}, "
+                  f"plan={self.plan.label}). Returned displacement may be inaccurate.")
+        if self.verbose:
+            print(f"[VoxelSim FEA] MG solve: {self.last_iters} CG iters "
+                  f"(converged={self.last_converged}), total={(time.perf_counter() - t0) * 1e3:.1f}ms | "
+                  f"device={info.device_ms:.1f}ms setup={info.setup_ms:.1f}ms "
+                  f"true residual={info.true_resid:.3e}")
+        return u
+
+
+MGSolver._apply_pooled = lambda self, u: self._apply(0, u)
