@@ -84,8 +84,16 @@ typedef struct vf_options {
   int32_t max_outer;       /* VF_PREC_MIXED: refinement steps cap           */
   double  omega;           /* Jacobi damping (multigrid.py:86, default 0.6) */
   double  inner_tol;       /* VF_PREC_MIXED: residual reduction per inner solve */
+  int32_t omega_mode;      /* VF_OMEGA_FIXED: omega on every level (reference);
+                              VF_OMEGA_AUTO: omega_l = omega_rel * 2 / lambda_l with
+                              lambda_l a power-iteration estimate of
+                              lambda_max(D^-1 A_l) taken at set_material */
+  int32_t power_iters;     /* VF_OMEGA_AUTO: power iterations per level (20) */
+  double  omega_rel;       /* VF_OMEGA_AUTO: fraction of the stability limit (0.8) */
   int32_t reserved[8];
 } vf_options;
+
+enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
 
 typedef struct vf_solve_info {
   int32_t iters;           /* PCG iterations (all inner iterations for MIXED);
@@ -131,6 +139,9 @@ int         vf_destroy(vf_solver* s);
 const char* vf_last_error(const vf_solver* s);
 int         vf_num_levels(const vf_solver* s, int32_t* n);
 int         vf_level_dims(const vf_solver* s, int32_t level, int32_t* dims3);
+/* Damping used on a level and, with VF_OMEGA_AUTO, the lambda_max(D^-1 A)
+ * estimate behind it (valid after vf_set_material). */
+int         vf_level_omega(const vf_solver* s, int32_t level, double* omega, double* lambda);
 
 /* ---- problem definition --------------------------------------------------- */
 /* MGSolver._build_free (multigrid.py:255-278) / VoxelFEA.set_fixed

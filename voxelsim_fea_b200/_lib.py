@@ -29,6 +29,7 @@ VF_METHOD_MG, VF_METHOD_JACOBI = 0, 1
 VF_COARSE_REDISCRETIZE, VF_COARSE_GALERKIN = 0, 1
 VF_COARSEST_JACOBI, VF_COARSEST_CHOLESKY = 0, 1
 VF_SOLVE_DEVICE_PTRS = 1
+VF_OMEGA_FIXED, VF_OMEGA_AUTO = 0, 1
 
 PRECISIONS = {"fp64": VF_PREC_FP64, "mixed": VF_PREC_MIXED, "fp32": VF_PREC_FP32}
 COARSE_OPS = {"rediscretize": VF_COARSE_REDISCRETIZE, "galerkin": VF_COARSE_GALERKIN}
@@ -38,7 +39,7 @@ COARSEST = {"jacobi": VF_COARSEST_JACOBI, "cholesky": VF_COARSEST_CHOLESKY}
 EXPORTS = (
     "vf_abi_version", "vf_status_string", "vf_global_last_error", "vf_device_count",
     "vf_self_test", "vf_hex8_tables", "vf_options_default", "vf_create", "vf_destroy", "vf_last_error",
-    "vf_num_levels", "vf_level_dims", "vf_set_fixed", "vf_set_active", "vf_set_material",
+    "vf_num_levels", "vf_level_dims", "vf_level_omega", "vf_set_fixed", "vf_set_active", "vf_set_material",
     "vf_solve", "vf_solve_cb", "vf_resid_history", "vf_von_mises", "vf_strain_energy",
     "vf_drop_unsupported_islands", "vf_apply", "vf_smooth", "vf_restrict", "vf_prolongate",
     "vf_vcycle", "vf_inv_diagonal", "vf_time_kernel", "vf_get_stream", "vf_launch_count",
@@ -55,6 +56,8 @@ class VfOptions(ctypes.Structure):
         ("check_every", ctypes.c_int32), ("use_graphs", ctypes.c_int32),
         ("device", ctypes.c_int32), ("max_outer", ctypes.c_int32),
         ("omega", ctypes.c_double), ("inner_tol", ctypes.c_double),
+        ("omega_mode", ctypes.c_int32), ("power_iters", ctypes.c_int32),
+        ("omega_rel", ctypes.c_double),
         ("reserved", ctypes.c_int32 * 8),
     ]
 
@@ -99,6 +102,7 @@ def _declare(L):
         "vf_last_error": (ctypes.c_char_p, [_P]),
         "vf_num_levels": (ctypes.c_int, [_P, ctypes.POINTER(_I32)]),
         "vf_level_dims": (ctypes.c_int, [_P, _I32, ctypes.POINTER(_I32)]),
+        "vf_level_omega": (ctypes.c_int, [_P, _I32, _D, _D]),
         "vf_set_fixed": (ctypes.c_int, [_P, _P, ctypes.c_int64]),
         "vf_set_active": (ctypes.c_int, [_P, _P]),
         "vf_set_material": (ctypes.c_int, [_P, _P, _P, ctypes.c_uint32]),

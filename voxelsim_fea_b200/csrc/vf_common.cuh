@@ -130,6 +130,7 @@ struct OpArgs {
   KrylovState* ks;        // optional: skip when ks->done; finalize the dot
   int dot_slot;           // which reduction finalizes (see vf_reduce.cuh)
   const double* ke_tab;   // HOST pointer: [KE(nu) | K_lam | K_mu], 3 x 576 doubles
+  const double* omega_dev;  // device: damping of this level (overrides omega when set)
 };
 template <typename T> void launch_fine_op(const Grid& g, int epi, const OpArgs& a, cudaStream_t st);
 template <typename T> int fine_op_grid_blocks(const Grid& g);
@@ -145,7 +146,7 @@ void launch_stencil_mask_and_diag(const Grid& c, double* stencil, uint8_t* cmask
 // vf_transfer.cu -- restriction / prolongation / first sweep
 template <typename T> void launch_restrict(const Grid& f, const T* rf, const Grid& c, const uint8_t* cmask, T* rc, const KrylovState* ks, cudaStream_t st);
 template <typename T> void launch_prolong_add(const Grid& c, const T* ec, const Grid& f, const uint8_t* fmask, T* uf, const KrylovState* ks, cudaStream_t st);
-template <typename T> void launch_jacobi_from_zero(const Grid& g, const T* b, const T* minv3, const uint8_t* mask, double omega, T* u, const KrylovState* ks, cudaStream_t st);
+template <typename T> void launch_jacobi_from_zero(const Grid& g, const T* b, const T* minv3, const uint8_t* mask, double omega, const double* omega_dev, T* u, const KrylovState* ks, cudaStream_t st);
 
 // vf_dense.cu -- coarsest-level dense FP64 direct solve
 int dense_assemble(const Grid& c, const double* stencil, const uint8_t* cmask, double* A, int n, cudaStream_t st);
@@ -164,6 +165,11 @@ void launch_norm2_f64(const Grid& g, const double* v, double* partials, KrylovSt
 void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState* ks, cudaStream_t st);
 void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const KrylovState* ks, cudaStream_t st);
 void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st);
+// power iteration on D^-1 A (per-level damping)
+void launch_power_init(const Grid& g, double* x, const uint8_t* mask, cudaStream_t st);
+void launch_power_scale(const Grid& g, double* y, const double* minv3, double* partials, KrylovState* ks, cudaStream_t st);
+void launch_power_normalize(const Grid& g, const double* y, double* x, const KrylovState* ks, cudaStream_t st);
+void launch_power_omega(const KrylovState* ks, double omega_rel, double safety, double* omega_out, double* lambda_out, cudaStream_t st);
 
 // vf_post.cu -- post-processing and the island pre-step
 void launch_von_mises(const Grid& g, const double* u_pad, const double* Es_ref, const double* nu_ref, double nu,

@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(kOpThreads) k_fine_op(Grid g, OpArgs a, const 
   const T* __restrict__ E = (const T*)a.E;
   const T* __restrict__ MU = (const T*)a.mu;
   const uint8_t* __restrict__ mask = a.mask;
-  const T w = (T)a.omega;
+  const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
   const int nx1 = g.lx + 1, ny1 = g.ly + 1;
   const int nint = nx1 * ny1 * (g.lz + 1);
   double dot = 0.0;

@@ -135,6 +135,10 @@ struct vf_solver {
   unsigned long long chunk_kernels[3] = {0, 0, 0};
   std::vector<void*> allocs;
   double last_setup_ms = 0.0;
+  double last_best = 0.0;       // stall guard: best ratio of the last solve
+  double* d_omega = nullptr;    // damping per level (read by the smoothers)
+  double* d_lambda = nullptr;   // lambda_max(D^-1 A_l) estimates (VF_OMEGA_AUTO)
+  std::vector<double> h_omega, h_lambda;
 };
 
 namespace {
@@ -206,6 +210,7 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
   a.mu = s->lame ? Sel<T>::mu(l) : nullptr;
   a.mask = l.mask;
   a.omega = s->o.omega;
+  a.omega_dev = s->d_omega + li;
   a.dot_partials = partials;
   a.ks = ks;
   a.dot_slot = slot;
@@ -227,7 +232,7 @@ void smooth(vf_solver* s, int li, T* x, T* tmp, const T* b, int sweeps, bool fro
   int rest;
   if (from_zero) {
     T* first = (sweeps % 2 == 1) ? x : tmp;
-    launch_jacobi_from_zero<T>(l.g, b, Sel<T>::minv(l), l.mask, s->o.omega, first, ks, s->st);
+    launch_jacobi_from_zero<T>(l.g, b, Sel<T>::minv(l), l.mask, s->o.omega, s->d_omega + li, first, ks, s->st);
     cur = first;
     rest = sweeps - 1;
   } else {
@@ -449,6 +454,8 @@ int build_levels(vf_solver* s) {
   VF_ALLOC(s->ks, 1);
   VF_ALLOC(s->d_partials, 148 * 64);
   VF_ALLOC(s->d_info, 1);
+  VF_ALLOC(s->d_omega, 16);
+  VF_ALLOC(s->d_lambda, 16);
   VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
   memset(s->h_ks, 0, sizeof(KrylovState));
   return ensure_hist(s, 4096);
@@ -482,6 +489,38 @@ int build_masks(vf_solver* s) {
   for (size_t i = 1; i < s->L.size(); ++i)
     if (!s->L[i].galerkin) launch_inject_mask(s->L[i - 1].g, s->L[i - 1].mask, s->L[i].g, s->L[i].mask, s->st);
   VF_CHECK_LAUNCH();
+  return VF_OK;
+}
+
+// Per-level damping.  VF_OMEGA_FIXED: the reference's single omega.
+// VF_OMEGA_AUTO: omega_l = omega_rel * 2 / lambda_l, lambda_l from a power
+// iteration on D^-1 A_l (x <- D^-1 A x / ||.||), so the damped-Jacobi sweep
+// stays contractive on every level whatever the contrast (plain omega = 0.6
+// is divergent on high modes when lambda_max(D^-1 A) > 3.3, as on noise
+// geometry with void elements).
+int set_level_omegas(vf_solver* s) {
+  const int nl = nlev(s);
+  s->h_omega.assign(nl, s->o.omega);
+  s->h_lambda.assign(nl, 0.0);
+  if (s->o.omega_mode != VF_OMEGA_AUTO || !use_mg(s)) {
+    VF_TRY(cudaMemcpyAsync(s->d_omega, s->h_omega.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, s->st));
+    return VF_OK;
+  }
+  init_ks(*s->h_ks, 1.0, 1, 0, 0, 1.0);
+  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  for (int li = 0; li < nl; ++li) {
+    Level& l = s->L[li];
+    launch_power_init(l.g, l.w64[0], l.mask, s->st);
+    for (int k = 0; k < std::max(2, s->o.power_iters); ++k) {
+      level_op<double>(s, li, EPI_APPLY, l.w64[0], l.w64[1], nullptr, nullptr, nullptr, 0);
+      launch_power_scale(l.g, l.w64[1], l.minv64, s->d_partials, s->ks, s->st);
+      launch_power_normalize(l.g, l.w64[1], l.w64[0], s->ks, s->st);
+    }
+    launch_power_omega(s->ks, s->o.omega_rel, 1.1, s->d_omega + li, s->d_lambda + li, s->st);
+  }
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaMemcpyAsync(s->h_omega.data(), s->d_omega, sizeof(double) * nl, cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaMemcpyAsync(s->h_lambda.data(), s->d_lambda, sizeof(double) * nl, cudaMemcpyDeviceToHost, s->st));
   return VF_OK;
 }
 
@@ -599,6 +638,9 @@ void vf_options_default(vf_options* o) {
   o->max_outer = 20;
   o->omega = 0.6;
   o->inner_tol = 1e-4;
+  o->omega_mode = VF_OMEGA_FIXED;
+  o->power_iters = 20;
+  o->omega_rel = 0.8;
 }
 
 int vf_destroy(vf_solver* s) {
@@ -629,7 +671,8 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
     o = *opts;
   }
   if (o.precision < 0 || o.precision > 2 || o.method < 0 || o.method > 1 || o.coarse_op < 0 || o.coarse_op > 1 ||
-      o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0) {
+      o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0 ||
+      o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0) {
     g_last_error = "invalid vf_options field";
     return VF_ERR_ARG;
   }
@@ -664,6 +707,13 @@ const char* vf_last_error(const vf_solver* s) { return s ? s->err.c_str() : g_la
 int vf_num_levels(const vf_solver* s, int32_t* n) {
   if (!s || !n) return VF_ERR_ARG;
   *n = (int32_t)s->L.size();
+  return VF_OK;
+}
+
+int vf_level_omega(const vf_solver* s, int32_t level, double* omega, double* lambda) {
+  if (!s || level < 0 || level >= (int)s->h_omega.size()) return VF_ERR_ARG;
+  if (omega) *omega = s->h_omega[level];
+  if (lambda) *lambda = s->h_lambda[level];
   return VF_OK;
 }
 
@@ -771,6 +821,10 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
     launch_convert<double, float>(l.minv64, l.minv32, 3 * n, s->st);
   }
   VF_CHECK_LAUNCH();
+  {
+    int rc = set_level_omegas(s);
+    if (rc) return rc;
+  }
   if (use_mg(s) && s->o.coarsest == VF_COARSEST_CHOLESKY) {
     int rc = build_dense_coarsest(s);
     if (rc) return rc;
@@ -872,6 +926,7 @@ extern "C" int vf_solve_cb(vf_solver* s, const double* f, const double* x0, doub
     inf.converged = s->h_ks->status == KS_CONVERGED;
     inf.resid_ratio = s->h_ks->it > 0 ? s->h_ks->resid : std::numeric_limits<double>::quiet_NaN();
     status = map_status(s->h_ks->status);
+    s->last_best = s->h_ks->best;
   } else if (fp32) {
     // ---- FP32 vectors/operators, FP64 dots, no refinement ----
     float** v = s->k32;
@@ -958,11 +1013,11 @@ extern "C" int vf_solve_cb(vf_solver* s, const double* f, const double* x0, doub
   inf.status = status;
   if (info) *info = inf;
   if (status == VF_ERR_STALLED) {
-    char buf[256];
+    char buf[320];
     snprintf(buf, sizeof(buf),
              "MG-PCG stalled/diverged at iter %d (resid ratio %.3e, best seen %.3e) -- likely a small/thin "
              "essential-BC patch the coarse grid can't represent well",
-             inf.iters, inf.resid_ratio, s->h_ks->best);
+             inf.iters, inf.resid_ratio, s->last_best);
     s->err = buf;
   }
   return status;

@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256) k_stencil_op(Grid g, OpArgs a, const T* _
   const T* __restrict__ b = (const T*)a.b;
   const T* __restrict__ minv = (const T*)a.minv;
   const uint8_t* __restrict__ mask = a.mask;
-  const T w = (T)a.omega;
+  const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
   const int nx1 = g.lx + 1, ny1 = g.ly + 1;
   const int nint = nx1 * ny1 * (g.lz + 1);
   const long long n = g.n;

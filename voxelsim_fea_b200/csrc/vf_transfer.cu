@@ -97,9 +97,10 @@ __global__ void __launch_bounds__(256) k_prolong_add(Grid c, const T* __restrict
 
 template <typename T>
 __global__ void k_jacobi_from_zero(Grid g, const T* __restrict__ b, const T* __restrict__ minv,
-                                   const uint8_t* __restrict__ mask, T w, T* __restrict__ u,
-                                   const KrylovState* ks) {
+                                   const uint8_t* __restrict__ mask, T w0, const double* __restrict__ wdev,
+                                   T* __restrict__ u, const KrylovState* ks) {
   if (ks && ks->done) return;
+  const T w = wdev ? (T)(*wdev) : w0;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
     const uint8_t m = mask[p];
     const long long p3 = 3 * (long long)p;
@@ -135,14 +136,14 @@ void launch_prolong_add(const Grid& c, const T* ec, const Grid& f, const uint8_t
 }
 
 template <typename T>
-void launch_jacobi_from_zero(const Grid& g, const T* b, const T* minv3, const uint8_t* mask, double omega, T* u,
-                             const KrylovState* ks, cudaStream_t st) {
-  launch_k(k_jacobi_from_zero<T>, blocks_for(g.n), 256, 0, st, g, b, minv3, mask, (T)omega, u, ks);
+void launch_jacobi_from_zero(const Grid& g, const T* b, const T* minv3, const uint8_t* mask, double omega,
+                             const double* omega_dev, T* u, const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_jacobi_from_zero<T>, blocks_for(g.n), 256, 0, st, g, b, minv3, mask, (T)omega, omega_dev, u, ks);
 }
 
 template void launch_prolong_add<double>(const Grid&, const double*, const Grid&, const uint8_t*, double*, const KrylovState*, cudaStream_t);
 template void launch_prolong_add<float>(const Grid&, const float*, const Grid&, const uint8_t*, float*, const KrylovState*, cudaStream_t);
-template void launch_jacobi_from_zero<double>(const Grid&, const double*, const double*, const uint8_t*, double, double*, const KrylovState*, cudaStream_t);
-template void launch_jacobi_from_zero<float>(const Grid&, const float*, const float*, const uint8_t*, double, float*, const KrylovState*, cudaStream_t);
+template void launch_jacobi_from_zero<double>(const Grid&, const double*, const double*, const uint8_t*, double, const double*, double*, const KrylovState*, cudaStream_t);
+template void launch_jacobi_from_zero<float>(const Grid&, const float*, const float*, const uint8_t*, double, const double*, float*, const KrylovState*, cudaStream_t);
 
 }  // namespace vf

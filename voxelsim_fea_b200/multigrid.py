@@ -41,6 +41,9 @@ class SolverOptions:
     device: int = 0
     inner_tol: float = 1e-4          # mixed: residual reduction per inner solve
     max_outer: int = 20
+    omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
+    omega_rel: float = 0.8
+    power_iters: int = 20
 
     @classmethod
     def reference(cls, **kw):
@@ -49,15 +52,21 @@ class SolverOptions:
 
     @classmethod
     def robust(cls, **kw):
-        """FP64 Galerkin hierarchy with a direct coarsest solve ("plain GMG-PCG")."""
-        base = dict(coarse="galerkin", coarsest="cholesky")
+        """FP64 Galerkin hierarchy with a direct coarsest solve ("plain GMG-PCG").
+
+        The reference's stall guard (5x above the best ratio after 10
+        iterations) is off: it was tuned for the rediscretized hierarchy, and
+        the CG residual norm of a converging solve on high-contrast geometry is
+        not monotone."""
+        base = dict(coarse="galerkin", coarsest="cholesky", omega_mode="auto", stall_guard=False)
         base.update(kw)
         return cls(**base)
 
     @classmethod
     def fast(cls, **kw):
         """Galerkin hierarchy, mixed precision with FP64 refinement."""
-        base = dict(coarse="galerkin", coarsest="cholesky", precision="mixed")
+        base = dict(coarse="galerkin", coarsest="cholesky", precision="mixed", omega_mode="auto",
+                    stall_guard=False)
         base.update(kw)
         return cls(**base)
 
@@ -124,6 +133,9 @@ class MGSolver:
         o.device = int(self.options.device)
         o.inner_tol = float(self.options.inner_tol)
         o.max_outer = int(self.options.max_outer)
+        o.omega_mode = {"fixed": _lib.VF_OMEGA_FIXED, "auto": _lib.VF_OMEGA_AUTO}[self.options.omega_mode]
+        o.omega_rel = float(self.options.omega_rel)
+        o.power_iters = int(self.options.power_iters)
         h = ctypes.c_void_p()
         _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
                    None, "vf_create")
@@ -236,6 +248,13 @@ class MGSolver:
         _lib.check(_lib.load().vf_vcycle(self._handle(), _lib.PRECISIONS[precision], _lib.ptr(b),
                                          _lib.ptr(out)), self._h)
         return out
+
+    def level_omega(self, li):
+        """(omega, lambda_max estimate) of level li after set_density."""
+        w = ctypes.c_double()
+        lam = ctypes.c_double()
+        _lib.check(_lib.load().vf_level_omega(self._handle(), li, ctypes.byref(w), ctypes.byref(lam)), self._h)
+        return w.value, lam.value
 
     def inv_diagonal(self, li):
         """levels[li]['Minv'] (core/multigrid.py:300-304), 3 values per node."""
