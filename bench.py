@@ -115,6 +115,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# --------------------------------------------------------------------------- replicas
+def max_over_ranks(value, dist=None, device=None):
+    """Max of a per-rank float over the process group (identity without one).
+    Every rank calls it at the same point (timing is max over ranks)."""
+    if dist is None or not dist.is_initialized():
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # --------------------------------------------------------------------------- reference arm
 def cpu_sample_solve():
     """One reference-algorithm solve on the bounded CPU sample; returns (seconds, dof, iters)."""
@@ -238,23 +250,40 @@ def run_b200(args):
         ev1 = torch.cuda.Event(enable_timing=True)
         if sampler:
             sampler.start()
+        if args.nvtx:
+            torch.cuda.nvtx.range_push("vf_timed")
         ev0.record(ext)
         res = None
         for _ in range(steps):
             res = step(sv)
         ev1.record(ext)
+        if args.nvtx:
+            torch.cuda.synchronize()
+            torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         if dist:
             dist.barrier()
         s1 = ctypes.c_uint64()
         L.vf_launch_count(ctypes.byref(s1))
-        ms = ev0.elapsed_time(ev1) / steps
-        if dist:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / steps, dist, "cuda")
         return ms, res, clocks, int(s1.value - s0.value)
+
+    if args.kernel_profile:
+        # set-up once, then KERNEL alone inside an NVTX range (for ncu --nvtx-include "vf_kernel/")
+        kid = {"apply": 0, "smooth": 1, "resid": 2, "restrict": 3, "prolong": 4, "vcycle": 5}[args.kernel_profile]
+        prec = _lib.VF_PREC_FP64 if args.kernel_precision == "fp64" else _lib.VF_PREC_FP32
+        step(fast)
+        torch.cuda.synchronize()
+        kms = ctypes.c_double()
+        torch.cuda.nvtx.range_push("vf_kernel")
+        _lib.check(L.vf_time_kernel(fast._h, kid, prec, 3, ctypes.byref(kms)), fast._h)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"kernel": args.kernel_profile, "precision": args.kernel_precision,
+                          "ms_per_launch": kms.value, "workload": args.workload}), flush=True)
+        fast.close()
+        return 0
 
     sampler = ClockSampler(local) if rank == 0 else None
     ms, (iters, true_resid, outer), clocks, launches = timed(fast, args.steps, args.warmup, sampler)
@@ -310,11 +339,7 @@ def run_b200(args):
         for _ in range(ke):
             u_h = fast.solve(E_mg, f_h, tol=TOL)
         t1 = time.perf_counter()
-        ems = (t1 - t0) * 1e3 / ke
-        if dist:
-            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks((t1 - t0) * 1e3 / ke, dist, "cuda")
         e2e = {"value": world * ndof / (ems / 1e3) / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": int(8 * nelem + 8 * ndof), "d2h_bytes_per_step": int(8 * ndof),
                "ms_per_step": ems, "true_resid": float(fast.last_info.true_resid),
@@ -362,6 +387,10 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nvtx", action="store_true", help="wrap the timed steps in NVTX range vf_timed")
+    ap.add_argument("--kernel-profile", choices=("apply", "smooth", "resid", "restrict", "prolong", "vcycle"),
+                    help="set up, then run one kernel 3x inside NVTX range vf_kernel and exit")
+    ap.add_argument("--kernel-precision", choices=("fp32", "fp64"), default="fp32")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
