@@ -43,6 +43,7 @@ EXPORTS = (
     "vf_solve", "vf_solve_cb", "vf_resid_history", "vf_von_mises", "vf_strain_energy",
     "vf_drop_unsupported_islands", "vf_apply", "vf_smooth", "vf_restrict", "vf_prolongate",
     "vf_vcycle", "vf_inv_diagonal", "vf_time_kernel", "vf_get_stream", "vf_launch_count",
+    "vf_apply_noalloc",
 )
 
 
@@ -124,6 +125,7 @@ def _declare(L):
         "vf_time_kernel": (ctypes.c_int, [_P, _I32, _I32, _I32, _D]),
         "vf_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
         "vf_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64)]),
+        "vf_apply_noalloc": (ctypes.c_int, [_I32, _I32, _I32, ctypes.c_double, _P, _P, _P, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

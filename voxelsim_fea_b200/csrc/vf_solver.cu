@@ -42,9 +42,13 @@ void launch_strain_energy_tab(const Grid& g, const double* u_pad, const uint8_t*
 
 using namespace vf;
 
+namespace vf {
+thread_local std::string g_last_error;   // vf_global_last_error (shared with vf_noalloc.cu)
+}
+
 namespace {
 
-thread_local std::string g_last_error;
+using vf::g_last_error;
 std::atomic<unsigned long long> g_launches{0};
 
 // Kernel nodes of an instantiated chunk graph.
