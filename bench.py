@@ -221,7 +221,7 @@ def run_b200(args):
     def solver(opts):
         return MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=w["levels"], options=opts)
 
-    fast = solver(SolverOptions.fast(device=local, check_every=args.check_every))
+    fast = solver(SolverOptions.fast(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk))
     E_d = torch.from_numpy(np.ascontiguousarray(E_mg)).cuda()
     f_d = torch.from_numpy(np.ascontiguousarray(p["f"], dtype=np.float64)).cuda()
     u_d = torch.empty(ndof, dtype=torch.float64, device="cuda")
@@ -277,7 +277,7 @@ def run_b200(args):
         torch.cuda.synchronize()
         kms = ctypes.c_double()
         torch.cuda.nvtx.range_push("vf_kernel")
-        _lib.check(L.vf_time_kernel(fast._h, kid, prec, 3, ctypes.byref(kms)), fast._h)
+        _lib.check(L.vf_time_kernel(fast._h, kid, prec, args.kernel_iters, ctypes.byref(kms)), fast._h)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
         print(json.dumps({"kernel": args.kernel_profile, "precision": args.kernel_precision,
@@ -287,6 +287,10 @@ def run_b200(args):
 
     sampler = ClockSampler(local) if rank == 0 else None
     ms, (iters, true_resid, outer), clocks, launches = timed(fast, args.steps, args.warmup, sampler)
+    if not (true_resid < TOL):
+        # a solve that did not reach the tolerance is not a time-to-solution
+        raise SystemExit(f"bench: solve did not reach tol={TOL:g} (true residual {true_resid:.3e}, "
+                         f"{iters} iterations): no valid measurement")
     value = world * ndof / (ms / 1e3) / 1e6
 
     # plain FP64 GMG-PCG (same hierarchy, FP64 everywhere) on the same GPU
@@ -319,7 +323,7 @@ def run_b200(args):
     achieved = sweep_bytes / (kms.value / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None,
-                "kernel": "k_fine_op<float, EPI_SMOOTH> (fused damped-Jacobi sweep, level 0)",
+                "kernel": "k_modal_op<float, SMOOTH> (fused damped-Jacobi sweep, level 0)",
                 "ms_per_launch": kms.value, "algorithmic_bytes_per_launch": sweep_bytes,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650 GB/s",
                 "matvec_ms_per_launch": amv.value,
@@ -391,6 +395,8 @@ def main():
     ap.add_argument("--kernel-profile", choices=("apply", "smooth", "resid", "restrict", "prolong", "vcycle"),
                     help="set up, then run one kernel 3x inside NVTX range vf_kernel and exit")
     ap.add_argument("--kernel-precision", choices=("fp32", "fp64"), default="fp32")
+    ap.add_argument("--modal-zchunk", type=int, default=0, help="z-planes per CTA of the modal kernel (0 = auto)")
+    ap.add_argument("--kernel-iters", type=int, default=3, help="launches timed by --kernel-profile")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -90,10 +90,21 @@ typedef struct vf_options {
                               lambda_max(D^-1 A_l) taken at set_material */
   int32_t power_iters;     /* VF_OMEGA_AUTO: power iterations per level (20) */
   double  omega_rel;       /* VF_OMEGA_AUTO: fraction of the stability limit (0.8) */
+  int32_t fine_kernel;     /* VF_FINE_MODAL (default) | VF_FINE_GATHER: kernel of the
+                              element-operator levels (same operator, different form) */
+  int32_t modal_zchunk;    /* z-planes per CTA of the modal kernel; 0 = automatic */
+  int32_t coarse_storage;  /* Galerkin stencils as applied in the V-cycle:
+                              VF_STENCIL_SYM_HALF (default): symmetric, diagonally
+                              scaled, FP16 values for the FP32 V-cycle and FP64 for FP64;
+                              VF_STENCIL_SYM: symmetric scaled FP32 / FP64;
+                              VF_STENCIL_FULL: all 27 blocks, unscaled */
   int32_t reserved[8];
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
+enum { VF_FINE_MODAL = 0,     /* modal z-marching kernel (vf_modal.cu) */
+       VF_FINE_GATHER = 1 };  /* node-centric 27-neighbour gather (vf_matvec.cu) */
+enum { VF_STENCIL_SYM_HALF = 0, VF_STENCIL_SYM = 1, VF_STENCIL_FULL = 2 };
 
 typedef struct vf_solve_info {
   int32_t iters;           /* PCG iterations (all inner iterations for MIXED);

@@ -133,6 +133,13 @@ struct OpArgs {
   const double* omega_dev;  // device: damping of this level (overrides omega when set)
 };
 template <typename T> void launch_fine_op(const Grid& g, int epi, const OpArgs& a, cudaStream_t st);
+
+// vf_modal.cu -- the same operator in modal z-marching form (default).
+// Per-mode material factors: L_k = Elam * cL[k], M_k = Emu * cM[k].
+struct ModalConst { float cLf[3], cMf[3]; double cLd[3], cMd[3]; };
+ModalConst modal_constants(double nu, bool lame);
+template <typename T> void launch_modal_op(const Grid& g, int epi, const OpArgs& a, const ModalConst& mc, int ty,
+                                           int zchunk, cudaStream_t st);
 template <typename T> int fine_op_grid_blocks(const Grid& g);
 
 // vf_stencil.cu -- assembled 27-point block stencils (Galerkin levels)
@@ -154,7 +161,7 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
 template <typename T> void launch_dense_solve(const Grid& c, const double* Ainv, int n, const T* b, T* x, const KrylovState* ks, cudaStream_t st);
 
 // vf_krylov.cu -- fused PCG vector kernels with deterministic FP64 reductions
-constexpr int kVecBlocks = 148 * 4;     // grid of the vector kernels (fixed => deterministic)
+constexpr int kVecBlocks = 148 * 8;     // grid of the vector kernels (fixed => deterministic)
 constexpr int kVecThreads = 256;
 template <typename T> void launch_dot(const Grid& g, const T* a, const T* b, double* partials, KrylovState* ks, int slot, cudaStream_t st);
 template <typename T> void launch_cg_update(const Grid& g, T* x, const T* p, T* r, const T* Ap, double* partials, KrylovState* ks, double* hist, cudaStream_t st);

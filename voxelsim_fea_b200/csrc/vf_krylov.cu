@@ -10,13 +10,38 @@ namespace vf {
 
 namespace {
 
+// 16-byte vectors: padded vectors hold 3 * px * py * pz values with px a
+// multiple of 4, so their length is a multiple of 12 (and of 4 and 2).
+template <typename T> struct V16;
+template <> struct V16<float> {
+  using V = float4;
+  static constexpr int W = 4;
+  __device__ __forceinline__ static double dot(V a, V b) {
+    return (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+  }
+  __device__ __forceinline__ static V axpy(float s, V x, V y) {   // y + s x
+    return make_float4(fmaf(s, x.x, y.x), fmaf(s, x.y, y.y), fmaf(s, x.z, y.z), fmaf(s, x.w, y.w));
+  }
+};
+template <> struct V16<double> {
+  using V = double2;
+  static constexpr int W = 2;
+  __device__ __forceinline__ static double dot(V a, V b) { return a.x * b.x + a.y * b.y; }
+  __device__ __forceinline__ static V axpy(double s, V x, V y) { return make_double2(fma(s, x.x, y.x), fma(s, x.y, y.y)); }
+};
+
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_dot(long long n3, const T* __restrict__ a, const T* __restrict__ b,
                                                      double* partials, KrylovState* ks, int slot) {
   if (ks->done && slot != SLOT_FNORM && slot != SLOT_RZ_INIT && slot != SLOT_OUTER && slot != SLOT_PLAIN) return;
+  using H = V16<T>;
+  using V = typename H::V;
+  const long long nv = n3 / H::W;
+  const V* av = reinterpret_cast<const V*>(a);
+  const V* bv = reinterpret_cast<const V*>(b);
   double s = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
-    s += (double)a[i] * (double)b[i];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x)
+    s += H::dot(__ldg(av + i), __ldg(bv + i));
   reduce_and_finalize(s, partials, ks, slot, nullptr);
 }
 
@@ -25,13 +50,21 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_update(long long n3, T* __re
                                                            T* __restrict__ r, const T* __restrict__ Ap,
                                                            double* partials, KrylovState* ks, double* hist) {
   if (ks->done) return;
+  using H = V16<T>;
+  using V = typename H::V;
   const T alpha = (T)ks->alpha;
+  const long long nv = n3 / H::W;
+  V* xv = reinterpret_cast<V*>(x);
+  V* rv = reinterpret_cast<V*>(r);
+  const V* pv = reinterpret_cast<const V*>(p);
+  const V* av = reinterpret_cast<const V*>(Ap);
   double s = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
-    x[i] += alpha * p[i];
-    const T ri = r[i] - alpha * Ap[i];
-    r[i] = ri;
-    s += (double)ri * (double)ri;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const V pi = __ldg(pv + i), ai = __ldg(av + i);
+    xv[i] = H::axpy(alpha, pi, xv[i]);
+    const V ri = H::axpy(-alpha, ai, rv[i]);
+    rv[i] = ri;
+    s += H::dot(ri, ri);
   }
   reduce_and_finalize(s, partials, ks, SLOT_RR, hist);
 }
@@ -40,10 +73,15 @@ template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_p_update(long long n3, T* __restrict__ p, const T* __restrict__ z,
                                                           const KrylovState* ks) {
   if (ks->done) return;
+  using H = V16<T>;
+  using V = typename H::V;
   const bool restart = ks->restart != 0;
-  const T beta = (T)ks->beta;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
-    p[i] = restart ? z[i] : z[i] + beta * p[i];
+  const T beta = restart ? (T)0 : (T)ks->beta;
+  const long long nv = n3 / H::W;
+  V* pv = reinterpret_cast<V*>(p);
+  const V* zv = reinterpret_cast<const V*>(z);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x)
+    pv[i] = restart ? __ldg(zv + i) : H::axpy(beta, pv[i], __ldg(zv + i));
 }
 
 template <typename T>
@@ -62,8 +100,11 @@ __global__ void k_jacobi_precond(int n, const T* __restrict__ r, const T* __rest
 template <typename T>
 __global__ void k_copy(long long n3, const T* __restrict__ s, T* __restrict__ d, const KrylovState* ks) {
   if (ks && ks->done) return;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
-    d[i] = s[i];
+  const long long n16 = n3 * (long long)sizeof(T) / 16;   // 16-byte chunks
+  const float4* sv = reinterpret_cast<const float4*>(s);
+  float4* dv = reinterpret_cast<float4*>(d);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n16; i += (long long)gridDim.x * blockDim.x)
+    dv[i] = __ldg(sv + i);
 }
 
 // Mixed precision: r32 = r64 / ||r64|| (inner solves see a unit right-hand

@@ -30,17 +30,24 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Block-wide sum in a fixed order; valid in thread 0.  blockDim.x <= 1024.
+// Linear thread / block indices (kernels may use 2-D blocks and 3-D grids).
+__device__ __forceinline__ int lin_tid() { return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z); }
+__device__ __forceinline__ int lin_nthreads() { return blockDim.x * blockDim.y * blockDim.z; }
+__device__ __forceinline__ unsigned lin_bid() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+__device__ __forceinline__ unsigned lin_nblocks() { return gridDim.x * gridDim.y * gridDim.z; }
+
+// Block-wide sum in a fixed order; valid in thread 0.  <= 1024 threads, whole warps.
 __device__ __forceinline__ double block_sum(double v) {
   __shared__ double s_warp[32];
   v = warp_sum(v);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int t0 = lin_tid();
+  const int lane = t0 & 31, w = t0 >> 5;
   __syncthreads();
   if (lane == 0) s_warp[w] = v;
   __syncthreads();
   double t = 0.0;
   if (w == 0) {
-    t = (lane < (int)((blockDim.x + 31) >> 5)) ? s_warp[lane] : 0.0;
+    t = (lane < ((lin_nthreads() + 31) >> 5)) ? s_warp[lane] : 0.0;
     t = warp_sum(t);
   }
   return t;
@@ -91,24 +98,26 @@ __device__ inline void finalize_slot(KrylovState* ks, int slot, double total, do
 }
 
 // Called by every thread of every CTA with its own partial `v`.  The CTA sum
-// goes to partials[blockIdx.x]; the last CTA finalizes.
+// goes to partials[linear block id]; the last CTA finalizes.
 __device__ inline void reduce_and_finalize(double v, double* partials, KrylovState* ks, int slot,
                                            double* hist) {
   __shared__ bool s_last;
   double bsum = block_sum(v);
-  if (threadIdx.x == 0) {
-    partials[blockIdx.x] = bsum;
+  const int tid = lin_tid();
+  const unsigned nb = lin_nblocks();
+  if (tid == 0) {
+    partials[lin_bid()] = bsum;
     __threadfence();
     unsigned int prev = atomicAdd(&ks->counter[slot], 1u);
-    s_last = (prev == gridDim.x - 1);
+    s_last = (prev == nb - 1);
   }
   __syncthreads();
   if (!s_last) return;
   __threadfence();
   double t = 0.0;
-  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += ((volatile double*)partials)[i];
+  for (int i = tid; i < (int)nb; i += lin_nthreads()) t += ((volatile double*)partials)[i];
   t = block_sum(t);
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     finalize_slot(ks, slot, t, hist);
     ks->counter[slot] = 0u;
     __threadfence();

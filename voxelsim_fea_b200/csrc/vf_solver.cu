@@ -23,9 +23,14 @@
 #include "vf_common.cuh"
 #include "vf_hex8.h"
 #include "vf_reduce.cuh"
+#include <cuda_fp16.h>
 
 namespace vf {
 unsigned long long direct_launches();
+template <typename S, typename Q>
+void launch_stencil_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc, Q* sqrtd, cudaStream_t st_);
+template <typename T, typename S>
+void launch_stencil_sym_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st);
 // launchers defined in other translation units without a header entry
 void launch_elem_allfree(const Grid& f, const uint8_t* fmask, uint8_t* allfree, cudaStream_t st);
 void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu, const uint8_t* fmask,
@@ -67,10 +72,14 @@ unsigned long long graph_kernel_nodes(cudaGraph_t g) {
 
 struct Level {
   Grid g{};
+  int zchunk = 0;          // modal kernel: z-planes per CTA
   uint8_t* mask = nullptr;
   bool galerkin = false;   // operator is the assembled stencil
   double* E64 = nullptr; double* mu64 = nullptr; double* minv64 = nullptr; double* st64 = nullptr;
   float* E32 = nullptr; float* mu32 = nullptr; float* minv32 = nullptr; float* st32 = nullptr;
+  // symmetric scaled stencils (Galerkin levels): 123 values per node + sqrt(diag)
+  double* sym64 = nullptr; double* sq64 = nullptr;
+  float* sym32 = nullptr; __half* sym16 = nullptr; float* sq32 = nullptr;
   double* w64[4] = {nullptr, nullptr, nullptr, nullptr};   // x, tmp, resid, rhs
   float* w32[4] = {nullptr, nullptr, nullptr, nullptr};
 };
@@ -101,6 +110,7 @@ struct vf_solver {
   int nx = 0, ny = 0, nz = 0;
   std::vector<Level> L;
   double tab[1728];    // KE(nu) | K_lam | K_mu
+  vf::ModalConst mc{}, mc_lame{};
   double B0[144];
   double* d_Gtab = nullptr;   // Galerkin child tables (8 or 16 x 576)
   double* d_Ktab = nullptr;   // KE or K_lam|K_mu (576 or 1152)
@@ -203,6 +213,15 @@ int nlev(const vf_solver* s) { return use_mg(s) ? (int)s->L.size() : 1; }
 // ---------------------------------------------------------------------------
 // operator dispatch on one level
 // ---------------------------------------------------------------------------
+template <typename T> void level_sym_op(vf_solver* s, Level& l, int epi, const OpArgs& a);
+template <> void level_sym_op<double>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
+  launch_stencil_sym_op<double, double>(l.g, epi, a, l.sym64, l.sq64, s->st);
+}
+template <> void level_sym_op<float>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
+  if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) launch_stencil_sym_op<float, __half>(l.g, epi, a, l.sym16, l.sq32, s->st);
+  else launch_stencil_sym_op<float, float>(l.g, epi, a, l.sym32, l.sq32, s->st);
+}
+
 template <typename T>
 void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, KrylovState* ks, double* partials,
               int slot) {
@@ -219,8 +238,11 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
   a.ks = ks;
   a.dot_slot = slot;
   a.ke_tab = s->tab;
-  if (l.galerkin) launch_stencil_op<T>(l.g, epi, a, Sel<T>::st(l), s->st);
-  else launch_fine_op<T>(l.g, epi, a, s->st);
+  if (l.galerkin) {
+    if (s->o.coarse_storage == VF_STENCIL_FULL) launch_stencil_op<T>(l.g, epi, a, Sel<T>::st(l), s->st);
+    else level_sym_op<T>(s, l, epi, a);
+  } else if (s->o.fine_kernel == VF_FINE_GATHER) launch_fine_op<T>(l.g, epi, a, s->st);
+  else launch_modal_op<T>(l.g, epi, a, s->lame ? s->mc_lame : s->mc, 8, l.zchunk, s->st);
 }
 
 // `sweeps` damped-Jacobi sweeps on x (in place, through tmp); from_zero uses
@@ -433,7 +455,14 @@ int build_levels(vf_solver* s) {
       VF_ALLOC(l.E32, n);
     } else {
       VF_ALLOC(l.st64, 243 * n);
-      VF_ALLOC(l.st32, 243 * n);
+      if (s->o.coarse_storage == VF_STENCIL_FULL) VF_ALLOC(l.st32, 243 * n);
+      else {
+        VF_ALLOC(l.sym64, 123 * n);
+        VF_ALLOC(l.sq64, 3 * n);
+        VF_ALLOC(l.sq32, 3 * n);
+        if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) VF_ALLOC(l.sym16, 123 * n);
+        else VF_ALLOC(l.sym32, 123 * n);
+      }
     }
     for (int k = 0; k < 4; ++k) {
       VF_ALLOC(l.w64[k], 3 * n);
@@ -465,8 +494,23 @@ int build_levels(vf_solver* s) {
   return ensure_hist(s, 4096);
 }
 
+// z-planes per CTA of the modal kernel: about 4 CTAs per SM over the level
+// (22 planes measured best on the 256x128x128 fine level).
+int auto_zchunk(const Grid& g, int requested) {
+  if (requested > 0) return requested;
+  const long long tiles = (long long)((g.lx + 1 + 30) / 31) * ((g.ly + 1 + 6) / 7);
+  long long nz = (4LL * 148 + tiles - 1) / tiles;
+  if (nz < 1) nz = 1;
+  const int planes = g.lz + 1;
+  int zc = (int)((planes + nz - 1) / nz);
+  return zc < 2 ? 2 : zc;
+}
+
 int upload_tables(vf_solver* s) {
   hex8_tables(s->nu, s->tab, s->B0);
+  s->mc = vf::modal_constants(s->nu, false);
+  s->mc_lame = vf::modal_constants(s->nu, true);
+  for (auto& l : s->L) l.zchunk = auto_zchunk(l.g, s->o.modal_zchunk);
   std::vector<double> G(8 * 576), GL(16 * 576);
   galerkin_child_tables(s->tab, G.data());
   galerkin_child_tables(s->tab + 576, GL.data());
@@ -645,6 +689,9 @@ void vf_options_default(vf_options* o) {
   o->omega_mode = VF_OMEGA_FIXED;
   o->power_iters = 20;
   o->omega_rel = 0.8;
+  o->fine_kernel = VF_FINE_MODAL;
+  o->modal_zchunk = 0;
+  o->coarse_storage = VF_STENCIL_SYM_HALF;
 }
 
 int vf_destroy(vf_solver* s) {
@@ -676,7 +723,9 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
   }
   if (o.precision < 0 || o.precision > 2 || o.method < 0 || o.method > 1 || o.coarse_op < 0 || o.coarse_op > 1 ||
       o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0 ||
-      o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0) {
+      o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0 ||
+      o.fine_kernel < 0 || o.fine_kernel > 1 || o.modal_zchunk < 0 || o.coarse_storage < 0 ||
+      o.coarse_storage > 2) {
     g_last_error = "invalid vf_options field";
     return VF_ERR_ARG;
   }
@@ -819,8 +868,14 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
     if (!l.galerkin) {
       launch_convert<double, float>(l.E64, l.E32, n, s->st);
       if (lame) launch_convert<double, float>(l.mu64, l.mu32, n, s->st);
-    } else {
+    } else if (s->o.coarse_storage == VF_STENCIL_FULL) {
       launch_convert<double, float>(l.st64, l.st32, 243 * n, s->st);
+    } else {
+      launch_stencil_compress<double, double>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+      if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
+        launch_stencil_compress<__half, float>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
+      else
+        launch_stencil_compress<float, float>(l.g, l.st64, l.mask, l.sym32, l.sq32, s->st);
     }
     launch_convert<double, float>(l.minv64, l.minv32, 3 * n, s->st);
   }

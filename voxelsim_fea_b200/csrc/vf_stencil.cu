@@ -22,6 +22,10 @@
 //   * galerkin_from_stencil: level l -> l+1 for l >= 1 (stencil RAP).
 //   * stencil_mask_and_diag: D_{l+1} = {DOFs with a non-zero Galerkin
 //     diagonal}; zero their rows/columns; Jacobi inverse diagonal.
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
 #include "vf_common.cuh"
 #include "vf_reduce.cuh"
 
@@ -414,5 +418,169 @@ void launch_galerkin_mask(const Grid& c, double* stencil, uint8_t* cmask, double
 void launch_stencil_diag(const Grid& c, double* stencil, const uint8_t* cmask, double* minv3, cudaStream_t st) {
   launch_k(k_apply_mask_diag, blocks_for(c.n, 256), 256, 0, st, c, stencil, cmask, minv3);
 }
+
+// ---------------------------------------------------------------------------
+// Compressed symmetric stencil (the operator of the Galerkin levels as the
+// V-cycle applies it).
+//
+// A Galerkin operator is symmetric, so only the diagonal block (6 values) and
+// the 13 "upper" neighbour blocks (offsets s = 14..26, 9 values each) are
+// stored: 123 values per node; the 13 lower blocks are read transposed from
+// the neighbour that stores them.  Values are the symmetrically scaled
+// A~ = D^-1/2 A D^-1/2 (unit diagonal, |entries| <= 1 for an SPD operator), so
+// half precision keeps its relative precision over any stiffness contrast;
+// the apply computes y = D^1/2 A~ (D^1/2 u) with sqrtd = D^1/2 per DOF (0 on
+// non-free DOFs).  Layout SoA: stc[k * n + p], k in [0, 123):
+//   k = 0..5   diagonal block (r,c) = (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
+//   k = 6 + 9*(s-14) + 3*r + c   upper block s, DOF r of p with DOF c of p+off(s)
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename S> __device__ __forceinline__ S st_from(double v);
+template <> __device__ __forceinline__ float st_from<float>(double v) { return (float)v; }
+template <> __device__ __forceinline__ double st_from<double>(double v) { return v; }
+template <> __device__ __forceinline__ __half st_from<__half>(double v) { return __double2half(v); }
+__device__ __forceinline__ float st_to(float v) { return v; }
+__device__ __forceinline__ double st_to(double v) { return v; }
+__device__ __forceinline__ float st_to(__half v) { return __half2float(v); }
+__device__ __forceinline__ int diag_r(int k) { return k < 3 ? 0 : (k < 5 ? 1 : 2); }
+__device__ __forceinline__ int diag_c(int k) { return k < 3 ? k : (k < 5 ? k - 2 : 2); }
+
+template <typename S, typename Q>
+__global__ void k_stencil_compress(Grid g, const double* __restrict__ st, const uint8_t* __restrict__ mask,
+                                   S* __restrict__ stc, Q* __restrict__ sqrtd) {
+  const long long n = g.n;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(g, p, x, y, z);
+    const bool inside = (x >= 0 && x <= g.lx && y >= 0 && y <= g.ly && z >= 0 && z <= g.lz);
+    double sp[3];
+    for (int r = 0; r < 3; ++r) {
+      const double d = st[((long long)13 * 9 + r * 4) * n + p];
+      sp[r] = (inside && ((mask[p] >> r) & 1) && d > 0.0) ? 1.0 / sqrt(d) : 0.0;
+      sqrtd[3 * (long long)p + r] = (Q)(sp[r] > 0.0 ? 1.0 / sp[r] : 0.0);
+    }
+    for (int k = 0; k < 6; ++k) {
+      const int r = diag_r(k), c = diag_c(k);
+      stc[(long long)k * n + p] = st_from<S>(st[((long long)13 * 9 + r * 3 + c) * n + p] * sp[r] * sp[c]);
+    }
+    for (int s = 14; s < 27; ++s) {
+      const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+      double sq[3] = {0.0, 0.0, 0.0};
+      if (inside) {
+        const int q = g.idx(x + dx, y + dy, z + dz);
+        for (int c = 0; c < 3; ++c) {
+          const double d = st[((long long)13 * 9 + c * 4) * n + q];
+          sq[c] = (((mask[q] >> c) & 1) && d > 0.0) ? 1.0 / sqrt(d) : 0.0;
+        }
+      }
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+          const double v = inside ? st[((long long)s * 9 + r * 3 + c) * n + p] * sp[r] * sq[c] : 0.0;
+          stc[(long long)(6 + 9 * (s - 14) + 3 * r + c) * n + p] = st_from<S>(v);
+        }
+    }
+  }
+}
+
+template <typename T, typename S, int EPI>
+__global__ void __launch_bounds__(256) k_stencil_sym_op(Grid g, OpArgs a, const S* __restrict__ stc,
+                                                        const T* __restrict__ sqd) {
+  KrylovState* ks = a.ks;
+  if (ks && ks->done) return;
+  using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
+  const T* __restrict__ u = (const T*)a.u;
+  T* __restrict__ out = (T*)a.out;
+  const T* __restrict__ b = (const T*)a.b;
+  const T* __restrict__ minv = (const T*)a.minv;
+  const uint8_t* __restrict__ mask = a.mask;
+  const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
+  const int nx1 = g.lx + 1, ny1 = g.ly + 1;
+  const int nint = nx1 * ny1 * (g.lz + 1);
+  const long long n = g.n;
+  double dot = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int x = t % nx1;
+    const int rr = t / nx1;
+    const int y = rr % ny1;
+    const int z = rr / ny1;
+    const int p = g.idx(x, y, z);
+    A a0, a1, a2;
+    {
+      const long long p3 = 3 * (long long)p;
+      const A v0 = (A)__ldg(sqd + p3) * (A)__ldg(u + p3), v1 = (A)__ldg(sqd + p3 + 1) * (A)__ldg(u + p3 + 1);
+      const A v2 = (A)__ldg(sqd + p3 + 2) * (A)__ldg(u + p3 + 2);
+      const A d00 = st_to(__ldg(stc + p)), d01 = st_to(__ldg(stc + n + p)), d02 = st_to(__ldg(stc + 2 * n + p));
+      const A d11 = st_to(__ldg(stc + 3 * n + p)), d12 = st_to(__ldg(stc + 4 * n + p));
+      const A d22 = st_to(__ldg(stc + 5 * n + p));
+      a0 = d00 * v0 + d01 * v1 + d02 * v2;
+      a1 = d01 * v0 + d11 * v1 + d12 * v2;
+      a2 = d02 * v0 + d12 * v1 + d22 * v2;
+    }
+#pragma unroll
+    for (int s = 14; s < 27; ++s) {
+      const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+      const int kb = 6 + 9 * (s - 14);
+      {  // upper neighbour q = p + off(s): own block
+        const long long q3 = 3 * (long long)g.idx(x + dx, y + dy, z + dz);
+        const A v0 = (A)__ldg(sqd + q3) * (A)__ldg(u + q3), v1 = (A)__ldg(sqd + q3 + 1) * (A)__ldg(u + q3 + 1);
+        const A v2 = (A)__ldg(sqd + q3 + 2) * (A)__ldg(u + q3 + 2);
+        const S* B = stc + (long long)kb * n + p;
+        a0 += st_to(__ldg(B)) * v0 + st_to(__ldg(B + n)) * v1 + st_to(__ldg(B + 2 * n)) * v2;
+        a1 += st_to(__ldg(B + 3 * n)) * v0 + st_to(__ldg(B + 4 * n)) * v1 + st_to(__ldg(B + 5 * n)) * v2;
+        a2 += st_to(__ldg(B + 6 * n)) * v0 + st_to(__ldg(B + 7 * n)) * v1 + st_to(__ldg(B + 8 * n)) * v2;
+      }
+      {  // lower neighbour q = p - off(s): its block s couples q -> p; apply the transpose
+        const int q = g.idx(x - dx, y - dy, z - dz);
+        const long long q3 = 3 * (long long)q;
+        const A v0 = (A)__ldg(sqd + q3) * (A)__ldg(u + q3), v1 = (A)__ldg(sqd + q3 + 1) * (A)__ldg(u + q3 + 1);
+        const A v2 = (A)__ldg(sqd + q3 + 2) * (A)__ldg(u + q3 + 2);
+        const S* B = stc + (long long)kb * n + q;
+        a0 += st_to(__ldg(B)) * v0 + st_to(__ldg(B + 3 * n)) * v1 + st_to(__ldg(B + 6 * n)) * v2;
+        a1 += st_to(__ldg(B + n)) * v0 + st_to(__ldg(B + 4 * n)) * v1 + st_to(__ldg(B + 7 * n)) * v2;
+        a2 += st_to(__ldg(B + 2 * n)) * v0 + st_to(__ldg(B + 5 * n)) * v1 + st_to(__ldg(B + 8 * n)) * v2;
+      }
+    }
+    const uint8_t m = mask[p];
+    const long long p3 = 3 * (long long)p;
+    const T k0 = (m & 1) ? (T)(a0 * (A)sqd[p3]) : (T)0;
+    const T k1 = (m & 2) ? (T)(a1 * (A)sqd[p3 + 1]) : (T)0;
+    const T k2 = (m & 4) ? (T)(a2 * (A)sqd[p3 + 2]) : (T)0;
+    if (EPI == EPI_APPLY) {
+      out[p3] = k0; out[p3 + 1] = k1; out[p3 + 2] = k2;
+      if (a.dot_partials)
+        dot += (double)u[p3] * (double)k0 + (double)u[p3 + 1] * (double)k1 + (double)u[p3 + 2] * (double)k2;
+    } else if (EPI == EPI_SMOOTH) {
+      const T r0 = b[p3] - k0, r1 = b[p3 + 1] - k1, r2 = b[p3 + 2] - k2;
+      out[p3] = u[p3] + ((m & 1) ? w * (minv[p3] * r0) : (T)0);
+      out[p3 + 1] = u[p3 + 1] + ((m & 2) ? w * (minv[p3 + 1] * r1) : (T)0);
+      out[p3 + 2] = u[p3 + 2] + ((m & 4) ? w * (minv[p3 + 2] * r2) : (T)0);
+    } else {
+      out[p3] = b[p3] - k0; out[p3 + 1] = b[p3 + 1] - k1; out[p3 + 2] = b[p3 + 2] - k2;
+    }
+  }
+  if (EPI == EPI_APPLY && a.dot_partials && ks) reduce_and_finalize(dot, a.dot_partials, ks, a.dot_slot, nullptr);
+}
+
+}  // namespace
+
+template <typename S, typename Q>
+void launch_stencil_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc, Q* sqrtd, cudaStream_t st_) {
+  launch_k(k_stencil_compress<S, Q>, blocks_for(g.n, 256), 256, 0, st_, g, st, mask, stc, sqrtd);
+}
+template void launch_stencil_compress<__half, float>(const Grid&, const double*, const uint8_t*, __half*, float*, cudaStream_t);
+template void launch_stencil_compress<float, float>(const Grid&, const double*, const uint8_t*, float*, float*, cudaStream_t);
+template void launch_stencil_compress<double, double>(const Grid&, const double*, const uint8_t*, double*, double*, cudaStream_t);
+
+template <typename T, typename S>
+void launch_stencil_sym_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
+  const int blocks = stencil_op_grid_blocks<T>(g);
+  if (epi == EPI_APPLY) launch_k(k_stencil_sym_op<T, S, EPI_APPLY>, blocks, 256, 0, st, g, a, stc, sqrtd);
+  else if (epi == EPI_SMOOTH) launch_k(k_stencil_sym_op<T, S, EPI_SMOOTH>, blocks, 256, 0, st, g, a, stc, sqrtd);
+  else launch_k(k_stencil_sym_op<T, S, EPI_RESID>, blocks, 256, 0, st, g, a, stc, sqrtd);
+}
+template void launch_stencil_sym_op<float, __half>(const Grid&, int, const OpArgs&, const __half*, const float*, cudaStream_t);
+template void launch_stencil_sym_op<float, float>(const Grid&, int, const OpArgs&, const float*, const float*, cudaStream_t);
+template void launch_stencil_sym_op<double, double>(const Grid&, int, const OpArgs&, const double*, const double*, cudaStream_t);
 
 }  // namespace vf
