@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <type_traits>
 #include <utility>
 
 namespace vf {
@@ -145,6 +146,23 @@ template <typename T> int fine_op_grid_blocks(const Grid& g);
 // vf_stencil.cu -- assembled 27-point block stencils (Galerkin levels)
 template <typename T> void launch_stencil_op(const Grid& g, int epi, const OpArgs& a, const T* stencil, cudaStream_t st);
 template <typename T> int stencil_op_grid_blocks(const Grid& g);
+// Warp-chunked storage of the symmetric scaled stencil (128 values per node,
+// 123 used): value k of node p at off(p, k) in units of S.  Chunk j (16 bytes)
+// of 32 consecutive nodes is contiguous.  Q: type of the D^1/2 scale vector.
+template <typename S> struct SymLayout {
+  static constexpr int VPC = 16 / (int)sizeof(S);
+  static constexpr int NCH = 128 / VPC;
+  using Q = typename std::conditional<sizeof(S) == 8, double, float>::type;
+  __host__ __device__ static constexpr long long off(long long p, int k) {
+    return ((p >> 5) * NCH + k / VPC) * (32LL * VPC) + (p & 31) * VPC + (k % VPC);
+  }
+  static size_t count(long long n) { return (size_t)((n + 31) / 32) * 32 * 128; }
+};
+template <typename S> void launch_stencil_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc,
+                                                   typename SymLayout<S>::Q* sqrtd, cudaStream_t st_);
+template <typename T, typename S> void launch_stencil_sym_op(const Grid& g, int epi, const OpArgs& a, const S* stc,
+                                                             const T* sqrtd, int zchunk, cudaStream_t st);
+int sym_zchunk(const Grid& g);
 void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu, const uint8_t* fmask,
                                const Grid& c, double* stencil_c, const double* Gtab, int lame, cudaStream_t st);
 void launch_galerkin_from_stencil(const Grid& f, const double* stencil_f, const Grid& c, double* stencil_c, cudaStream_t st);

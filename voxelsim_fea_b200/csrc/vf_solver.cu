@@ -27,10 +27,6 @@
 
 namespace vf {
 unsigned long long direct_launches();
-template <typename S, typename Q>
-void launch_stencil_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc, Q* sqrtd, cudaStream_t st_);
-template <typename T, typename S>
-void launch_stencil_sym_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st);
 // launchers defined in other translation units without a header entry
 void launch_elem_allfree(const Grid& f, const uint8_t* fmask, uint8_t* allfree, cudaStream_t st);
 void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu, const uint8_t* fmask,
@@ -73,6 +69,7 @@ unsigned long long graph_kernel_nodes(cudaGraph_t g) {
 struct Level {
   Grid g{};
   int zchunk = 0;          // modal kernel: z-planes per CTA
+  int szchunk = 0;         // marching stencil kernel: z-planes per CTA
   uint8_t* mask = nullptr;
   bool galerkin = false;   // operator is the assembled stencil
   double* E64 = nullptr; double* mu64 = nullptr; double* minv64 = nullptr; double* st64 = nullptr;
@@ -215,11 +212,12 @@ int nlev(const vf_solver* s) { return use_mg(s) ? (int)s->L.size() : 1; }
 // ---------------------------------------------------------------------------
 template <typename T> void level_sym_op(vf_solver* s, Level& l, int epi, const OpArgs& a);
 template <> void level_sym_op<double>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
-  launch_stencil_sym_op<double, double>(l.g, epi, a, l.sym64, l.sq64, s->st);
+  launch_stencil_sym_op<double, double>(l.g, epi, a, l.sym64, l.sq64, l.szchunk, s->st);
 }
 template <> void level_sym_op<float>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
-  if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) launch_stencil_sym_op<float, __half>(l.g, epi, a, l.sym16, l.sq32, s->st);
-  else launch_stencil_sym_op<float, float>(l.g, epi, a, l.sym32, l.sq32, s->st);
+  if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
+    launch_stencil_sym_op<float, __half>(l.g, epi, a, l.sym16, l.sq32, l.szchunk, s->st);
+  else launch_stencil_sym_op<float, float>(l.g, epi, a, l.sym32, l.sq32, l.szchunk, s->st);
 }
 
 template <typename T>
@@ -457,11 +455,11 @@ int build_levels(vf_solver* s) {
       VF_ALLOC(l.st64, 243 * n);
       if (s->o.coarse_storage == VF_STENCIL_FULL) VF_ALLOC(l.st32, 243 * n);
       else {
-        VF_ALLOC(l.sym64, 123 * n);
+        VF_ALLOC(l.sym64, SymLayout<double>::count(n));
         VF_ALLOC(l.sq64, 3 * n);
         VF_ALLOC(l.sq32, 3 * n);
-        if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) VF_ALLOC(l.sym16, 123 * n);
-        else VF_ALLOC(l.sym32, 123 * n);
+        if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) VF_ALLOC(l.sym16, SymLayout<__half>::count(n));
+        else VF_ALLOC(l.sym32, SymLayout<float>::count(n));
       }
     }
     for (int k = 0; k < 4; ++k) {
@@ -510,7 +508,10 @@ int upload_tables(vf_solver* s) {
   hex8_tables(s->nu, s->tab, s->B0);
   s->mc = vf::modal_constants(s->nu, false);
   s->mc_lame = vf::modal_constants(s->nu, true);
-  for (auto& l : s->L) l.zchunk = auto_zchunk(l.g, s->o.modal_zchunk);
+  for (auto& l : s->L) {
+    l.zchunk = auto_zchunk(l.g, s->o.modal_zchunk);
+    l.szchunk = sym_zchunk(l.g);
+  }
   std::vector<double> G(8 * 576), GL(16 * 576);
   galerkin_child_tables(s->tab, G.data());
   galerkin_child_tables(s->tab + 576, GL.data());
@@ -871,11 +872,11 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
     } else if (s->o.coarse_storage == VF_STENCIL_FULL) {
       launch_convert<double, float>(l.st64, l.st32, 243 * n, s->st);
     } else {
-      launch_stencil_compress<double, double>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+      launch_stencil_compress<double>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
       if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
-        launch_stencil_compress<__half, float>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
+        launch_stencil_compress<__half>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
       else
-        launch_stencil_compress<float, float>(l.g, l.st64, l.mask, l.sym32, l.sq32, s->st);
+        launch_stencil_compress<float>(l.g, l.st64, l.mask, l.sym32, l.sq32, s->st);
     }
     launch_convert<double, float>(l.minv64, l.minv32, 3 * n, s->st);
   }

@@ -420,8 +420,7 @@ void launch_stencil_diag(const Grid& c, double* stencil, const uint8_t* cmask, d
 }
 
 // ---------------------------------------------------------------------------
-// Compressed symmetric stencil (the operator of the Galerkin levels as the
-// V-cycle applies it).
+// Symmetric, diagonally scaled Galerkin stencils (default coarse storage).
 //
 // A Galerkin operator is symmetric, so only the diagonal block (6 values) and
 // the 13 "upper" neighbour blocks (offsets s = 14..26, 9 values each) are
@@ -430,9 +429,13 @@ void launch_stencil_diag(const Grid& c, double* stencil, const uint8_t* cmask, d
 // A~ = D^-1/2 A D^-1/2 (unit diagonal, |entries| <= 1 for an SPD operator), so
 // half precision keeps its relative precision over any stiffness contrast;
 // the apply computes y = D^1/2 A~ (D^1/2 u) with sqrtd = D^1/2 per DOF (0 on
-// non-free DOFs).  Layout SoA: stc[k * n + p], k in [0, 123):
+// non-free DOFs).  Value order within a node, k in [0, 128):
 //   k = 0..5   diagonal block (r,c) = (0,0) (0,1) (0,2) (1,1) (1,2) (2,2)
 //   k = 6 + 9*(s-14) + 3*r + c   upper block s, DOF r of p with DOF c of p+off(s)
+//   k = 123..127 zero padding
+// Storage is warp-chunked (SymLayout): 16-byte chunk j of 32 consecutive nodes
+// is contiguous, so a warp loads a chunk of its 32 nodes in one 512-byte
+// transaction whatever the alignment of its first node.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -440,15 +443,14 @@ template <typename S> __device__ __forceinline__ S st_from(double v);
 template <> __device__ __forceinline__ float st_from<float>(double v) { return (float)v; }
 template <> __device__ __forceinline__ double st_from<double>(double v) { return v; }
 template <> __device__ __forceinline__ __half st_from<__half>(double v) { return __double2half(v); }
-__device__ __forceinline__ float st_to(float v) { return v; }
-__device__ __forceinline__ double st_to(double v) { return v; }
-__device__ __forceinline__ float st_to(__half v) { return __half2float(v); }
-__device__ __forceinline__ int diag_r(int k) { return k < 3 ? 0 : (k < 5 ? 1 : 2); }
-__device__ __forceinline__ int diag_c(int k) { return k < 3 ? k : (k < 5 ? k - 2 : 2); }
+__host__ __device__ constexpr int diag_r(int k) { return k < 3 ? 0 : (k < 5 ? 1 : 2); }
+__host__ __device__ constexpr int diag_c(int k) { return k < 3 ? k : (k < 5 ? k - 2 : 2); }
 
-template <typename S, typename Q>
+template <typename S>
 __global__ void k_stencil_compress(Grid g, const double* __restrict__ st, const uint8_t* __restrict__ mask,
-                                   S* __restrict__ stc, Q* __restrict__ sqrtd) {
+                                   S* __restrict__ stc, typename SymLayout<S>::Q* __restrict__ sqrtd) {
+  using L = SymLayout<S>;
+  using Q = typename L::Q;
   const long long n = g.n;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
     int x, y, z;
@@ -462,7 +464,7 @@ __global__ void k_stencil_compress(Grid g, const double* __restrict__ st, const 
     }
     for (int k = 0; k < 6; ++k) {
       const int r = diag_r(k), c = diag_c(k);
-      stc[(long long)k * n + p] = st_from<S>(st[((long long)13 * 9 + r * 3 + c) * n + p] * sp[r] * sp[c]);
+      stc[L::off(p, k)] = st_from<S>(st[((long long)13 * 9 + r * 3 + c) * n + p] * sp[r] * sp[c]);
     }
     for (int s = 14; s < 27; ++s) {
       const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
@@ -477,75 +479,175 @@ __global__ void k_stencil_compress(Grid g, const double* __restrict__ st, const 
       for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) {
           const double v = inside ? st[((long long)s * 9 + r * 3 + c) * n + p] * sp[r] * sq[c] : 0.0;
-          stc[(long long)(6 + 9 * (s - 14) + 3 * r + c) * n + p] = st_from<S>(v);
+          stc[L::off(p, 6 + 9 * (s - 14) + 3 * r + c)] = st_from<S>(v);
         }
     }
+    for (int k = 123; k < 128; ++k) stc[L::off(p, k)] = st_from<S>(0.0);
   }
 }
 
+// One 16-byte chunk of stencil values, unpacked to the accumulation type.
+template <typename S, typename A> struct Chunk;
+template <> struct Chunk<__half, float> {
+  float v[8];
+  __device__ __forceinline__ void load(const __half* base) {
+    const uint4 w = __ldg(reinterpret_cast<const uint4*>(base));
+    const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      __half2 h;
+      memcpy(&h, &ws[i], 4);
+      const float2 f = __half22float2(h);
+      v[2 * i] = f.x; v[2 * i + 1] = f.y;
+    }
+  }
+};
+template <> struct Chunk<float, float> {
+  float v[4];
+  __device__ __forceinline__ void load(const float* base) {
+    const float4 w = __ldg(reinterpret_cast<const float4*>(base));
+    v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
+  }
+};
+template <> struct Chunk<double, double> {
+  double v[2];
+  __device__ __forceinline__ void load(const double* base) {
+    const double2 w = __ldg(reinterpret_cast<const double2*>(base));
+    v[0] = w.x; v[1] = w.y;
+  }
+};
+
+constexpr int SX = 32, SY = 8;   // node tile of the marching stencil kernel
+
+// y = mask(D^1/2 A~ D^1/2 u) with the epilogues of the fine operator.  A CTA
+// owns a 32 x 8 tile of node columns and marches along z over `zchunk`
+// planes; v = D^1/2 u of the halo tile lives in a 4-plane shared ring (one
+// barrier per plane: the slot written for plane z+1 was last read two steps
+// earlier), the next plane is prefetched into registers while the current one
+// is computed, and the stencil values stream through coalesced 16-byte loads.
 template <typename T, typename S, int EPI>
-__global__ void __launch_bounds__(256) k_stencil_sym_op(Grid g, OpArgs a, const S* __restrict__ stc,
-                                                        const T* __restrict__ sqd) {
+__global__ void __launch_bounds__(SX * SY, 2) k_sym_march(Grid g, OpArgs a, const S* __restrict__ stc,
+                                                           const T* __restrict__ sqd, int zchunk) {
+  using Lay = SymLayout<S>;
+  using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
+  constexpr int VPC = Lay::VPC;
+  constexpr int HX = SX + 2, HY = SY + 2, NH = HX * HY;
+  constexpr int NTH = SX * SY;
+  constexpr int NL = (NH + NTH - 1) / NTH;
+  __shared__ A vs[4][3][HY][HX];
+
   KrylovState* ks = a.ks;
   if (ks && ks->done) return;
-  using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
   const T* __restrict__ u = (const T*)a.u;
   T* __restrict__ out = (T*)a.out;
   const T* __restrict__ b = (const T*)a.b;
   const T* __restrict__ minv = (const T*)a.minv;
   const uint8_t* __restrict__ mask = a.mask;
   const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
-  const int nx1 = g.lx + 1, ny1 = g.ly + 1;
-  const int nint = nx1 * ny1 * (g.lz + 1);
-  const long long n = g.n;
-  double dot = 0.0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
-    const int x = t % nx1;
-    const int rr = t / nx1;
-    const int y = rr % ny1;
-    const int z = rr / ny1;
-    const int p = g.idx(x, y, z);
-    A a0, a1, a2;
-    {
-      const long long p3 = 3 * (long long)p;
-      const A v0 = (A)__ldg(sqd + p3) * (A)__ldg(u + p3), v1 = (A)__ldg(sqd + p3 + 1) * (A)__ldg(u + p3 + 1);
-      const A v2 = (A)__ldg(sqd + p3 + 2) * (A)__ldg(u + p3 + 2);
-      const A d00 = st_to(__ldg(stc + p)), d01 = st_to(__ldg(stc + n + p)), d02 = st_to(__ldg(stc + 2 * n + p));
-      const A d11 = st_to(__ldg(stc + 3 * n + p)), d12 = st_to(__ldg(stc + 4 * n + p));
-      const A d22 = st_to(__ldg(stc + 5 * n + p));
-      a0 = d00 * v0 + d01 * v1 + d02 * v2;
-      a1 = d01 * v0 + d11 * v1 + d12 * v2;
-      a2 = d02 * v0 + d12 * v1 + d22 * v2;
+
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SX + tx;
+  const int X0 = blockIdx.x * SX, Y0 = blockIdx.y * SY;
+  const int zb = blockIdx.z * zchunk;
+  const int ze = min(zb + zchunk, g.lz + 1);
+  const int sz = g.px * g.py;
+  const int x = X0 + tx, y = Y0 + ty;
+  const bool active = (x <= g.lx) && (y <= g.ly);
+
+  // halo elements of this thread: in-plane storage offset (or -1)
+  int hoff[NL];
+  int hsl[NL];
+#pragma unroll
+  for (int q = 0; q < NL; ++q) {
+    const int e = tid + q * NTH;
+    const int i = e % HX, j = e / HX;
+    const int xs = X0 + i, ys = Y0 + j;   // storage coordinates (x + 1, y + 1)
+    hsl[q] = e < NH ? e : -1;
+    hoff[q] = (e < NH && xs < g.px && ys < g.py) ? ys * g.px + xs : -1;
+  }
+  A pv[NL][3];
+  auto fetch = [&](int zz) {   // logical plane zz in [-1, lz + 1]
+#pragma unroll
+    for (int q = 0; q < NL; ++q) {
+      const bool ok = hoff[q] >= 0;
+      const long long p3 = ok ? 3LL * ((long long)(zz + 1) * sz + hoff[q]) : 0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pv[q][c] = ok ? (A)__ldg(sqd + p3 + c) * (A)__ldg(u + p3 + c) : (A)0;
     }
+  };
+  auto store = [&](int zz) {
+    const int slot = (zz + 1) & 3;
+#pragma unroll
+    for (int q = 0; q < NL; ++q)
+      if (hsl[q] >= 0) {
+        const int i = hsl[q] % HX, j = hsl[q] / HX;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) vs[slot][c][j][i] = pv[q][c];
+      }
+  };
+
+  double dot = 0.0;
+  fetch(zb - 1);
+  store(zb - 1);
+  fetch(zb);
+  store(zb);
+  if (zb + 1 <= g.lz + 1) fetch(zb + 1);
+#pragma unroll 1
+  for (int z = zb; z < ze; ++z) {
+    store(z + 1);                         // plane z+1 <= lz+1 always (z <= lz)
+    if (z + 2 <= g.lz + 1) fetch(z + 2);
+    __syncthreads();
+    if (!active) continue;
+    const int p = g.idx(x, y, z);
+    const int s0 = (z + 1) & 3;
+    auto V = [&](int dx, int dy, int dz, int c) -> A {
+      return vs[(s0 + dz + 4) & 3][c][ty + 1 + dy][tx + 1 + dx];
+    };
+    A acc[3] = {(A)0, (A)0, (A)0};
+    // own values: diagonal block and the 13 upper blocks
+    const S* own = stc + Lay::off(p, 0);
+#pragma unroll
+    for (int j = 0; j < 123 / VPC + 1; ++j) {
+      Chunk<S, A> ch;
+      ch.load(own + (long long)j * 32 * VPC);
+#pragma unroll
+      for (int i = 0; i < VPC; ++i) {
+        const int k = j * VPC + i;
+        if (k < 6) {
+          const int r = diag_r(k), c = diag_c(k);
+          acc[r] += ch.v[i] * V(0, 0, 0, c);
+          if (r != c) acc[c] += ch.v[i] * V(0, 0, 0, r);
+        } else if (k < 123) {
+          const int s = 14 + (k - 6) / 9, rc = (k - 6) % 9;
+          acc[rc / 3] += ch.v[i] * V(s % 3 - 1, (s / 3) % 3 - 1, s / 9 - 1, rc % 3);
+        }
+      }
+    }
+    // lower blocks: block s of q = p - off(s), transposed
 #pragma unroll
     for (int s = 14; s < 27; ++s) {
       const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
-      const int kb = 6 + 9 * (s - 14);
-      {  // upper neighbour q = p + off(s): own block
-        const long long q3 = 3 * (long long)g.idx(x + dx, y + dy, z + dz);
-        const A v0 = (A)__ldg(sqd + q3) * (A)__ldg(u + q3), v1 = (A)__ldg(sqd + q3 + 1) * (A)__ldg(u + q3 + 1);
-        const A v2 = (A)__ldg(sqd + q3 + 2) * (A)__ldg(u + q3 + 2);
-        const S* B = stc + (long long)kb * n + p;
-        a0 += st_to(__ldg(B)) * v0 + st_to(__ldg(B + n)) * v1 + st_to(__ldg(B + 2 * n)) * v2;
-        a1 += st_to(__ldg(B + 3 * n)) * v0 + st_to(__ldg(B + 4 * n)) * v1 + st_to(__ldg(B + 5 * n)) * v2;
-        a2 += st_to(__ldg(B + 6 * n)) * v0 + st_to(__ldg(B + 7 * n)) * v1 + st_to(__ldg(B + 8 * n)) * v2;
-      }
-      {  // lower neighbour q = p - off(s): its block s couples q -> p; apply the transpose
-        const int q = g.idx(x - dx, y - dy, z - dz);
-        const long long q3 = 3 * (long long)q;
-        const A v0 = (A)__ldg(sqd + q3) * (A)__ldg(u + q3), v1 = (A)__ldg(sqd + q3 + 1) * (A)__ldg(u + q3 + 1);
-        const A v2 = (A)__ldg(sqd + q3 + 2) * (A)__ldg(u + q3 + 2);
-        const S* B = stc + (long long)kb * n + q;
-        a0 += st_to(__ldg(B)) * v0 + st_to(__ldg(B + 3 * n)) * v1 + st_to(__ldg(B + 6 * n)) * v2;
-        a1 += st_to(__ldg(B + n)) * v0 + st_to(__ldg(B + 4 * n)) * v1 + st_to(__ldg(B + 7 * n)) * v2;
-        a2 += st_to(__ldg(B + 2 * n)) * v0 + st_to(__ldg(B + 5 * n)) * v1 + st_to(__ldg(B + 8 * n)) * v2;
+      const int q = p - ((dz * g.py + dy) * g.px + dx);
+      const int k0 = 6 + 9 * (s - 14);
+      const S* base = stc + Lay::off(q, 0);
+#pragma unroll
+      for (int j = k0 / VPC; j <= (k0 + 8) / VPC; ++j) {
+        Chunk<S, A> ch;
+        ch.load(base + (long long)j * 32 * VPC);
+#pragma unroll
+        for (int i = 0; i < VPC; ++i) {
+          const int k = j * VPC + i;
+          if (k >= k0 && k < k0 + 9) {
+            const int r = (k - k0) / 3, c = (k - k0) % 3;
+            acc[c] += ch.v[i] * V(-dx, -dy, -dz, r);
+          }
+        }
       }
     }
     const uint8_t m = mask[p];
     const long long p3 = 3 * (long long)p;
-    const T k0 = (m & 1) ? (T)(a0 * (A)sqd[p3]) : (T)0;
-    const T k1 = (m & 2) ? (T)(a1 * (A)sqd[p3 + 1]) : (T)0;
-    const T k2 = (m & 4) ? (T)(a2 * (A)sqd[p3 + 2]) : (T)0;
+    const T k0 = (m & 1) ? (T)(acc[0] * (A)sqd[p3]) : (T)0;
+    const T k1 = (m & 2) ? (T)(acc[1] * (A)sqd[p3 + 1]) : (T)0;
+    const T k2 = (m & 4) ? (T)(acc[2] * (A)sqd[p3 + 2]) : (T)0;
     if (EPI == EPI_APPLY) {
       out[p3] = k0; out[p3 + 1] = k1; out[p3 + 2] = k2;
       if (a.dot_partials)
@@ -564,23 +666,36 @@ __global__ void __launch_bounds__(256) k_stencil_sym_op(Grid g, OpArgs a, const 
 
 }  // namespace
 
-template <typename S, typename Q>
-void launch_stencil_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc, Q* sqrtd, cudaStream_t st_) {
-  launch_k(k_stencil_compress<S, Q>, blocks_for(g.n, 256), 256, 0, st_, g, st, mask, stc, sqrtd);
+template <typename S>
+void launch_stencil_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc,
+                             typename SymLayout<S>::Q* sqrtd, cudaStream_t st_) {
+  launch_k(k_stencil_compress<S>, blocks_for(g.n, 256), 256, 0, st_, g, st, mask, stc, sqrtd);
 }
-template void launch_stencil_compress<__half, float>(const Grid&, const double*, const uint8_t*, __half*, float*, cudaStream_t);
-template void launch_stencil_compress<float, float>(const Grid&, const double*, const uint8_t*, float*, float*, cudaStream_t);
-template void launch_stencil_compress<double, double>(const Grid&, const double*, const uint8_t*, double*, double*, cudaStream_t);
+template void launch_stencil_compress<__half>(const Grid&, const double*, const uint8_t*, __half*, float*, cudaStream_t);
+template void launch_stencil_compress<float>(const Grid&, const double*, const uint8_t*, float*, float*, cudaStream_t);
+template void launch_stencil_compress<double>(const Grid&, const double*, const uint8_t*, double*, double*, cudaStream_t);
+
+// z-planes per CTA of the marching stencil kernel: about 4 CTAs per SM.
+int sym_zchunk(const Grid& g) {
+  const long long tiles = (long long)((g.lx + 1 + SX - 1) / SX) * ((g.ly + 1 + SY - 1) / SY);
+  long long nz = (4LL * 148 + tiles - 1) / tiles;
+  if (nz < 1) nz = 1;
+  const int planes = g.lz + 1;
+  return (int)((planes + nz - 1) / nz);
+}
 
 template <typename T, typename S>
-void launch_stencil_sym_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
-  const int blocks = stencil_op_grid_blocks<T>(g);
-  if (epi == EPI_APPLY) launch_k(k_stencil_sym_op<T, S, EPI_APPLY>, blocks, 256, 0, st, g, a, stc, sqrtd);
-  else if (epi == EPI_SMOOTH) launch_k(k_stencil_sym_op<T, S, EPI_SMOOTH>, blocks, 256, 0, st, g, a, stc, sqrtd);
-  else launch_k(k_stencil_sym_op<T, S, EPI_RESID>, blocks, 256, 0, st, g, a, stc, sqrtd);
+void launch_stencil_sym_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, int zchunk,
+                           cudaStream_t st) {
+  if (zchunk < 1) zchunk = sym_zchunk(g);
+  const dim3 grid((g.lx + 1 + SX - 1) / SX, (g.ly + 1 + SY - 1) / SY, (g.lz + 1 + zchunk - 1) / zchunk);
+  const dim3 block(SX, SY);
+  if (epi == EPI_APPLY) launch_k(k_sym_march<T, S, EPI_APPLY>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
+  else if (epi == EPI_SMOOTH) launch_k(k_sym_march<T, S, EPI_SMOOTH>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
+  else launch_k(k_sym_march<T, S, EPI_RESID>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
 }
-template void launch_stencil_sym_op<float, __half>(const Grid&, int, const OpArgs&, const __half*, const float*, cudaStream_t);
-template void launch_stencil_sym_op<float, float>(const Grid&, int, const OpArgs&, const float*, const float*, cudaStream_t);
-template void launch_stencil_sym_op<double, double>(const Grid&, int, const OpArgs&, const double*, const double*, cudaStream_t);
+template void launch_stencil_sym_op<float, __half>(const Grid&, int, const OpArgs&, const __half*, const float*, int, cudaStream_t);
+template void launch_stencil_sym_op<float, float>(const Grid&, int, const OpArgs&, const float*, const float*, int, cudaStream_t);
+template void launch_stencil_sym_op<double, double>(const Grid&, int, const OpArgs&, const double*, const double*, int, cudaStream_t);
 
 }  // namespace vf
