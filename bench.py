@@ -221,7 +221,10 @@ def run_b200(args):
     def solver(opts):
         return MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=w["levels"], options=opts)
 
-    fast = solver(SolverOptions.fast(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk))
+    fkw = dict(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk, mixed_mode=args.mixed_mode)
+    if args.inner_tol is not None:
+        fkw["inner_tol"] = args.inner_tol
+    fast = solver(SolverOptions.fast(**fkw))
     E_d = torch.from_numpy(np.ascontiguousarray(E_mg)).cuda()
     f_d = torch.from_numpy(np.ascontiguousarray(p["f"], dtype=np.float64)).cuda()
     u_d = torch.empty(ndof, dtype=torch.float64, device="cuda")
@@ -397,6 +400,9 @@ def main():
     ap.add_argument("--kernel-precision", choices=("fp32", "fp64"), default="fp32")
     ap.add_argument("--modal-zchunk", type=int, default=0, help="z-planes per CTA of the modal kernel (0 = auto)")
     ap.add_argument("--kernel-iters", type=int, default=3, help="launches timed by --kernel-profile")
+    ap.add_argument("--mixed-mode", choices=("reliable", "restart"), default="reliable")
+    ap.add_argument("--inner-tol", type=float, default=None,
+                    help="mixed: residual reduction between FP64 corrections (solver default if unset)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -83,7 +83,9 @@ typedef struct vf_options {
   int32_t device;          /* CUDA device ordinal                           */
   int32_t max_outer;       /* VF_PREC_MIXED: refinement steps cap           */
   double  omega;           /* Jacobi damping (multigrid.py:86, default 0.6) */
-  double  inner_tol;       /* VF_PREC_MIXED: residual reduction per inner solve */
+  double  inner_tol;       /* VF_PREC_MIXED: residual reduction between FP64 corrections
+                              (1e-2; the FP32 recurrence residual runs ahead of the
+                              true one by up to 100x below ~1e-4 of its start)   */
   int32_t omega_mode;      /* VF_OMEGA_FIXED: omega on every level (reference);
                               VF_OMEGA_AUTO: omega_l = omega_rel * 2 / lambda_l with
                               lambda_l a power-iteration estimate of
@@ -98,18 +100,25 @@ typedef struct vf_options {
                               scaled, FP16 values for the FP32 V-cycle and FP64 for FP64;
                               VF_STENCIL_SYM: symmetric scaled FP32 / FP64;
                               VF_STENCIL_FULL: all 27 blocks, unscaled */
-  int32_t reserved[8];
+  int32_t mixed_mode;      /* VF_PREC_MIXED: VF_MIXED_RELIABLE (default): one FP32 CG whose
+                              residual is replaced by the FP64 true residual (and the FP32
+                              increment folded into the FP64 solution) each time it has
+                              dropped by inner_tol; VF_MIXED_RESTART: iterative refinement,
+                              a fresh FP32 PCG per outer step */
+  int32_t reserved[7];
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
 enum { VF_FINE_MODAL = 0,     /* modal z-marching kernel (vf_modal.cu) */
        VF_FINE_GATHER = 1 };  /* node-centric 27-neighbour gather (vf_matvec.cu) */
 enum { VF_STENCIL_SYM_HALF = 0, VF_STENCIL_SYM = 1, VF_STENCIL_FULL = 2 };
+enum { VF_MIXED_RELIABLE = 0, VF_MIXED_RESTART = 1 };
 
 typedef struct vf_solve_info {
   int32_t iters;           /* PCG iterations (all inner iterations for MIXED);
                               MGSolver.last_iters (multigrid.py:515)        */
-  int32_t outer_iters;     /* refinement steps (MIXED), else 0              */
+  int32_t outer_iters;     /* MIXED: residual replacements (RELIABLE) or
+                              refinement steps (RESTART), else 0            */
   int32_t converged;       /* MGSolver.last_converged                       */
   int32_t status;          /* VF_OK, VF_ERR_STALLED, VF_ERR_BREAKDOWN, ...   */
   double  resid_ratio;     /* MGSolver.last_resid_ratio (recurrence, or the

@@ -32,6 +32,7 @@ VF_SOLVE_DEVICE_PTRS = 1
 VF_OMEGA_FIXED, VF_OMEGA_AUTO = 0, 1
 VF_FINE_MODAL, VF_FINE_GATHER = 0, 1
 STENCIL_STORAGE = {"sym_half": 0, "sym": 1, "full": 2}
+MIXED_MODES = {"reliable": 0, "restart": 1}
 
 PRECISIONS = {"fp64": VF_PREC_FP64, "mixed": VF_PREC_MIXED, "fp32": VF_PREC_FP32}
 COARSE_OPS = {"rediscretize": VF_COARSE_REDISCRETIZE, "galerkin": VF_COARSE_GALERKIN}
@@ -62,8 +63,8 @@ class VfOptions(ctypes.Structure):
         ("omega_mode", ctypes.c_int32), ("power_iters", ctypes.c_int32),
         ("omega_rel", ctypes.c_double),
         ("fine_kernel", ctypes.c_int32), ("modal_zchunk", ctypes.c_int32),
-        ("coarse_storage", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 8),
+        ("coarse_storage", ctypes.c_int32), ("mixed_mode", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
 

@@ -84,6 +84,7 @@ struct KrylovState {
   double best;      // stall guard: best ratio seen
   double scale;     // mixed: the residual scale of the current inner solve
   double hist_scale;
+  double rr_trigger;  // > 0: stop the chunk (KS_RELIABLE) once rr drops below it
   int it;           // iterations completed (this solve)
   int it_base;      // history offset (mixed: inner iterations before this solve)
   int max_it;
@@ -96,7 +97,7 @@ struct KrylovState {
 };
 
 enum KState { KS_RUNNING = 0, KS_CONVERGED = 1, KS_MAXIT = 2, KS_STALLED = 3,
-              KS_BREAKDOWN = 4, KS_NONFINITE = 5 };
+              KS_BREAKDOWN = 4, KS_NONFINITE = 5, KS_RELIABLE = 6 };
 
 // ----------------------------------------------------------------------------
 // Launchers (defined in the .cu files; all asynchronous on `st`).
@@ -189,6 +190,7 @@ template <typename T> void launch_copy_vec(const Grid& g, const T* src, T* dst, 
 void launch_norm2_f64(const Grid& g, const double* v, double* partials, KrylovState* ks, int slot, cudaStream_t st);
 void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState* ks, cudaStream_t st);
 void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const KrylovState* ks, cudaStream_t st);
+void launch_ir_replace(const Grid& g, const double* r64, float* r32, const KrylovState* ks, cudaStream_t st);
 void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st);
 // power iteration on D^-1 A (per-level damping)
 void launch_power_init(const Grid& g, double* x, const uint8_t* mask, cudaStream_t st);

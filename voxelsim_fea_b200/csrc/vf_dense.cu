@@ -197,8 +197,16 @@ __global__ void k_dense_solve(Grid c, const double* __restrict__ Ainv, int n, co
   const int wpb = blockDim.x >> 5;
   for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
     const double* row = Ainv + (long long)i * n;
-    double s = 0.0;
-    for (int j = lane; j < n; j += 32) s += row[j] * sb[j];
+    // eight independent partial sums keep eight 256-byte row segments in
+    // flight per warp (the GEMV streams n^2 doubles per call)
+    double part[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int j = lane;
+    for (; j + 7 * 32 < n; j += 8 * 32) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) part[k] += __ldg(row + j + 32 * k) * sb[j + 32 * k];
+    }
+    for (; j < n; j += 32) part[7] += __ldg(row + j) * sb[j];
+    double s = ((part[0] + part[1]) + (part[2] + part[3])) + ((part[4] + part[5]) + (part[6] + part[7]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) {

@@ -124,6 +124,15 @@ __global__ void k_ir_accumulate(long long n3, double* __restrict__ x64, const fl
     x64[i] += s * (double)d32[i];
 }
 
+// r32 = r64 / scale with the scale fixed for the whole mixed solve
+__global__ void k_ir_replace(long long n3, const double* __restrict__ r64, float* __restrict__ r32,
+                             const KrylovState* ks) {
+  const double s = ks->scale;
+  const double inv = s > 0.0 ? 1.0 / s : 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    r32[i] = (float)(r64[i] * inv);
+}
+
 __global__ void k_sub_from(long long n3, const double* __restrict__ f, double* __restrict__ r) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
     r[i] = f[i] - r[i];
@@ -216,6 +225,9 @@ void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState
 }
 void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const KrylovState* ks, cudaStream_t st) {
   launch_k(k_ir_accumulate, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x64, d32, ks);
+}
+void launch_ir_replace(const Grid& g, const double* r64, float* r32, const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_ir_replace, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r64, r32, ks);
 }
 void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st) {
   launch_k(k_sub_from, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, f, r);

@@ -80,6 +80,7 @@ __device__ inline void finalize_slot(KrylovState* ks, int slot, double total, do
       if (ks->stall_guard && it >= 10 && ratio > 5.0 * ks->best) {
         ks->done = 1; ks->status = KS_STALLED; break;
       }
+      if (total < ks->rr_trigger) { ks->done = 1; ks->status = KS_RELIABLE; break; }
       if (it >= ks->max_it) { ks->done = 1; ks->status = KS_MAXIT; }
       break;
     }

@@ -77,16 +77,22 @@ __global__ void __launch_bounds__(256) k_prolong_add(Grid c, const T* __restrict
     const int p = f.idx(x, y, z);
     const uint8_t m = fm[p];
     if (!m) continue;
+    // all eight coarse corners, weight 0 on the unused ones: the loads are
+    // independent (one latency) and x0+1 <= c.lx+1 stays on the padded grid
     const int x0 = x >> 1, y0 = y >> 1, z0 = z >> 1;
-    const int nxs = (x & 1) + 1, nys = (y & 1) + 1, nzs = (z & 1) + 1;
-    const T wx = (x & 1) ? (T)0.5 : (T)1, wy = (y & 1) ? (T)0.5 : (T)1, wz = (z & 1) ? (T)0.5 : (T)1;
+    const T wx[2] = {(x & 1) ? (T)0.5 : (T)1, (x & 1) ? (T)0.5 : (T)0};
+    const T wy[2] = {(y & 1) ? (T)0.5 : (T)1, (y & 1) ? (T)0.5 : (T)0};
+    const T wz[2] = {(z & 1) ? (T)0.5 : (T)1, (z & 1) ? (T)0.5 : (T)0};
     T e0 = 0, e1 = 0, e2 = 0;
-    for (int kz = 0; kz < nzs; ++kz)
-      for (int ky = 0; ky < nys; ++ky)
-        for (int kx = 0; kx < nxs; ++kx) {
-          const T w = wx * wy * wz;
+#pragma unroll
+    for (int kz = 0; kz < 2; ++kz)
+#pragma unroll
+      for (int ky = 0; ky < 2; ++ky)
+#pragma unroll
+        for (int kx = 0; kx < 2; ++kx) {
+          const T w = wx[kx] * wy[ky] * wz[kz];
           const long long q = 3 * (long long)c.idx(x0 + kx, y0 + ky, z0 + kz);
-          e0 += w * ec[q]; e1 += w * ec[q + 1]; e2 += w * ec[q + 2];
+          e0 += w * __ldg(ec + q); e1 += w * __ldg(ec + q + 1); e2 += w * __ldg(ec + q + 2);
         }
     const long long p3 = 3 * (long long)p;
     if (m & 1) uf[p3] += e0;

@@ -39,8 +39,9 @@ class SolverOptions:
     check_every: int = 8             # PCG iterations per device graph launch
     use_graphs: bool = True
     device: int = 0
-    inner_tol: float = 1e-4          # mixed: residual reduction per inner solve
-    max_outer: int = 20
+    inner_tol: float = 1e-2          # mixed: residual reduction between FP64 corrections
+    max_outer: int = 20              # mixed: cap on FP64 corrections
+    mixed_mode: str = "reliable"     # mixed: "reliable" (residual replacement) | "restart" (refinement)
     omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
     omega_rel: float = 0.8
     power_iters: int = 20
@@ -142,6 +143,7 @@ class MGSolver:
         o.fine_kernel = {"modal": _lib.VF_FINE_MODAL, "gather": _lib.VF_FINE_GATHER}[self.options.fine_kernel]
         o.modal_zchunk = int(self.options.modal_zchunk)
         o.coarse_storage = _lib.STENCIL_STORAGE[self.options.coarse_storage]
+        o.mixed_mode = _lib.MIXED_MODES[self.options.mixed_mode]
         h = ctypes.c_void_p()
         _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
                    None, "vf_create")
