@@ -273,6 +273,35 @@ int vf_apply_noalloc(int32_t nx, int32_t ny, int32_t nz, double nu, const double
                      const uint8_t* free_mask, const double* u, double* y, double* u_dot_y,
                      void* stream);
 
+/* ---- learned preconditioner stage: BF16 tensor-core 3x3x3 convolutions --------
+ * No counterpart in the reference (its solver has no learned part).  Building
+ * blocks of the U-Net trained by voxelsim_fea_b200.learned and run inside the
+ * flexible-CG preconditioner.  All pointers are device pointers; tensors are
+ * channels-last BF16 boxes [Z][Y][X][C], zero-padded ("same" convolution);
+ * weights [27][cout][cin] BF16 with tap = (dz+1)*9 + (dy+1)*3 + (dx+1)
+ * (cross-correlation, the torch conv3d convention).  FP32 accumulation on the
+ * tensor cores.  (cin, cout) in {(16,16) (16,32) (32,16) (32,32) (32,64)
+ * (64,32) (64,64)}; other pairs return VF_ERR_ARG.  `stream`: cudaStream_t. */
+/* out = relu?(conv(in, w) + bias + skip); bias (FP32, cout), skip (BF16, cout
+ * channels) optional; out_f32 non-NULL writes FP32 instead of BF16 `out`. */
+int vf_nn_conv3d_forward(const void* in, const void* w, const float* bias, const void* skip,
+                         int32_t relu, void* out, float* out_f32, int32_t X, int32_t Y, int32_t Z,
+                         int32_t cin, int32_t cout, void* stream);
+/* dx = conv^T(dy) * (gate > 0 if gate): the data gradient of a layer with cin
+ * inputs and cout outputs; w_t [27][cin][cout] is w with its taps mirrored and
+ * its channel axes swapped; gate (BF16, cin channels) is the layer input saved
+ * in the forward pass when that input came out of a ReLU. */
+int vf_nn_conv3d_backward_data(const void* dy, const void* w_t, const void* gate, void* dx,
+                               int32_t X, int32_t Y, int32_t Z, int32_t cin, int32_t cout,
+                               void* stream);
+/* dw[27][cout][cin] (FP32) (+)= sum_v dy[v][co] x[v + off(tap)][ci]; work is a
+ * caller-provided scratch of vf_nn_wgrad_workspace() bytes (deterministic
+ * per-CTA partial sums, reduced in a fixed order). */
+int vf_nn_conv3d_backward_weight(const void* x, const void* dy, float* dw, int32_t accumulate,
+                                 float* work, size_t work_bytes, int32_t X, int32_t Y, int32_t Z,
+                                 int32_t cin, int32_t cout, void* stream);
+size_t vf_nn_wgrad_workspace(int32_t cin, int32_t cout, int32_t X, int32_t Y, int32_t Z);
+
 #ifdef __cplusplus
 }
 #endif

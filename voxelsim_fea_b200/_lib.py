@@ -47,6 +47,8 @@ EXPORTS = (
     "vf_drop_unsupported_islands", "vf_apply", "vf_smooth", "vf_restrict", "vf_prolongate",
     "vf_vcycle", "vf_inv_diagonal", "vf_time_kernel", "vf_get_stream", "vf_launch_count",
     "vf_apply_noalloc",
+    "vf_nn_conv3d_forward", "vf_nn_conv3d_backward_data", "vf_nn_conv3d_backward_weight",
+    "vf_nn_wgrad_workspace",
 )
 
 
@@ -131,6 +133,11 @@ def _declare(L):
         "vf_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_void_p)]),
         "vf_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint64)]),
         "vf_apply_noalloc": (ctypes.c_int, [_I32, _I32, _I32, ctypes.c_double, _P, _P, _P, _P, _P, _P]),
+        "vf_nn_conv3d_forward": (ctypes.c_int, [_P, _P, _P, _P, _I32, _P, _P, _I32, _I32, _I32, _I32, _I32, _P]),
+        "vf_nn_conv3d_backward_data": (ctypes.c_int, [_P, _P, _P, _P, _I32, _I32, _I32, _I32, _I32, _P]),
+        "vf_nn_conv3d_backward_weight": (ctypes.c_int, [_P, _P, _P, _I32, _P, ctypes.c_size_t, _I32, _I32, _I32,
+                                                        _I32, _I32, _P]),
+        "vf_nn_wgrad_workspace": (ctypes.c_size_t, [_I32, _I32, _I32, _I32, _I32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
