@@ -310,6 +310,24 @@ def run_b200(args):
                  "mdof_per_s": ndof / (pms / 1e3) / 1e6, "speedup_of_mixed": pms / ms}
         ps.close()
 
+    # learned stage + mixed precision (flexible CG with the U-Net stage after
+    # each V-cycle), packaged weights; reported beside the mixed solver
+    learned = None
+    if not args.no_learned:
+        from voxelsim_fea_b200.learned import stage
+        ls = solver(SolverOptions.fast(**fkw))
+        stage.enable_default(ls)
+        L.vf_get_stream(ls._h, ctypes.byref(stream_ptr))
+        ext_save = ext
+        ext = torch.cuda.ExternalStream(stream_ptr.value)
+        lms, (lit, lres, lout), _, _ = timed(ls, max(1, args.steps // 2), 1)
+        ext = ext_save
+        learned = {"ms_per_solve": lms, "iterations": lit, "true_resid": lres, "corrections": lout,
+                   "mdof_per_s": ndof / (lms / 1e3) / 1e6,
+                   "speedup_vs_plain_fp64": (plain["ms_per_solve"] / lms) if plain else None,
+                   "converged": bool(lres < TOL)}
+        ls.close()
+
     # roofline of the dominant kernel: fused FP32 Jacobi sweep on the fine level
     nodes = (nx + 1) * (ny + 1) * (nz + 1)
     kms = ctypes.c_double()
@@ -324,8 +342,11 @@ def run_b200(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = sweep_bytes / (kms.value / 1e3) / 1e9
+    # DRAM traffic of one launch from the ncu capture summarised in
+    # profiles/k_modal_op_smooth_fp32_bracket256.md (read + write, same workload)
+    traffic = 188.54e6 + 34.62e6
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
+                "frac": achieved / peak, "traffic": traffic, "traffic_unit": "B per launch (ncu)",
                 "kernel": "k_modal_op<float, SMOOTH> (fused damped-Jacobi sweep, level 0)",
                 "ms_per_launch": kms.value, "algorithmic_bytes_per_launch": sweep_bytes,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650 GB/s",
@@ -370,6 +391,7 @@ def run_b200(args):
             "iterations": iters, "outer_iterations": outer, "true_resid": true_resid,
             "time_to_solution_s": ms / 1e3,
             "plain_fp64": plain,
+            "learned_mixed": learned,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -392,6 +414,7 @@ def main():
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="bracket_256x128x128")
     ap.add_argument("--check-every", type=int, default=8)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-stage arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nvtx", action="store_true", help="wrap the timed steps in NVTX range vf_timed")

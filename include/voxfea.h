@@ -105,7 +105,10 @@ typedef struct vf_options {
                               increment folded into the FP64 solution) each time it has
                               dropped by inner_tol; VF_MIXED_RESTART: iterative refinement,
                               a fresh FP32 PCG per outer step */
-  int32_t reserved[7];
+  int32_t flexible;        /* 1: flexible CG (Notay's FCG(1): beta = -z.Ap / p.Ap), which
+                              stays correct for a preconditioner that varies between
+                              iterations; always on while a learned stage is enabled */
+  int32_t reserved[6];
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
@@ -301,6 +304,38 @@ int vf_nn_conv3d_backward_weight(const void* x, const void* dy, float* dw, int32
                                  float* work, size_t work_bytes, int32_t X, int32_t Y, int32_t Z,
                                  int32_t cin, int32_t cout, void* stream);
 size_t vf_nn_wgrad_workspace(int32_t cin, int32_t cout, int32_t X, int32_t Y, int32_t Z);
+
+/* The learned stage inside the solver's preconditioner: after the V-cycle,
+ *   z += P^L NN(R^L (r - A z))
+ * with NN the 3-level U-Net (10 convolutions, see vf_learned.cu) run on the
+ * node grid of hierarchy level L (>= 1) padded to multiples of 4; its input is
+ * the restricted residual scaled by its RMS, the occupancy and the normalised
+ * log-modulus of the voxels around each node; its output (x RMS / Eref, Eref
+ * the largest voxel modulus) is the level-L correction.  Enabling it switches
+ * the iteration to flexible CG.  Parameters: per layer W[27][cout][cin] then
+ * b[cout], FP32, vf_learned_param_count() values. */
+int64_t vf_learned_param_count(void);
+/* Create the stage on `level` (re-created if the level changes), upload
+ * `params` when non-NULL, and enable (enable = 1) or disable it. */
+int vf_learned_configure(vf_solver* s, int32_t level, const float* params, int64_t n_params,
+                         int32_t enable);
+/* dims3: the U-Net grid (X, Y, Z); level: the hierarchy level it runs on. */
+int vf_learned_info(const vf_solver* s, int32_t* dims3, int32_t* level);
+/* The U-Net input for a level-L residual given on the host in the reference
+ * node layout of level L: written to in_dev (device, BF16 [Z][Y][X][16]);
+ * *scale_out = the residual RMS, *eref_out = Eref.  For training. */
+int vf_learned_input(vf_solver* s, const double* r_level, void* in_dev, float* scale_out,
+                     double* eref_out);
+/* The whole stage on host arrays: e_fine = P^L NN(R^L r_fine) (FP64 transfers,
+ * the inference kernels of the solver).  For tests. */
+int vf_learned_apply(vf_solver* s, const double* r_fine, double* e_fine);
+/* e_out = (I - M A)^n e_in: n stationary iterations of the FP32 V-cycle M of
+ * the mixed solver on an error vector (host arrays, reference layout); the
+ * training data of the learned stage. */
+int vf_mg_propagate(vf_solver* s, const double* e_in, int32_t n, double* e_out);
+/* Free-DOF bits of hierarchy level `level` (one byte per node, reference node
+ * order of that level). */
+int vf_level_mask(vf_solver* s, int32_t level, uint8_t* out);
 
 #ifdef __cplusplus
 }

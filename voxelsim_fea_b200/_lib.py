@@ -48,7 +48,8 @@ EXPORTS = (
     "vf_vcycle", "vf_inv_diagonal", "vf_time_kernel", "vf_get_stream", "vf_launch_count",
     "vf_apply_noalloc",
     "vf_nn_conv3d_forward", "vf_nn_conv3d_backward_data", "vf_nn_conv3d_backward_weight",
-    "vf_nn_wgrad_workspace",
+    "vf_nn_wgrad_workspace", "vf_learned_param_count", "vf_learned_configure", "vf_learned_info",
+    "vf_learned_input", "vf_learned_apply", "vf_level_mask", "vf_mg_propagate",
 )
 
 
@@ -66,7 +67,8 @@ class VfOptions(ctypes.Structure):
         ("omega_rel", ctypes.c_double),
         ("fine_kernel", ctypes.c_int32), ("modal_zchunk", ctypes.c_int32),
         ("coarse_storage", ctypes.c_int32), ("mixed_mode", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("flexible", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -138,6 +140,13 @@ def _declare(L):
         "vf_nn_conv3d_backward_weight": (ctypes.c_int, [_P, _P, _P, _I32, _P, ctypes.c_size_t, _I32, _I32, _I32,
                                                         _I32, _I32, _P]),
         "vf_nn_wgrad_workspace": (ctypes.c_size_t, [_I32, _I32, _I32, _I32, _I32]),
+        "vf_learned_param_count": (ctypes.c_int64, []),
+        "vf_learned_configure": (ctypes.c_int, [_P, _I32, _P, ctypes.c_int64, _I32]),
+        "vf_learned_info": (ctypes.c_int, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+        "vf_learned_input": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_float), _D]),
+        "vf_learned_apply": (ctypes.c_int, [_P, _P, _P]),
+        "vf_level_mask": (ctypes.c_int, [_P, _I32, _P]),
+        "vf_mg_propagate": (ctypes.c_int, [_P, _P, _I32, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

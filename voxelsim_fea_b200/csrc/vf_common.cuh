@@ -85,6 +85,8 @@ struct KrylovState {
   double scale;     // mixed: the residual scale of the current inner solve
   double hist_scale;
   double rr_trigger;  // > 0: stop the chunk (KS_RELIABLE) once rr drops below it
+  double zap;         // flexible CG: z.Ap of the last iteration
+  double gnum, gden;  // learned stage: step gamma = gnum / gden
   int it;           // iterations completed (this solve)
   int it_base;      // history offset (mixed: inner iterations before this solve)
   int max_it;
@@ -93,7 +95,7 @@ struct KrylovState {
   int stall_guard;
   int restart;      // beta := 0 (rz == 0, multigrid.py:534-545)
   int pad;
-  unsigned int counter[8];   // last-block-done counters of the reductions
+  unsigned int counter[12];  // last-block-done counters of the reductions
 };
 
 enum KState { KS_RUNNING = 0, KS_CONVERGED = 1, KS_MAXIT = 2, KS_STALLED = 3,
@@ -185,6 +187,8 @@ constexpr int kVecThreads = 256;
 template <typename T> void launch_dot(const Grid& g, const T* a, const T* b, double* partials, KrylovState* ks, int slot, cudaStream_t st);
 template <typename T> void launch_cg_update(const Grid& g, T* x, const T* p, T* r, const T* Ap, double* partials, KrylovState* ks, double* hist, cudaStream_t st);
 template <typename T> void launch_p_update(const Grid& g, T* p, const T* z, KrylovState* ks, cudaStream_t st);
+template <typename T> void launch_dot_fcg(const Grid& g, const T* r, const T* z, const T* Ap, double* partials,
+                                          KrylovState* ks, cudaStream_t st);
 template <typename T> void launch_jacobi_precond(const Grid& g, const T* r, const T* minv3, const uint8_t* mask, T* z, const KrylovState* ks, cudaStream_t st);
 template <typename T> void launch_copy_vec(const Grid& g, const T* src, T* dst, const KrylovState* ks, cudaStream_t st);
 void launch_norm2_f64(const Grid& g, const double* v, double* partials, KrylovState* ks, int slot, cudaStream_t st);
@@ -192,6 +196,9 @@ void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState
 void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const KrylovState* ks, cudaStream_t st);
 void launch_ir_replace(const Grid& g, const double* r64, float* r32, const KrylovState* ks, cudaStream_t st);
 void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st);
+template <typename T> void launch_sub_inplace(const Grid& g, T* y, const T* x, cudaStream_t st);
+template <typename T> void launch_axpy_gamma(const Grid& g, T* z, const T* c, const KrylovState* ks, const int* skip,
+                                             cudaStream_t st);
 // power iteration on D^-1 A (per-level damping)
 void launch_power_init(const Grid& g, double* x, const uint8_t* mask, cudaStream_t st);
 void launch_power_scale(const Grid& g, double* y, const double* minv3, double* partials, KrylovState* ks, cudaStream_t st);

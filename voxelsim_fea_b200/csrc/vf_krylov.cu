@@ -69,6 +69,26 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_update(long long n3, T* __re
   reduce_and_finalize(s, partials, ks, SLOT_RR, hist);
 }
 
+// (r.z, z.Ap) in one pass -> flexible-CG beta
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_dot_fcg(long long n3, const T* __restrict__ r, const T* __restrict__ z,
+                                                         const T* __restrict__ Ap, double* partials, KrylovState* ks) {
+  if (ks->done) return;
+  using H = V16<T>;
+  using V = typename H::V;
+  const long long nv = n3 / H::W;
+  const V* rv = reinterpret_cast<const V*>(r);
+  const V* zv = reinterpret_cast<const V*>(z);
+  const V* av = reinterpret_cast<const V*>(Ap);
+  double s1 = 0.0, s2 = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+    const V zz = __ldg(zv + i);
+    s1 += H::dot(__ldg(rv + i), zz);
+    s2 += H::dot(zz, __ldg(av + i));
+  }
+  reduce2_and_finalize(s1, s2, partials, ks, SLOT_FCG);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_p_update(long long n3, T* __restrict__ p, const T* __restrict__ z,
                                                           const KrylovState* ks) {
@@ -122,6 +142,25 @@ __global__ void k_ir_accumulate(long long n3, double* __restrict__ x64, const fl
   const double s = ks->scale;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
     x64[i] += s * (double)d32[i];
+}
+
+// z += gamma c, gamma = (c.r1) / (c.A c): the A-norm-optimal step along the
+// learned correction c (0 when c.A c is not positive)
+template <typename T>
+__global__ void k_axpy_gamma(long long n3, T* __restrict__ z, const T* __restrict__ c, const KrylovState* ks,
+                             const int* skip) {
+  if (skip && *skip) return;
+  const double den = ks->gden;
+  const T g = (den > 0.0) ? (T)(ks->gnum / den) : (T)0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    z[i] += g * c[i];
+}
+
+// y -= x (no state)
+template <typename T>
+__global__ void k_sub_inplace(long long n3, T* __restrict__ y, const T* __restrict__ x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+    y[i] -= x[i];
 }
 
 // r32 = r64 / scale with the scale fixed for the whole mixed solve
@@ -229,14 +268,34 @@ void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const Kr
 void launch_ir_replace(const Grid& g, const double* r64, float* r32, const KrylovState* ks, cudaStream_t st) {
   launch_k(k_ir_replace, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r64, r32, ks);
 }
+template <typename T>
+void launch_axpy_gamma(const Grid& g, T* z, const T* c, const KrylovState* ks, const int* skip, cudaStream_t st) {
+  launch_k(k_axpy_gamma<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, z, c, ks, skip);
+}
+template <typename T>
+void launch_sub_inplace(const Grid& g, T* y, const T* x, cudaStream_t st) {
+  launch_k(k_sub_inplace<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, y, x);
+}
+template void launch_sub_inplace<float>(const Grid&, float*, const float*, cudaStream_t);
+template void launch_sub_inplace<double>(const Grid&, double*, const double*, cudaStream_t);
+template void launch_axpy_gamma<float>(const Grid&, float*, const float*, const KrylovState*, const int*, cudaStream_t);
+template void launch_axpy_gamma<double>(const Grid&, double*, const double*, const KrylovState*, const int*,
+                                        cudaStream_t);
 void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st) {
   launch_k(k_sub_from, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, f, r);
+}
+
+template <typename T>
+void launch_dot_fcg(const Grid& g, const T* r, const T* z, const T* Ap, double* partials, KrylovState* ks,
+                    cudaStream_t st) {
+  launch_k(k_dot_fcg<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r, z, Ap, partials, ks);
 }
 
 #define VF_INST(T)                                                                                            \
   template void launch_dot<T>(const Grid&, const T*, const T*, double*, KrylovState*, int, cudaStream_t);    \
   template void launch_cg_update<T>(const Grid&, T*, const T*, T*, const T*, double*, KrylovState*, double*, cudaStream_t); \
   template void launch_p_update<T>(const Grid&, T*, const T*, KrylovState*, cudaStream_t);                   \
+  template void launch_dot_fcg<T>(const Grid&, const T*, const T*, const T*, double*, KrylovState*, cudaStream_t); \
   template void launch_jacobi_precond<T>(const Grid&, const T*, const T*, const uint8_t*, T*, const KrylovState*, cudaStream_t); \
   template void launch_copy_vec<T>(const Grid&, const T*, T*, const KrylovState*, cudaStream_t);
 VF_INST(double)

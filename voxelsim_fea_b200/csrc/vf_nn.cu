@@ -87,6 +87,7 @@ template <int CIN, int COUT>
 __global__ void __launch_bounds__(NTHREADS) k_conv3(NnConvArgs a) {
   constexpr int CP = CIN + 8;
   constexpr int NT = COUT / 8;       // n-tiles of 8 output channels
+  if (a.skip_flag && *a.skip_flag) return;
   extern __shared__ __align__(16) unsigned char smem[];
   bf16* sIn = reinterpret_cast<bf16*>(smem);
   bf16* sW = sIn + NHALO * CP;       // [9][COUT][CP]

@@ -20,6 +20,7 @@ struct NnConvArgs {
   float* out_f32;
   int X, Y, Z;
   int relu;
+  const int* skip_flag = nullptr;   // device flag: the launch is a no-op while *skip_flag != 0
 };
 
 // Supported (cin, cout): (16,16) (16,32) (32,16) (32,32) (32,64) (64,32) (64,64).
@@ -28,5 +29,24 @@ int nn_conv_forward(int cin, int cout, const NnConvArgs& a, cudaStream_t st);
 int nn_conv_wgrad(int cin, int cout, const void* x, const void* dy, float* dw, float* work, size_t work_bytes, int X,
                   int Y, int Z, int accumulate, cudaStream_t st);
 size_t nn_wgrad_work_bytes(int cin, int cout, int X, int Y, int Z);
+
+// ---- U-Net inference stage (vf_learned.cu) ----
+struct Grid;
+struct NnStage;
+long long nn_param_count();
+NnStage* nn_create(const Grid& gL, int level, cudaStream_t st, cudaError_t* err);
+void nn_destroy(NnStage* s);
+void nn_dims(const NnStage* s, int* xyz);
+cudaError_t nn_set_weights(NnStage* s, const float* host, cudaStream_t st);
+bool nn_has_weights(const NnStage* s);
+// static features from the fine modulus (padded voxel layout of g0); eref_dev: device max modulus
+void nn_set_features(NnStage* s, const Grid& g0, const double* E0, const double* eref_dev, cudaStream_t st);
+template <typename T> void nn_make_input(NnStage* s, const Grid& gL, const T* r, const int* skip, cudaStream_t st);
+void nn_forward(NnStage* s, const int* skip, cudaStream_t st);
+template <typename T> void nn_make_output(NnStage* s, const Grid& gL, const uint8_t* maskL, T* e, const int* skip,
+                                          cudaStream_t st);
+const void* nn_input_buffer(const NnStage* s);
+const float* nn_scale_buffer(const NnStage* s);
+void launch_max_f64(const double* v, long long n, double* out, cudaStream_t st);
 
 }  // namespace vf

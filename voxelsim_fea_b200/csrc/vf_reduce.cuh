@@ -21,7 +21,10 @@ enum RedSlot {
   SLOT_RZ_INIT = 3,  // r.z before the loop (multigrid.py:476)
   SLOT_FNORM = 4,    // ||f||^2   -> fnorm (multigrid.py:471)
   SLOT_OUTER = 5,    // ||r64||^2 -> outer (refinement) residual
-  SLOT_PLAIN = 6     // sum stored in ks->rr only
+  SLOT_PLAIN = 6,    // sum stored in ks->rr only
+  SLOT_FCG = 7,      // (r.z, z.Ap) -> flexible-CG beta = -z.Ap / p.Ap (Notay's FCG(1))
+  SLOT_GNUM = 8,     // c.r1  -> learned-stage step numerator
+  SLOT_GDEN = 9      // c.Ac  -> learned-stage step denominator
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -94,7 +97,46 @@ __device__ inline void finalize_slot(KrylovState* ks, int slot, double total, do
     case SLOT_RZ_INIT: ks->rz = total; ks->restart = 0; break;
     case SLOT_FNORM: ks->fnorm = sqrt(total); break;
     case SLOT_OUTER: ks->rr = total; ks->resid = sqrt(total) / ks->fnorm; break;
+    case SLOT_GNUM: ks->gnum = total; break;
+    case SLOT_GDEN: ks->gden = total; break;
     default: ks->rr = total; break;
+  }
+}
+
+// Two sums in one pass (partials hold 2 doubles per CTA); the last CTA finalizes
+// both together.  Used by the flexible-CG beta.
+__device__ inline void reduce2_and_finalize(double a, double b, double* partials, KrylovState* ks, int slot) {
+  __shared__ bool s_last2;
+  const double sa = block_sum(a);
+  const double sb = block_sum(b);
+  const int tid = lin_tid();
+  const unsigned nb = lin_nblocks();
+  if (tid == 0) {
+    partials[2 * lin_bid()] = sa;
+    partials[2 * lin_bid() + 1] = sb;
+    __threadfence();
+    unsigned int prev = atomicAdd(&ks->counter[slot], 1u);
+    s_last2 = (prev == nb - 1);
+  }
+  __syncthreads();
+  if (!s_last2) return;
+  __threadfence();
+  double ta = 0.0, tb = 0.0;
+  for (int i = tid; i < (int)nb; i += lin_nthreads()) {
+    ta += ((volatile double*)partials)[2 * i];
+    tb += ((volatile double*)partials)[2 * i + 1];
+  }
+  ta = block_sum(ta);
+  tb = block_sum(tb);
+  if (tid == 0) {
+    // FCG(1): p_new = z - (z.Ap / p.Ap) p; alpha next = (r.z) / (p_new.Ap_new)
+    ks->rz_new = ta;
+    ks->zap = tb;
+    if (ks->pAp != 0.0) { ks->restart = 0; ks->beta = -tb / ks->pAp; }
+    else { ks->restart = 1; ks->beta = 0.0; }
+    ks->rz = ta;
+    ks->counter[slot] = 0u;
+    __threadfence();
   }
 }
 

@@ -23,6 +23,7 @@
 #include "vf_common.cuh"
 #include "vf_hex8.h"
 #include "vf_reduce.cuh"
+#include "vf_nn.cuh"
 #include <cuda_fp16.h>
 
 namespace vf {
@@ -147,6 +148,11 @@ struct vf_solver {
   std::vector<void*> allocs;
   double last_setup_ms = 0.0;
   double last_best = 0.0;       // stall guard: best ratio of the last solve
+  // learned preconditioner stage (vf_learned.cu)
+  vf::NnStage* nn = nullptr;
+  int nn_level = 1;
+  bool nn_on = false;
+  double* d_nn_eref = nullptr;  // [0] max voxel modulus, [1..] reduction scratch
   double* d_omega = nullptr;    // damping per level (read by the smoothers)
   double* d_lambda = nullptr;   // lambda_max(D^-1 A_l) estimates (VF_OMEGA_AUTO)
   std::vector<double> h_omega, h_lambda;
@@ -180,7 +186,9 @@ int dalloc(vf_solver* s, T** p, size_t count) {
     s->err = std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) + " B): " + cudaGetErrorString(e);
     return VF_ERR_NOMEM;
   }
-  e = cudaMemset(q, 0, std::max<size_t>(count, 1) * sizeof(T));
+  // zeroed on the solver's own (non-blocking) stream: a legacy-stream memset
+  // is not ordered before the solver's kernels and could land after them
+  e = cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(T), s->st);
   if (e != cudaSuccess) { s->err = cudaGetErrorString(e); return VF_ERR_CUDA; }
   s->allocs.push_back(q);
   *p = (T*)q;
@@ -304,10 +312,63 @@ template <typename T> T** kvec(vf_solver* s);
 template <> double** kvec<double>(vf_solver* s) { return s->k64; }
 template <> float** kvec<float>(vf_solver* s) { return s->k32; }
 
+bool flexible(const vf_solver* s) { return s->o.flexible || s->nn_on; }
+
+// Learned stage after the V-cycle: z += gamma c, c = P^L NN(R^L r1),
+// r1 = r - A z.  The residual the V-cycle leaves is restricted to hierarchy
+// level L, the U-Net maps it (with the occupancy / modulus features) to a
+// level-L correction, the V-cycle's own prolongation carries it back to the
+// fine grid, and gamma = (c.r1) / (c.A c) is the A-norm-optimal step along it
+// -- the network gives a direction, the step never increases the error of z.
+template <typename T>
+void learned_stage(vf_solver* s, const T* r, T* z, KrylovState* ks) {
+  Level& l0 = s->L[0];
+  T* r1 = Sel<T>::w(l0, 2);   // level-0 work vectors are free once the V-cycle is done
+  T* c = Sel<T>::w(l0, 1);
+  T* Ac = Sel<T>::w(l0, 0);
+  KrylovState* kk = s->ks;     // the step reductions (also before the loop, where ks == nullptr)
+  level_op<T>(s, 0, EPI_RESID, z, r1, r, ks, nullptr, 0);
+  const T* cur = r1;
+  for (int li = 0; li < s->nn_level; ++li) {
+    Level& f = s->L[li];
+    Level& c = s->L[li + 1];
+    launch_restrict<T>(f.g, cur, c.g, c.mask, Sel<T>::w(c, 3), ks, s->st);
+    cur = Sel<T>::w(c, 3);
+  }
+  Level& lL = s->L[s->nn_level];
+  const int* skip = ks ? &ks->done : nullptr;
+  nn_make_input<T>(s->nn, lL.g, cur, skip, s->st);
+  nn_forward(s->nn, skip, s->st);
+  nn_make_output<T>(s->nn, lL.g, lL.mask, Sel<T>::w(lL, 0), skip, s->st);
+  for (int li = s->nn_level; li >= 1; --li) {
+    Level& cl = s->L[li];
+    Level& f = s->L[li - 1];
+    T* target = (li == 1) ? c : Sel<T>::w(f, 0);
+    cudaMemsetAsync(target, 0, sizeof(T) * 3 * (size_t)f.g.n, s->st);
+    launch_prolong_add<T>(cl.g, Sel<T>::w(cl, 0), f.g, f.mask, target, ks, s->st);
+  }
+  level_op<T>(s, 0, EPI_APPLY, c, Ac, nullptr, kk, s->d_partials, SLOT_GDEN);
+  launch_dot<T>(l0.g, c, r1, s->d_partials, kk, SLOT_GNUM, s->st);
+  launch_axpy_gamma<T>(l0.g, z, c, kk, skip, s->st);
+}
+
 template <typename T>
 void precondition(vf_solver* s, const T* r, T* z, KrylovState* ks) {
-  if (use_mg(s)) vcycle<T>(s, 0, r, z, ks);
-  else launch_jacobi_precond<T>(s->L[0].g, r, Sel<T>::minv(s->L[0]), s->L[0].mask, z, ks, s->st);
+  if (use_mg(s)) {
+    vcycle<T>(s, 0, r, z, ks);
+    if (s->nn_on) learned_stage<T>(s, r, z, ks);
+  } else {
+    launch_jacobi_precond<T>(s->L[0].g, r, Sel<T>::minv(s->L[0]), s->L[0].mask, z, ks, s->st);
+  }
+}
+
+// After z = M r: the beta reduction (PCG r.z, or flexible (r.z, z.Ap)) and p = z + beta p.
+template <typename T>
+void update_direction(vf_solver* s, const T* r, const T* z, T* p, const T* Ap) {
+  const Grid& g = s->L[0].g;
+  if (flexible(s)) launch_dot_fcg<T>(g, r, z, Ap, s->d_partials, s->ks, s->st);
+  else launch_dot<T>(g, r, z, s->d_partials, s->ks, SLOT_RZ, s->st);
+  launch_p_update<T>(g, p, z, s->ks, s->st);
 }
 
 // One PCG iteration (core/multigrid.py:497-546 / core/fea.py:548-580).
@@ -320,8 +381,7 @@ void pcg_iteration(vf_solver* s) {
   level_op<T>(s, 0, EPI_APPLY, p, Ap, nullptr, s->ks, s->d_partials, SLOT_PAP);
   launch_cg_update<T>(g, x, p, r, Ap, s->d_partials, s->ks, s->d_hist, s->st);
   precondition<T>(s, r, z, s->ks);
-  launch_dot<T>(g, r, z, s->d_partials, s->ks, SLOT_RZ, s->st);
-  launch_p_update<T>(g, p, z, s->ks, s->st);
+  update_direction<T>(s, r, z, p, Ap);
 }
 
 int graph_slot(const vf_solver* s, bool fp32) { return use_mg(s) ? (fp32 ? 1 : 0) : 2; }
@@ -486,6 +546,7 @@ int build_levels(vf_solver* s) {
   VF_ALLOC(s->d_partials, 148 * 64);
   VF_ALLOC(s->d_info, 1);
   VF_ALLOC(s->d_omega, 16);
+  VF_ALLOC(s->d_nn_eref, 148 * 4 + 1);
   VF_ALLOC(s->d_lambda, 16);
   VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
   memset(s->h_ks, 0, sizeof(KrylovState));
@@ -494,6 +555,15 @@ int build_levels(vf_solver* s) {
 
 // z-planes per CTA of the modal kernel: about 4 CTAs per SM over the level
 // (22 planes measured best on the 256x128x128 fine level).
+// occupancy / log-modulus features of the learned stage (shear modulus when
+// the Poisson ratio is per voxel, else E), normalised by the largest modulus
+void nn_refresh_features(vf_solver* s) {
+  Level& l0 = s->L[0];
+  const double* mod = s->lame ? l0.mu64 : l0.E64;
+  launch_max_f64(mod, (long long)l0.g.n, s->d_nn_eref, s->st);
+  nn_set_features(s->nn, l0.g, mod, s->d_nn_eref, s->st);
+}
+
 int auto_zchunk(const Grid& g, int requested) {
   if (requested > 0) return requested;
   const long long tiles = (long long)((g.lx + 1 + 30) / 31) * ((g.ly + 1 + 6) / 7);
@@ -520,10 +590,13 @@ int upload_tables(vf_solver* s) {
   VF_ALLOC(s->d_Ktab, 576);
   VF_ALLOC(s->d_Gtab_lame, 16 * 576);
   VF_ALLOC(s->d_Ktab_lame, 1152);
-  VF_TRY(cudaMemcpy(s->d_Gtab, G.data(), sizeof(double) * 8 * 576, cudaMemcpyHostToDevice));
-  VF_TRY(cudaMemcpy(s->d_Ktab, s->tab, sizeof(double) * 576, cudaMemcpyHostToDevice));
-  VF_TRY(cudaMemcpy(s->d_Gtab_lame, GL.data(), sizeof(double) * 16 * 576, cudaMemcpyHostToDevice));
-  VF_TRY(cudaMemcpy(s->d_Ktab_lame, s->tab + 576, sizeof(double) * 1152, cudaMemcpyHostToDevice));
+  // stream-ordered with the solver's kernels; the host vectors stay alive
+  // until the synchronisation below
+  VF_TRY(cudaMemcpyAsync(s->d_Gtab, G.data(), sizeof(double) * 8 * 576, cudaMemcpyHostToDevice, s->st));
+  VF_TRY(cudaMemcpyAsync(s->d_Ktab, s->tab, sizeof(double) * 576, cudaMemcpyHostToDevice, s->st));
+  VF_TRY(cudaMemcpyAsync(s->d_Gtab_lame, GL.data(), sizeof(double) * 16 * 576, cudaMemcpyHostToDevice, s->st));
+  VF_TRY(cudaMemcpyAsync(s->d_Ktab_lame, s->tab + 576, sizeof(double) * 1152, cudaMemcpyHostToDevice, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
   return VF_OK;
 }
 
@@ -703,6 +776,7 @@ int vf_destroy(vf_solver* s) {
   for (auto& gexe : s->chunk)
     if (gexe) cudaGraphExecDestroy(gexe);
   for (void* p : s->allocs) cudaFree(p);
+  if (s->nn) vf::nn_destroy(s->nn);
   if (s->h_ks) cudaFreeHost(s->h_ks);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
@@ -890,6 +964,8 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
     int rc = build_dense_coarsest(s);
     if (rc) return rc;
   }
+  if (s->nn) nn_refresh_features(s);
+  VF_CHECK_LAUNCH();
   VF_TRY(cudaEventRecord(s->ev1, s->st));
   VF_TRY(cudaEventSynchronize(s->ev1));
   float ms = 0.f;
@@ -998,8 +1074,7 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
     // the chunk stopped inside an iteration, right after r was updated: finish
     // that iteration on the replaced residual (z = M r, beta, p = z + beta p)
     precondition<float>(s, v[1], v[2], s->ks);
-    launch_dot<float>(g, v[1], v[2], s->d_partials, s->ks, SLOT_RZ, s->st);
-    launch_p_update<float>(g, v[3], v[2], s->ks, s->st);
+    update_direction<float>(s, v[1], v[2], v[3], v[4]);
     VF_CHECK_LAUNCH();
   }
   s->history.resize(inf.iters);
@@ -1521,6 +1596,156 @@ int vf_self_test(int32_t device) {
   if (rc && s) g_last_error = s->err.empty() ? g_last_error : s->err;
   vf_destroy(s);
   return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// learned preconditioner stage
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int64_t vf_learned_param_count(void) { return (int64_t)vf::nn_param_count(); }
+
+int vf_learned_configure(vf_solver* s, int32_t level, const float* params, int64_t n_params, int32_t enable) {
+  if (!s) return VF_ERR_ARG;
+  if (!use_mg(s) || level < 1 || level >= (int)s->L.size()) {
+    s->err = "learned stage: level must be a coarse level of the multigrid hierarchy";
+    return VF_ERR_ARG;
+  }
+  if (params && n_params != vf::nn_param_count()) {
+    s->err = "learned stage: expected " + std::to_string(vf::nn_param_count()) + " parameters";
+    return VF_ERR_ARG;
+  }
+  cudaSetDevice(s->device);
+  if (!s->nn || s->nn_level != level) {
+    if (s->nn) { VF_TRY(cudaStreamSynchronize(s->st)); vf::nn_destroy(s->nn); s->nn = nullptr; }
+    cudaError_t e = cudaSuccess;
+    s->nn = vf::nn_create(s->L[level].g, level, s->st, &e);
+    if (!s->nn) { s->err = std::string("learned stage: ") + cudaGetErrorString(e); return VF_ERR_NOMEM; }
+    s->nn_level = level;
+    if (s->have_material) nn_refresh_features(s);
+  }
+  if (params) VF_TRY(vf::nn_set_weights(s->nn, params, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  const bool on = enable && vf::nn_has_weights(s->nn);
+  if (enable && !on) { s->err = "learned stage: no weights"; return VF_ERR_STATE; }
+  if (on != s->nn_on) {
+    s->nn_on = on;
+    for (auto& gexe : s->chunk)   // the captured iterations change
+      if (gexe) { cudaGraphExecDestroy(gexe); gexe = nullptr; }
+  }
+  return VF_OK;
+}
+
+int vf_mg_propagate(vf_solver* s, const double* e_in, int32_t n, double* e_out) {
+  if (!s || !e_in || !e_out || n < 0) return VF_ERR_ARG;
+  if (!s->have_material || !use_mg(s)) { s->err = "set_material first (multigrid)"; return VF_ERR_STATE; }
+  cudaSetDevice(s->device);
+  Level& l0 = s->L[0];
+  const Grid& g = l0.g;
+  const size_t nref = 3 * (size_t)g.nodes_ref();
+  float** v = s->k32;
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, e_in, sizeof(double) * nref, cudaMemcpyHostToDevice, s->st));
+  launch_pack_vec<double>(g, s->d_ref_a, s->r64, l0.mask, s->st);
+  launch_convert<double, float>(s->r64, v[0], 3LL * g.n, s->st);
+  for (int j = 0; j < n; ++j) {   // e <- e - V(A e), the FP32 V-cycle of the mixed solver
+    level_op<float>(s, 0, EPI_APPLY, v[0], v[1], nullptr, nullptr, nullptr, 0);
+    vcycle<float>(s, 0, v[1], v[2], nullptr);
+    launch_sub_inplace<float>(g, v[0], v[2], s->st);
+  }
+  launch_convert<float, double>(v[0], s->r64, 3LL * g.n, s->st);
+  launch_unpack_vec<double>(g, s->r64, s->d_ref_c, s->st);
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaMemcpyAsync(e_out, s->d_ref_c, sizeof(double) * nref, cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  return VF_OK;
+}
+
+int vf_level_mask(vf_solver* s, int32_t level, uint8_t* out) {
+  if (!s || !out || level < 0 || level >= (int)s->L.size()) return VF_ERR_ARG;
+  cudaSetDevice(s->device);
+  const Grid& g = s->L[level].g;
+  std::vector<uint8_t> pad(g.n);
+  VF_TRY(cudaMemcpyAsync(pad.data(), s->L[level].mask, g.n, cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  const int nx1 = g.lx + 1, ny1 = g.ly + 1;
+  for (int z = 0; z <= g.lz; ++z)
+    for (int y = 0; y <= g.ly; ++y)
+      for (int x = 0; x <= g.lx; ++x) out[x + (size_t)nx1 * (y + (size_t)ny1 * z)] = pad[g.idx(x, y, z)];
+  return VF_OK;
+}
+
+int vf_learned_info(const vf_solver* s, int32_t* dims3, int32_t* level) {
+  if (!s || !s->nn) return VF_ERR_STATE;
+  int d[3];
+  vf::nn_dims(s->nn, d);
+  if (dims3) { dims3[0] = d[0]; dims3[1] = d[1]; dims3[2] = d[2]; }
+  if (level) *level = s->nn_level;
+  return VF_OK;
+}
+
+int vf_learned_input(vf_solver* s, const double* r_level, void* in_dev, float* scale_out, double* eref_out) {
+  if (!s || !r_level || !in_dev) return VF_ERR_ARG;
+  if (!s->nn || !s->have_material) { s->err = "learned stage: configure and set_material first"; return VF_ERR_STATE; }
+  cudaSetDevice(s->device);
+  Level& lL = s->L[s->nn_level];
+  const size_t nref = 3 * (size_t)lL.g.nodes_ref();
+  double* pad = lL.w64[3];
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, r_level, sizeof(double) * nref, cudaMemcpyHostToDevice, s->st));
+  launch_pack_vec<double>(lL.g, s->d_ref_a, pad, lL.mask, s->st);
+  vf::nn_make_input<double>(s->nn, lL.g, pad, nullptr, s->st);
+  int d[3];
+  vf::nn_dims(s->nn, d);
+  VF_TRY(cudaMemcpyAsync(in_dev, vf::nn_input_buffer(s->nn), (size_t)d[0] * d[1] * d[2] * 16 * 2,
+                         cudaMemcpyDeviceToDevice, s->st));
+  float sc = 0.f;
+  double er = 0.0;
+  VF_TRY(cudaMemcpyAsync(&sc, vf::nn_scale_buffer(s->nn), sizeof(float), cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaMemcpyAsync(&er, s->d_nn_eref, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  VF_CHECK_LAUNCH();
+  if (scale_out) *scale_out = sc;
+  if (eref_out) *eref_out = er;
+  return VF_OK;
+}
+
+int vf_learned_apply(vf_solver* s, const double* r_fine, double* e_fine) {
+  if (!s || !r_fine || !e_fine) return VF_ERR_ARG;
+  if (!s->nn || !vf::nn_has_weights(s->nn) || !s->have_material) {
+    s->err = "learned stage: configure with weights and set_material first";
+    return VF_ERR_STATE;
+  }
+  cudaSetDevice(s->device);
+  Level& l0 = s->L[0];
+  const size_t nref = 3 * (size_t)l0.g.nodes_ref();
+  VF_TRY(cudaMemcpyAsync(s->d_ref_a, r_fine, sizeof(double) * nref, cudaMemcpyHostToDevice, s->st));
+  double* r = s->k64[1];
+  double* e = s->k64[2];
+  launch_pack_vec<double>(l0.g, s->d_ref_a, r, l0.mask, s->st);
+  const double* cur = r;
+  for (int li = 0; li < s->nn_level; ++li) {
+    Level& f = s->L[li];
+    Level& c = s->L[li + 1];
+    launch_restrict<double>(f.g, cur, c.g, c.mask, c.w64[3], nullptr, s->st);
+    cur = c.w64[3];
+  }
+  Level& lL = s->L[s->nn_level];
+  vf::nn_make_input<double>(s->nn, lL.g, cur, nullptr, s->st);
+  vf::nn_forward(s->nn, nullptr, s->st);
+  vf::nn_make_output<double>(s->nn, lL.g, lL.mask, lL.w64[0], nullptr, s->st);
+  for (int li = s->nn_level; li >= 1; --li) {
+    Level& c = s->L[li];
+    Level& f = s->L[li - 1];
+    double* target = (li == 1) ? e : f.w64[0];
+    cudaMemsetAsync(target, 0, sizeof(double) * 3 * (size_t)f.g.n, s->st);
+    launch_prolong_add<double>(c.g, c.w64[0], f.g, f.mask, target, nullptr, s->st);
+  }
+  launch_unpack_vec<double>(l0.g, e, s->d_ref_c, s->st);
+  VF_CHECK_LAUNCH();
+  VF_TRY(cudaMemcpyAsync(e_fine, s->d_ref_c, sizeof(double) * nref, cudaMemcpyDeviceToHost, s->st));
+  VF_TRY(cudaStreamSynchronize(s->st));
+  return VF_OK;
 }
 
 }  // extern "C"

@@ -79,13 +79,14 @@ def conv3d_backward_weight(x, dy):
 
 
 class Conv3dFn(torch.autograd.Function):
-    """y = conv(x, w) + b with the libvoxfea kernels in both directions."""
+    """y = conv(x, w) + b with the libvoxfea kernels in both directions
+    (BF16 output, or FP32 with ``out_f32``)."""
 
     @staticmethod
-    def forward(ctx, x, w, b):
+    def forward(ctx, x, w, b, out_f32=False):
         wb = w.to(torch.bfloat16).contiguous()
         ctx.save_for_backward(x, wb)
-        return conv3d_forward(x.contiguous(), wb, bias=b)
+        return conv3d_forward(x.contiguous(), wb, bias=b, out_f32=out_f32)
 
     @staticmethod
     def backward(ctx, dy):
@@ -94,8 +95,8 @@ class Conv3dFn(torch.autograd.Function):
         dx = conv3d_backward_data(dy, wb) if ctx.needs_input_grad[0] else None
         dw = conv3d_backward_weight(x, dy) if ctx.needs_input_grad[1] else None
         db = dy.float().sum(dim=(0, 1, 2)) if ctx.needs_input_grad[2] else None
-        return dx, dw, db
+        return dx, dw, db, None
 
 
-def conv3d(x, w, b):
-    return Conv3dFn.apply(x, w, b)
+def conv3d(x, w, b, out_f32=False):
+    return Conv3dFn.apply(x, w, b, out_f32)

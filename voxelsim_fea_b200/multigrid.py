@@ -42,6 +42,7 @@ class SolverOptions:
     inner_tol: float = 1e-2          # mixed: residual reduction between FP64 corrections
     max_outer: int = 20              # mixed: cap on FP64 corrections
     mixed_mode: str = "reliable"     # mixed: "reliable" (residual replacement) | "restart" (refinement)
+    flexible: bool = False           # flexible CG (automatic with a learned stage)
     omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
     omega_rel: float = 0.8
     power_iters: int = 20
@@ -144,6 +145,7 @@ class MGSolver:
         o.modal_zchunk = int(self.options.modal_zchunk)
         o.coarse_storage = _lib.STENCIL_STORAGE[self.options.coarse_storage]
         o.mixed_mode = _lib.MIXED_MODES[self.options.mixed_mode]
+        o.flexible = int(bool(self.options.flexible))
         h = ctypes.c_void_p()
         _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
                    None, "vf_create")
