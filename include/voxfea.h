@@ -276,6 +276,18 @@ int vf_apply_noalloc(int32_t nx, int32_t ny, int32_t nz, double nu, const double
                      const uint8_t* free_mask, const double* u, double* y, double* u_dot_y,
                      void* stream);
 
+/* ---- block right-hand sides ----------------------------------------------------
+ * k load cases on one geometry (the reference solves them one call at a time:
+ * MGSolver.solve, core/multigrid.py:439-583, once per case).  F and U hold k
+ * vectors of 3*(nx+1)*(ny+1)*(nz+1) values back to back (host, or device with
+ * VF_SOLVE_DEVICE_PTRS); infos receives k records.  The k solves share this
+ * solver's operator data (set up once by vf_set_material) and run concurrently,
+ * each on its own stream with its own vectors, Krylov state and CUDA graphs
+ * (created on first use and kept for later calls).  Not with the learned stage
+ * enabled (VF_ERR_UNSUPPORTED). */
+int vf_solve_block(vf_solver* s, const double* F, int32_t k, double tol, int32_t max_it,
+                   uint32_t flags, double* U, vf_solve_info* infos);
+
 /* ---- learned preconditioner stage: BF16 tensor-core 3x3x3 convolutions --------
  * No counterpart in the reference (its solver has no learned part).  Building
  * blocks of the U-Net trained by voxelsim_fea_b200.learned and run inside the

@@ -49,7 +49,7 @@ EXPORTS = (
     "vf_apply_noalloc",
     "vf_nn_conv3d_forward", "vf_nn_conv3d_backward_data", "vf_nn_conv3d_backward_weight",
     "vf_nn_wgrad_workspace", "vf_learned_param_count", "vf_learned_configure", "vf_learned_info",
-    "vf_learned_input", "vf_learned_apply", "vf_level_mask", "vf_mg_propagate",
+    "vf_learned_input", "vf_learned_apply", "vf_level_mask", "vf_mg_propagate", "vf_solve_block",
 )
 
 
@@ -147,6 +147,8 @@ def _declare(L):
         "vf_learned_apply": (ctypes.c_int, [_P, _P, _P]),
         "vf_level_mask": (ctypes.c_int, [_P, _I32, _P]),
         "vf_mg_propagate": (ctypes.c_int, [_P, _P, _I32, _P]),
+        "vf_solve_block": (ctypes.c_int, [_P, _P, _I32, ctypes.c_double, _I32, ctypes.c_uint32, _P,
+                                          ctypes.POINTER(VfSolveInfo)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -31,6 +31,7 @@
 // the voxel column with that lower corner; outputs are produced for
 // tx >= 1, ty >= 1 (a node needs the four voxel columns around it), so a tile
 // advances by (31, TY-1) columns.  One node row/column of halo is loaded.
+#include <atomic>
 #include <cmath>
 
 #include "vf_common.cuh"
@@ -434,10 +435,10 @@ void launch_modal_op(const Grid& g, int epi, const OpArgs& a, const ModalConst& 
   do {                                                                                        \
     auto kern = k_modal_op<T, LM, EP, TYV>;                                                   \
     constexpr size_t smem = modal_smem_bytes<T, TYV, LM, EP>();                               \
-    static bool attr = false;                                                                 \
-    if (!attr) {                                                                              \
+    static std::atomic<bool> attr{false};                                                     \
+    if (!attr.load()) {                                                                       \
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
-      attr = true;                                                                            \
+      attr.store(true);                                                                       \
     }                                                                                         \
     launch_k(kern, grid, block, smem, st, g, a, mc, zchunk);                                  \
   } while (0)

@@ -23,6 +23,8 @@
 // (deterministic).
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 #include "vf_common.cuh"
 #include "vf_nn.cuh"
 
@@ -299,12 +301,12 @@ __global__ void k_reduce_partials(const float* __restrict__ partial, int nparts,
 template <int CIN, int COUT>
 int conv_forward_t(const NnConvArgs& a, cudaStream_t st) {
   constexpr size_t smem = conv_smem_bytes<CIN, COUT>();
-  static int attr_dev = -1;
+  static std::atomic<int> attr_dev{-1};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (attr_dev != dev) {
+  if (attr_dev.load() != dev) {
     cudaFuncSetAttribute(k_conv3<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_dev = dev;
+    attr_dev.store(dev);
   }
   const long long tiles = (long long)((a.X + OTX - 1) / OTX) * ((a.Y + OTY - 1) / OTY) * ((a.Z + OTZ - 1) / OTZ);
   if (tiles <= 0) return 0;
@@ -322,12 +324,12 @@ int conv_wgrad_t(const void* x, const void* dy, float* dw, float* work, size_t w
   nb = std::min<long long>(nb, (long long)(work_bytes / per));
   if (nb < 1) return -1;
   constexpr size_t smem = Cfg::smem();
-  static int attr_dev = -1;
+  static std::atomic<int> attr_dev{-1};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (attr_dev != dev) {
+  if (attr_dev.load() != dev) {
     cudaFuncSetAttribute(k_conv3_wgrad<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_dev = dev;
+    attr_dev.store(dev);
   }
   launch_k(k_conv3_wgrad<CIN, COUT>, dim3((unsigned)nb, 27 / Cfg::TAPS), dim3(NTHREADS), smem, st,
            (const bf16*)x, (const bf16*)dy, work, X, Y, Z);

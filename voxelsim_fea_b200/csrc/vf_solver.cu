@@ -17,6 +17,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/voxfea.h"
@@ -156,6 +157,10 @@ struct vf_solver {
   double* d_omega = nullptr;    // damping per level (read by the smoothers)
   double* d_lambda = nullptr;   // lambda_max(D^-1 A_l) estimates (VF_OMEGA_AUTO)
   std::vector<double> h_omega, h_lambda;
+  // block right-hand sides: solvers that share this one's operator data and
+  // own their vectors, Krylov state, stream and graphs (vf_solve_block)
+  std::vector<vf_solver*> children;
+  bool is_child = false;
 };
 
 namespace {
@@ -772,6 +777,8 @@ void vf_options_default(vf_options* o) {
 int vf_destroy(vf_solver* s) {
   if (!s) return VF_OK;
   cudaSetDevice(s->device);
+  for (vf_solver* c : s->children) vf_destroy(c);
+  s->children.clear();
   if (s->st) cudaStreamSynchronize(s->st);
   for (auto& gexe : s->chunk)
     if (gexe) cudaGraphExecDestroy(gexe);
@@ -1596,6 +1603,156 @@ int vf_self_test(int32_t device) {
   if (rc && s) g_last_error = s->err.empty() ? g_last_error : s->err;
   vf_destroy(s);
   return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// block right-hand sides
+// ---------------------------------------------------------------------------
+namespace {
+
+// Point a child at the master's operator data (moduli, masks, diagonals,
+// stencils, coarsest factor, damping) -- read-only during solves.
+void share_operator(vf_solver* c, const vf_solver* m) {
+  c->o = m->o;
+  c->lame = m->lame;
+  c->mc = m->mc;
+  c->mc_lame = m->mc_lame;
+  memcpy(c->tab, m->tab, sizeof(c->tab));
+  memcpy(c->B0, m->B0, sizeof(c->B0));
+  for (size_t i = 0; i < c->L.size(); ++i) {
+    Level& d = c->L[i];
+    const Level& sl = m->L[i];
+    d.g = sl.g; d.zchunk = sl.zchunk; d.szchunk = sl.szchunk; d.mask = sl.mask; d.galerkin = sl.galerkin;
+    d.E64 = sl.E64; d.mu64 = sl.mu64; d.minv64 = sl.minv64; d.st64 = sl.st64;
+    d.E32 = sl.E32; d.mu32 = sl.mu32; d.minv32 = sl.minv32; d.st32 = sl.st32;
+    d.sym64 = sl.sym64; d.sq64 = sl.sq64; d.sym32 = sl.sym32; d.sym16 = sl.sym16; d.sq32 = sl.sq32;
+  }
+  c->d_Ainv = m->d_Ainv;
+  c->dense_n = m->dense_n;
+  c->d_omega = m->d_omega;
+  c->d_lambda = m->d_lambda;
+  c->h_omega = m->h_omega;
+  c->h_lambda = m->h_lambda;
+  c->h_mask_ref = m->h_mask_ref;
+  c->h_active = m->h_active;
+  c->have_active = m->have_active;
+  c->d_active_ref = m->d_active_ref;
+  c->d_active_pad = m->d_active_pad;
+  c->have_fixed = m->have_fixed;
+  c->have_material = m->have_material;
+  c->last_setup_ms = 0.0;
+}
+
+int make_child(vf_solver* m, vf_solver** out) {
+  vf_solver* s = new vf_solver();
+  s->is_child = true;
+  s->device = m->device;
+  s->nu = m->nu;
+  s->nx = m->nx; s->ny = m->ny; s->nz = m->nz;
+  s->L.resize(m->L.size());
+  share_operator(s, m);
+  auto fail = [&](int code) {
+    m->err = "block solve: " + s->err;
+    vf_destroy(s);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) { s->err = "stream"; return fail(VF_ERR_CUDA); }
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  cudaEventCreate(&s->ev2);
+  auto body = [&]() -> int {
+    for (auto& l : s->L) {
+      const size_t n = l.g.n;
+      for (int k = 0; k < 4; ++k) {
+        VF_ALLOC(l.w64[k], 3 * n);
+        VF_ALLOC(l.w32[k], 3 * n);
+      }
+    }
+    const Grid& g0 = s->L[0].g;
+    for (int k = 0; k < 5; ++k) {
+      VF_ALLOC(s->k64[k], 3 * (size_t)g0.n);
+      VF_ALLOC(s->k32[k], 3 * (size_t)g0.n);
+    }
+    VF_ALLOC(s->f64, 3 * (size_t)g0.n);
+    VF_ALLOC(s->r64, 3 * (size_t)g0.n);
+    const size_t nref = 3 * (size_t)g0.nodes_ref();
+    VF_ALLOC(s->d_ref_a, nref);
+    VF_ALLOC(s->d_ref_b, nref);
+    VF_ALLOC(s->d_ref_c, nref);
+    VF_ALLOC(s->ks, 1);
+    VF_ALLOC(s->d_partials, 148 * 64);
+    VF_ALLOC(s->d_info, 1);
+    VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
+    memset(s->h_ks, 0, sizeof(KrylovState));
+    int rc = ensure_hist(s, 4096);
+    if (rc) return rc;
+    VF_TRY(cudaStreamSynchronize(s->st));
+    return VF_OK;
+  };
+  int rc = body();
+  if (rc) return fail(rc);
+  *out = s;
+  return VF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vf_solve_block(vf_solver* s, const double* F, int32_t k, double tol, int32_t max_it, uint32_t flags,
+                   double* U, vf_solve_info* infos) {
+  if (!s || !F || !U || k < 1) return VF_ERR_ARG;
+  if (s->is_child) return VF_ERR_STATE;
+  if (!s->have_fixed) { s->err = "call set_fixed() before solve()"; return VF_ERR_STATE; }
+  if (!s->have_material) { s->err = "call set_material() before solve()"; return VF_ERR_STATE; }
+  if (s->nn_on) {   // the stage's activation buffers belong to one solver
+    s->err = "block solve: disable the learned stage first (vf_learned_configure enable = 0)";
+    return VF_ERR_UNSUPPORTED;
+  }
+  cudaSetDevice(s->device);
+  VF_TRY(cudaStreamSynchronize(s->st));   // the operator is final
+  while ((int)s->children.size() < k - 1) {
+    vf_solver* c = nullptr;
+    int rc = make_child(s, &c);
+    if (rc) return rc;
+    s->children.push_back(c);
+  }
+  std::vector<vf_solver*> solvers{s};
+  for (int j = 0; j + 1 < k; ++j) {
+    vf_solver* c = s->children[j];
+    const bool had_graphs = c->chunk[0] || c->chunk[1] || c->chunk[2];
+    const double* oldA = c->d_Ainv;
+    share_operator(c, s);
+    // graphs hold operator pointers and option-dependent launch sequences: re-capture on change
+    if (had_graphs && (oldA != c->d_Ainv))
+      for (auto& gexe : c->chunk)
+        if (gexe) { cudaGraphExecDestroy(gexe); gexe = nullptr; }
+    solvers.push_back(c);
+  }
+  const size_t ndof = 3 * (size_t)s->L[0].g.nodes_ref();
+  std::vector<int> rcs(k, VF_OK);
+  std::vector<vf_solve_info> inf(k);
+  std::vector<std::thread> th;
+  for (int j = 0; j < k; ++j) {
+    th.emplace_back([&, j]() {
+      cudaSetDevice(s->device);
+      rcs[j] = vf_solve_cb(solvers[j], F + j * ndof, nullptr, tol, max_it, flags, U + j * ndof, &inf[j], nullptr,
+                           nullptr);
+    });
+  }
+  for (auto& t : th) t.join();
+  if (infos)
+    for (int j = 0; j < k; ++j) infos[j] = inf[j];
+  for (int j = 0; j < k; ++j)
+    if (rcs[j] != VF_OK && rcs[j] != VF_ERR_STALLED) {
+      if (j > 0) s->err = "block solve, right-hand side " + std::to_string(j) + ": " + solvers[j]->err;
+      return rcs[j];
+    }
+  for (int j = 0; j < k; ++j)
+    if (rcs[j] != VF_OK) return rcs[j];
+  return VF_OK;
 }
 
 }  // extern "C"

@@ -330,4 +330,27 @@ class MGSolver:
         return u
 
 
+def _solve_block(self, Evec_full, F, tol=1e-4, max_cg=None, nu_elem=None):
+    """k load cases on one geometry as one call (B200 extension; the reference
+    calls ``solve`` once per case): F is (k, ndof); returns U (k, ndof).  The
+    cases share the operator set-up and run concurrently on the device.
+    Per-case results land in ``last_block_info`` (k vf_solve_info records)."""
+    self.set_density(Evec_full, nu_elem=nu_elem)
+    F = np.ascontiguousarray(np.asarray(F, dtype=float).reshape(-1, self.ndof))
+    k = F.shape[0]
+    U = np.empty_like(F)
+    infos = (_lib.VfSolveInfo * k)()
+    rc = _lib.load().vf_solve_block(self._handle(), _lib.ptr(F), k, float(tol), int(max_cg or 0), 0,
+                                    _lib.ptr(U), infos)
+    self.last_block_info = list(infos)
+    if rc not in (_lib.VF_OK, _lib.VF_ERR_STALLED):
+        _lib.check(rc, self._h, "solve_block")
+    self.last_iters = max(int(i.iters) for i in infos)
+    self.last_converged = all(bool(i.converged) for i in infos)
+    if rc == _lib.VF_ERR_STALLED:
+        _lib.check(rc, self._h)
+    return U
+
+
+MGSolver.solve_block = _solve_block
 MGSolver._apply_pooled = lambda self, u: self._apply(0, u)
