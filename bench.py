@@ -205,6 +205,53 @@ def run_reference(args):
     return 0
 
 
+# --------------------------------------------------------------------------- batch of parts
+def run_batch(args):
+    """N independent seeded parts, edges uniform in {32, 48, ..., 128} per
+    axis, each its own solver; one step = set-up + solve of all parts in one
+    synchronous vf_solve_batch call (parts run concurrently on their own
+    streams).  Timed with the host clock around the call, after a device
+    synchronisation (the parts' streams have no single device timeline)."""
+    import torch
+    from voxelsim_fea_b200 import generators
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions, solve_batch
+    rng = np.random.default_rng(1234)
+    edges = (32, 48, 64, 80, 96, 112, 128)
+    parts, solvers = [], []
+    for i in range(args.batch):
+        sh = tuple(int(rng.choice(edges)) for _ in range(3))
+        p = generators.bracket(shape=sh, seed=5000 + i, sigma=3.0, load_n=2000.0, patch=8)
+        p["E_mg"] = mg_modulus(p)
+        parts.append(p)
+        solvers.append(MGSolver(*sh, p["fixed_dofs"], nu=p["nu"], options=SolverOptions.fast(),
+                                n_smooth=args.n_smooth))
+    ndof = sum(s.ndof for s in solvers)
+    E_list = [p["E_mg"] for p in parts]
+    F_list = [p["f"] for p in parts]
+    mc = args.max_it or None
+    for _ in range(args.warmup):
+        solve_batch(solvers, E_list, F_list, tol=TOL, max_cg=mc)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solve_batch(solvers, E_list, F_list, tol=TOL, max_cg=mc)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    worst = max(s.last_info.true_resid for s in solvers)
+    if not (worst < TOL):
+        raise SystemExit(f"bench: a batch part missed tol={TOL:g} (true residual {worst:.3e})")
+    line = {"metric": METRIC, "value": ndof / (ms / 1e3) / 1e6, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 dots, refinement residual, coarsest solve)",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"batch{args.batch}_parts_32-128", "dof": ndof, "parts": args.batch,
+                       "iterations_max": max(s.last_iters for s in solvers), "timing": "host clock, synchronous call"}}
+    print(json.dumps(line), flush=True)
+    for s in solvers:
+        s.close()
+    return 0
+
+
 # --------------------------------------------------------------------------- B200 arm
 def run_b200(args):
     import torch
@@ -235,7 +282,8 @@ def run_b200(args):
     nu_scalar = 0.3 if per_voxel_nu else float(p["nu"])
 
     def solver(opts):
-        return MGSolver(nx, ny, nz, p["fixed_dofs"], nu=nu_scalar, max_levels=w["levels"], options=opts)
+        return MGSolver(nx, ny, nz, p["fixed_dofs"], nu=nu_scalar, max_levels=w["levels"], options=opts,
+                        n_smooth=args.n_smooth)
 
     fkw = dict(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk, mixed_mode=args.mixed_mode)
     if args.inner_tol is not None:
@@ -448,6 +496,9 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-stage arm")
     ap.add_argument("--max-it", type=int, default=0, help="PCG iteration cap (0: the solver default, 1000)")
     ap.add_argument("--block", type=int, default=1, help="k load cases per step as one block solve")
+    ap.add_argument("--n-smooth", type=int, default=2, help="pre/post sweeps of the V-cycle")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="N independent parts (edges 32..128) per step in one vf_solve_batch call")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nvtx", action="store_true", help="wrap the timed steps in NVTX range vf_timed")
@@ -464,6 +515,8 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.batch:
+        return run_batch(args)
     return run_b200(args)
 
 

@@ -108,7 +108,10 @@ typedef struct vf_options {
   int32_t flexible;        /* 1: flexible CG (Notay's FCG(1): beta = -z.Ap / p.Ap), which
                               stays correct for a preconditioner that varies between
                               iterations; always on while a learned stage is enabled */
-  int32_t reserved[6];
+  int32_t autotune;        /* 1 (default): at the first vf_set_material, time candidate
+                              z-chunk sizes of the marching kernels on every level and keep
+                              the fastest (cached per grid shape for the process) */
+  int32_t reserved[5];
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
@@ -287,6 +290,16 @@ int vf_apply_noalloc(int32_t nx, int32_t ny, int32_t nz, double nu, const double
  * enabled (VF_ERR_UNSUPPORTED). */
 int vf_solve_block(vf_solver* s, const double* F, int32_t k, double tol, int32_t max_it,
                    uint32_t flags, double* U, vf_solve_info* infos);
+
+/* Many independent parts (each its own solver: own grid, geometry, stream) set
+ * up and solved concurrently in one call -- the reference solves one part per
+ * job.  For part i: E[i] / nu_elem[i] (optional, as vf_set_material; E == NULL
+ * or E[i] == NULL keeps the material already set), F[i] -> U[i] (host, or
+ * device with VF_SOLVE_DEVICE_PTRS), infos[i].  Returns the first failing
+ * part's status (vf_global_last_error names it). */
+int vf_solve_batch(vf_solver* const* solvers, int32_t n, const double* const* E,
+                   const double* const* nu_elem, const double* const* F, double tol,
+                   int32_t max_it, uint32_t flags, double* const* U, vf_solve_info* infos);
 
 /* ---- learned preconditioner stage: BF16 tensor-core 3x3x3 convolutions --------
  * No counterpart in the reference (its solver has no learned part).  Building

@@ -50,6 +50,7 @@ EXPORTS = (
     "vf_nn_conv3d_forward", "vf_nn_conv3d_backward_data", "vf_nn_conv3d_backward_weight",
     "vf_nn_wgrad_workspace", "vf_learned_param_count", "vf_learned_configure", "vf_learned_info",
     "vf_learned_input", "vf_learned_apply", "vf_level_mask", "vf_mg_propagate", "vf_solve_block",
+    "vf_solve_batch",
 )
 
 
@@ -67,8 +68,8 @@ class VfOptions(ctypes.Structure):
         ("omega_rel", ctypes.c_double),
         ("fine_kernel", ctypes.c_int32), ("modal_zchunk", ctypes.c_int32),
         ("coarse_storage", ctypes.c_int32), ("mixed_mode", ctypes.c_int32),
-        ("flexible", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("flexible", ctypes.c_int32), ("autotune", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
     ]
 
 
@@ -148,6 +149,8 @@ def _declare(L):
         "vf_level_mask": (ctypes.c_int, [_P, _I32, _P]),
         "vf_mg_propagate": (ctypes.c_int, [_P, _P, _I32, _P]),
         "vf_solve_block": (ctypes.c_int, [_P, _P, _I32, ctypes.c_double, _I32, ctypes.c_uint32, _P,
+                                          ctypes.POINTER(VfSolveInfo)]),
+        "vf_solve_batch": (ctypes.c_int, [_P, _I32, _P, _P, _P, ctypes.c_double, _I32, ctypes.c_uint32, _P,
                                           ctypes.POINTER(VfSolveInfo)]),
     }
     for name, (res, args) in sig.items():

@@ -94,7 +94,7 @@ struct KrylovState {
   int status;       // 0 running/ok, 1 converged, 2 max_it, 3 stalled, 4 breakdown, 5 nonfinite
   int stall_guard;
   int restart;      // beta := 0 (rz == 0, multigrid.py:534-545)
-  int pad;
+  int it_trigger;   // > 0: stop the chunk (KS_RELIABLE) once it reaches it
   unsigned int counter[12];  // last-block-done counters of the reductions
 };
 

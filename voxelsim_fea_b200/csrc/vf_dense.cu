@@ -258,9 +258,12 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
   return 0;
 }
 
-// b is staged in dynamic shared memory (n doubles, n <= 16384).
+// b is staged in dynamic shared memory (n doubles, n <= 16384).  The limit is
+// a per-function attribute shared by every solver of the process (solvers of
+// different sizes run concurrently in batch solves): always the maximum.
 void dense_prepare_smem(int n) {
-  const int bytes = (int)sizeof(double) * n;
+  (void)n;
+  const int bytes = (int)sizeof(double) * 16384;
   cudaFuncSetAttribute(k_dense_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_dense_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }

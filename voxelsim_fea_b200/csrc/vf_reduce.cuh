@@ -84,6 +84,7 @@ __device__ inline void finalize_slot(KrylovState* ks, int slot, double total, do
         ks->done = 1; ks->status = KS_STALLED; break;
       }
       if (total < ks->rr_trigger) { ks->done = 1; ks->status = KS_RELIABLE; break; }
+      if (ks->it_trigger > 0 && it >= ks->it_trigger) { ks->done = 1; ks->status = KS_RELIABLE; break; }
       if (it >= ks->max_it) { ks->done = 1; ks->status = KS_MAXIT; }
       break;
     }

@@ -16,8 +16,11 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "../../include/voxfea.h"
@@ -161,6 +164,7 @@ struct vf_solver {
   // own their vectors, Krylov state, stream and graphs (vf_solve_block)
   std::vector<vf_solver*> children;
   bool is_child = false;
+  bool tuned = false;
 };
 
 namespace {
@@ -569,6 +573,67 @@ void nn_refresh_features(vf_solver* s) {
   nn_set_features(s->nn, l0.g, mod, s->d_nn_eref, s->st);
 }
 
+// ---------------------------------------------------------------------------
+// autotuner: z-planes per CTA of the marching kernels, per level, timed with
+// CUDA events on the FP32 Jacobi sweep (the kernel the V-cycle runs most);
+// the choice is cached per (grid, kernel form) for the process.
+// ---------------------------------------------------------------------------
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
+int auto_zchunk(const Grid& g, int requested);
+
+int autotune_levels(vf_solver* s) {
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  VF_TRY(cudaEventCreate(&t0));
+  VF_TRY(cudaEventCreate(&t1));
+  struct Ev {
+    cudaEvent_t a, b;
+    ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } ev{t0, t1};
+  for (size_t li = 0; li < s->L.size(); ++li) {
+    Level& l = s->L[li];
+    const bool stencil = l.galerkin && s->o.coarse_storage != VF_STENCIL_FULL;
+    const bool modal = !l.galerkin && s->o.fine_kernel == VF_FINE_MODAL;
+    if (!stencil && !modal) continue;
+    if (modal && s->o.modal_zchunk > 0) continue;   // fixed by the caller
+    const auto key = std::make_tuple(l.g.lx, l.g.ly, l.g.lz, stencil ? 1 + s->o.coarse_storage : 0);
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        (stencil ? l.szchunk : l.zchunk) = it->second;
+        continue;
+      }
+    }
+    const int planes = l.g.lz + 1;
+    std::vector<int> cand;
+    const int base = stencil ? sym_zchunk(l.g) : auto_zchunk(l.g, 0);
+    for (int c : {base, 1, 2, 3, 4, 6, 8, 12, 16, 22, 33, 48, 65})
+      if (c >= 1 && c <= planes && (modal ? c >= 2 : true) &&
+          std::find(cand.begin(), cand.end(), c) == cand.end())
+        cand.push_back(c);
+    int best = base;
+    float best_ms = 1e30f;
+    for (int c : cand) {
+      (stencil ? l.szchunk : l.zchunk) = c;
+      level_op<float>(s, (int)li, EPI_SMOOTH, l.w32[0], l.w32[1], l.w32[3], nullptr, nullptr, 0);   // warm
+      VF_TRY(cudaEventRecord(t0, s->st));
+      for (int r = 0; r < 3; ++r)
+        level_op<float>(s, (int)li, EPI_SMOOTH, l.w32[0], l.w32[1], l.w32[3], nullptr, nullptr, 0);
+      VF_TRY(cudaEventRecord(t1, s->st));
+      VF_TRY(cudaEventSynchronize(t1));
+      VF_CHECK_LAUNCH();
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, t0, t1);
+      if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    (stencil ? l.szchunk : l.zchunk) = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  return VF_OK;
+}
+
 int auto_zchunk(const Grid& g, int requested) {
   if (requested > 0) return requested;
   const long long tiles = (long long)((g.lx + 1 + 30) / 31) * ((g.ly + 1 + 6) / 7);
@@ -772,6 +837,7 @@ void vf_options_default(vf_options* o) {
   o->modal_zchunk = 0;
   o->coarse_storage = VF_STENCIL_SYM_HALF;
   o->mixed_mode = VF_MIXED_RELIABLE;
+  o->autotune = 1;
 }
 
 int vf_destroy(vf_solver* s) {
@@ -973,6 +1039,14 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
   }
   if (s->nn) nn_refresh_features(s);
   VF_CHECK_LAUNCH();
+  if (s->o.autotune && !s->tuned && use_mg(s)) {
+    // the kernels' shapes are baked into the captured graphs: tune before any capture
+    int rc = autotune_levels(s);
+    if (rc) return rc;
+    s->tuned = true;
+    for (auto& gexe : s->chunk)
+      if (gexe) { cudaGraphExecDestroy(gexe); gexe = nullptr; }
+  }
   VF_TRY(cudaEventRecord(s->ev1, s->st));
   VF_TRY(cudaEventSynchronize(s->ev1));
   float ms = 0.f;
@@ -1036,9 +1110,13 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
   // two within a few percent (measured on the 64x16x16 cantilever)
   const double delta = std::min(std::max(s->o.inner_tol, 1e-6), 0.5);
   // CG state: ratio = ||r32|| (fnorm 1), history scaled back to ||r|| / ||f||
+  // a replacement cycle that has not gained delta after this many iterations
+  // is treated as a stall of the FP32 recurrence: replace AND restart
+  const int first_cycle_cap = 400;
   init_ks(*s->h_ks, tol * fnorm / scale, max_it, 0, 0, scale / fnorm);
   s->h_ks->scale = scale;
   s->h_ks->rr_trigger = delta * delta;
+  s->h_ks->it_trigger = first_cycle_cap;
   VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
   launch_ir_replace(g, s->r64, v[1], s->ks, s->st);
   cudaMemsetAsync(v[0], 0, sizeof(float) * 3 * (size_t)g.n, s->st);
@@ -1049,11 +1127,16 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
   double best = ratio;
   int no_gain = 0;
   const int max_updates = std::max(1, s->o.max_outer) * 8;
+  int cycle_start = 0, longest = 0;
   for (;;) {
     int rc = run_chunks<float>(s, progress, user, tol);
     if (rc) return rc;
     const int kst = s->h_ks->status;
     const int it = s->h_ks->it;
+    // stopped by the iteration cap, not by a residual drop: the cycle stalled
+    const bool stalled = kst == KS_RELIABLE && !(s->h_ks->rr < s->h_ks->rr_trigger);
+    if (!stalled) longest = std::max(longest, it - cycle_start);
+    cycle_start = it;
     // fold the FP32 increment into x (ks->scale == scale), restart the increment
     launch_ir_accumulate(g, x64, v[0], s->ks, s->st);
     cudaMemsetAsync(v[0], 0, sizeof(float) * 3 * (size_t)g.n, s->st);
@@ -1067,7 +1150,7 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
     if (kst == KS_MAXIT || kst == KS_BREAKDOWN || it >= max_it || inf.outer_iters >= max_updates) break;
     // FP32 floor: stop when corrections no longer reduce the true residual
     if (ratio < 0.5 * best) { best = ratio; no_gain = 0; }
-    else if (++no_gain >= 3) break;
+    else if (++no_gain >= 6) break;
     // replace the recurrence residual by the true one and carry on
     launch_ir_replace(g, s->r64, v[1], s->ks, s->st);
     VF_CHECK_LAUNCH();
@@ -1077,11 +1160,19 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
     s->h_ks->rr = rr32;
     s->h_ks->resid = rnorm / scale;
     s->h_ks->rr_trigger = delta * delta * rr32;
+    s->h_ks->it_trigger = it + std::max(100, 3 * std::max(longest, 1));
     VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
-    // the chunk stopped inside an iteration, right after r was updated: finish
-    // that iteration on the replaced residual (z = M r, beta, p = z + beta p)
-    precondition<float>(s, v[1], v[2], s->ks);
-    update_direction<float>(s, v[1], v[2], v[3], v[4]);
+    if (stalled) {
+      // restart the direction on the replaced residual: z = M r, p = z
+      precondition<float>(s, v[1], v[2], s->ks);
+      launch_dot<float>(g, v[1], v[2], s->d_partials, s->ks, SLOT_RZ_INIT, s->st);
+      launch_copy_vec<float>(g, v[2], v[3], s->ks, s->st);
+    } else {
+      // the chunk stopped inside an iteration, right after r was updated: finish
+      // that iteration on the replaced residual (z = M r, beta, p = z + beta p)
+      precondition<float>(s, v[1], v[2], s->ks);
+      update_direction<float>(s, v[1], v[2], v[3], v[4]);
+    }
     VF_CHECK_LAUNCH();
   }
   s->history.resize(inf.iters);
@@ -1752,6 +1843,40 @@ int vf_solve_block(vf_solver* s, const double* F, int32_t k, double tol, int32_t
     }
   for (int j = 0; j < k; ++j)
     if (rcs[j] != VF_OK) return rcs[j];
+  return VF_OK;
+}
+
+int vf_solve_batch(vf_solver* const* solvers, int32_t n, const double* const* E, const double* const* nu_elem,
+                   const double* const* F, double tol, int32_t max_it, uint32_t flags, double* const* U,
+                   vf_solve_info* infos) {
+  if (!solvers || !F || !U || n < 1) return VF_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (!solvers[i] || !F[i] || !U[i] || solvers[i]->is_child) return VF_ERR_ARG;
+  std::vector<int> rcs(n, VF_OK);
+  std::vector<vf_solve_info> inf(n);
+  std::vector<std::thread> th;
+  th.reserve(n);
+  for (int i = 0; i < n; ++i) {
+    th.emplace_back([&, i]() {
+      vf_solver* s = solvers[i];
+      cudaSetDevice(s->device);
+      if (E && E[i]) {
+        rcs[i] = vf_set_material(s, E[i], nu_elem ? nu_elem[i] : nullptr, flags & VF_SOLVE_DEVICE_PTRS);
+        if (rcs[i] != VF_OK) return;
+      }
+      rcs[i] = vf_solve_cb(s, F[i], nullptr, tol, max_it, flags, U[i], &inf[i], nullptr, nullptr);
+    });
+  }
+  for (auto& t : th) t.join();
+  if (infos)
+    for (int i = 0; i < n; ++i) infos[i] = inf[i];
+  for (int i = 0; i < n; ++i)
+    if (rcs[i] != VF_OK && rcs[i] != VF_ERR_STALLED) {
+      g_last_error = "batch part " + std::to_string(i) + ": " + solvers[i]->err;
+      return rcs[i];
+    }
+  for (int i = 0; i < n; ++i)
+    if (rcs[i] != VF_OK) return rcs[i];
   return VF_OK;
 }
 

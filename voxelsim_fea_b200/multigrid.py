@@ -43,6 +43,7 @@ class SolverOptions:
     max_outer: int = 20              # mixed: cap on FP64 corrections
     mixed_mode: str = "reliable"     # mixed: "reliable" (residual replacement) | "restart" (refinement)
     flexible: bool = False           # flexible CG (automatic with a learned stage)
+    autotune: bool = True            # time z-chunk candidates of the marching kernels at set-up
     omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
     omega_rel: float = 0.8
     power_iters: int = 20
@@ -146,6 +147,7 @@ class MGSolver:
         o.coarse_storage = _lib.STENCIL_STORAGE[self.options.coarse_storage]
         o.mixed_mode = _lib.MIXED_MODES[self.options.mixed_mode]
         o.flexible = int(bool(self.options.flexible))
+        o.autotune = int(bool(self.options.autotune))
         h = ctypes.c_void_p()
         _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
                    None, "vf_create")
@@ -353,4 +355,36 @@ def _solve_block(self, Evec_full, F, tol=1e-4, max_cg=None, nu_elem=None):
 
 
 MGSolver.solve_block = _solve_block
+
+
+def solve_batch(solvers, E_list, F_list, tol=1e-4, max_cg=None, nu_list=None):
+    """Independent parts in one call (B200 extension): solver i gets E_list[i]
+    (and nu_list[i]) and F_list[i]; all parts are set up and solved
+    concurrently.  Returns the list of displacements; per-part results land in
+    each solver's ``last_info``."""
+    n = len(solvers)
+    P = ctypes.c_void_p
+    Es = [_lib.f64(np.asarray(e, dtype=float).ravel()) for e in E_list]
+    Fs = [_lib.f64(np.asarray(f, dtype=float).ravel()) for f in F_list]
+    Ns = None if nu_list is None else [None if v is None else _lib.f64(np.asarray(v, dtype=float).ravel())
+                                       for v in nu_list]
+    Us = [np.empty(s.ndof) for s in solvers]
+    for s, e, f in zip(solvers, Es, Fs):
+        if e.size != s.nelem or f.size != s.ndof:
+            raise ValueError("batch: E / F sizes do not match the solver grids")
+    h = (P * n)(*[s._handle() for s in solvers])
+    e_arr = (P * n)(*[e.ctypes.data for e in Es])
+    n_arr = None if Ns is None else (P * n)(*[None if v is None else v.ctypes.data for v in Ns])
+    f_arr = (P * n)(*[f.ctypes.data for f in Fs])
+    u_arr = (P * n)(*[u.ctypes.data for u in Us])
+    infos = (_lib.VfSolveInfo * n)()
+    rc = _lib.load().vf_solve_batch(h, n, e_arr, n_arr, f_arr, float(tol), int(max_cg or 0), 0, u_arr, infos)
+    for s, i in zip(solvers, infos):
+        s.last_info = i
+        s.last_iters = int(i.iters)
+        s.last_converged = bool(i.converged)
+        s._density_set = True
+    if rc != _lib.VF_OK:
+        raise RuntimeError(f"solve_batch failed: {_lib.load().vf_global_last_error().decode()}")
+    return Us
 MGSolver._apply_pooled = lambda self, u: self._apply(0, u)
