@@ -606,27 +606,39 @@ int autotune_levels(vf_solver* s) {
       }
     }
     const int planes = l.g.lz + 1;
+    // CTAs of a candidate; candidates that leave SMs idle while a finer split
+    // would fill them are not considered (a short level is latency bound)
+    const long long tiles = stencil ? (long long)((l.g.lx + 32) / 32) * ((l.g.ly + 8) / 8)
+                                    : (long long)((l.g.lx + 31) / 31) * ((l.g.ly + 7) / 7);
+    auto ctas = [&](int c) { return tiles * ((planes + c - 1) / c); };
+    const long long floor_ctas = std::min<long long>(148, ctas(modal ? 2 : 1));
     std::vector<int> cand;
     const int base = stencil ? sym_zchunk(l.g) : auto_zchunk(l.g, 0);
     for (int c : {base, 1, 2, 3, 4, 6, 8, 12, 16, 22, 33, 48, 65})
-      if (c >= 1 && c <= planes && (modal ? c >= 2 : true) &&
+      if (c >= 1 && c <= planes && (modal ? c >= 2 : true) && ctas(c) >= floor_ctas &&
           std::find(cand.begin(), cand.end(), c) == cand.end())
         cand.push_back(c);
+    // two passes, minimum per candidate: the first pass also brings the
+    // clocks up after the set-up, which would otherwise favour late candidates
+    std::vector<float> tmin(cand.size(), 1e30f);
+    for (int pass = 0; pass < 2; ++pass)
+      for (size_t ci = 0; ci < cand.size(); ++ci) {
+        (stencil ? l.szchunk : l.zchunk) = cand[ci];
+        level_op<float>(s, (int)li, EPI_SMOOTH, l.w32[0], l.w32[1], l.w32[3], nullptr, nullptr, 0);   // warm
+        VF_TRY(cudaEventRecord(t0, s->st));
+        for (int r = 0; r < 6; ++r)
+          level_op<float>(s, (int)li, EPI_SMOOTH, l.w32[0], l.w32[1], l.w32[3], nullptr, nullptr, 0);
+        VF_TRY(cudaEventRecord(t1, s->st));
+        VF_TRY(cudaEventSynchronize(t1));
+        VF_CHECK_LAUNCH();
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        tmin[ci] = std::min(tmin[ci], ms);
+      }
     int best = base;
     float best_ms = 1e30f;
-    for (int c : cand) {
-      (stencil ? l.szchunk : l.zchunk) = c;
-      level_op<float>(s, (int)li, EPI_SMOOTH, l.w32[0], l.w32[1], l.w32[3], nullptr, nullptr, 0);   // warm
-      VF_TRY(cudaEventRecord(t0, s->st));
-      for (int r = 0; r < 3; ++r)
-        level_op<float>(s, (int)li, EPI_SMOOTH, l.w32[0], l.w32[1], l.w32[3], nullptr, nullptr, 0);
-      VF_TRY(cudaEventRecord(t1, s->st));
-      VF_TRY(cudaEventSynchronize(t1));
-      VF_CHECK_LAUNCH();
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, t0, t1);
-      if (ms < best_ms) { best_ms = ms; best = c; }
-    }
+    for (size_t ci = 0; ci < cand.size(); ++ci)
+      if (tmin[ci] < best_ms) { best_ms = tmin[ci]; best = cand[ci]; }
     (stencil ? l.szchunk : l.zchunk) = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_cache[key] = best;

@@ -525,8 +525,10 @@ constexpr int SX = 32, SY = 8;   // node tile of the marching stencil kernel
 // barrier per plane: the slot written for plane z+1 was last read two steps
 // earlier), the next plane is prefetched into registers while the current one
 // is computed, and the stencil values stream through coalesced 16-byte loads.
+// 4 CTAs (32 warps) per SM at <= 64 registers: the kernel is latency bound on
+// its stencil loads, and more resident warps hide more of it
 template <typename T, typename S, int EPI>
-__global__ void __launch_bounds__(SX * SY, 2) k_sym_march(Grid g, OpArgs a, const S* __restrict__ stc,
+__global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, const S* __restrict__ stc,
                                                            const T* __restrict__ sqd, int zchunk) {
   using Lay = SymLayout<S>;
   using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
