@@ -421,11 +421,12 @@ def run_b200(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = sweep_bytes / (kms.value / 1e3) / 1e9
     # DRAM traffic of one launch from the ncu capture summarised in
-    # profiles/k_modal_op_smooth_fp32_bracket256.md (read + write, same workload)
+    # profiles/k_modal_op_smooth_fp32_bracket256.md (read + write, same workload;
+    # the TMA-staged form reads the same arrays once per tile)
     traffic = 188.54e6 + 34.62e6
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "traffic_unit": "B per launch (ncu)",
-                "kernel": "k_modal_op<float, SMOOTH> (fused damped-Jacobi sweep, level 0)",
+                "kernel": "k_modal_tma<float, SMOOTH> (fused damped-Jacobi sweep, level 0, TMA-staged)",
                 "ms_per_launch": kms.value, "algorithmic_bytes_per_launch": sweep_bytes,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650 GB/s",
                 "matvec_ms_per_launch": amv.value,

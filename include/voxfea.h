@@ -115,8 +115,9 @@ typedef struct vf_options {
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
-enum { VF_FINE_MODAL = 0,     /* modal z-marching kernel (vf_modal.cu) */
-       VF_FINE_GATHER = 1 };  /* node-centric 27-neighbour gather (vf_matvec.cu) */
+enum { VF_FINE_MODAL = 0,     /* modal z-marching kernel, TMA-staged (vf_modal_tma.cu) */
+       VF_FINE_GATHER = 1,    /* node-centric 27-neighbour gather (vf_matvec.cu) */
+       VF_FINE_MODAL_CPASYNC = 2 };  /* modal z-marching kernel, cp.async-staged (vf_modal.cu) */
 enum { VF_STENCIL_SYM_HALF = 0, VF_STENCIL_SYM = 1, VF_STENCIL_FULL = 2 };
 enum { VF_MIXED_RELIABLE = 0, VF_MIXED_RESTART = 1 };
 

@@ -1,4 +1,5 @@
-"""The modal z-marching fine operator (default kernel) against the CPU oracle
+"""The modal z-marching fine operator (default kernel, TMA-staged; and its
+cp.async-staged form) against the CPU oracle
 and against the 27-neighbour gather kernel, on odd-sized grids that exercise
 partial tiles in x/y and unequal z-lanes, for several z-chunk sizes, both
 epilogues that carry extra data (Jacobi sweep, residual), FP64 and FP32, and a
@@ -52,7 +53,8 @@ def test_modal_smooth_and_lame_match_gather(gpu, prec):
     rng, E, fixed, nu, ndof = _problem(nx, ny, nz, 11, lame=True)
     a = MGSolver(nx, ny, nz, fixed, nu=0.3, options=SolverOptions(fine_kernel="modal", modal_zchunk=3))
     b = MGSolver(nx, ny, nz, fixed, nu=0.3, options=SolverOptions(fine_kernel="gather"))
-    for m in (a, b):
+    c = MGSolver(nx, ny, nz, fixed, nu=0.3, options=SolverOptions(fine_kernel="modal_cpasync", modal_zchunk=5))
+    for m in (a, b, c):
         m.set_density(E, nu_elem=nu)
     free = a.levels[0]["free"]
     u = rng.standard_normal(ndof) * free
@@ -63,6 +65,9 @@ def test_modal_smooth_and_lame_match_gather(gpu, prec):
     _close(a._apply(0, u, precision=prec), b._apply(0, u, precision=prec), RTOL[prec])
     _close(a._smooth(0, u, rhs, 3, precision=prec), b._smooth(0, u, rhs, 3, precision=prec),
            10 * RTOL[prec])
+    # the TMA-staged and the cp.async-staged forms do identical arithmetic
+    np.testing.assert_array_equal(a._apply(0, u, precision=prec), c._apply(0, u, precision=prec))
+    np.testing.assert_array_equal(a._smooth(0, u, rhs, 3, precision=prec), c._smooth(0, u, rhs, 3, precision=prec))
 
 
 def test_modal_solve_matches_gather_solve(gpu):

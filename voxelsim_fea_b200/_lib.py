@@ -30,7 +30,7 @@ VF_COARSE_REDISCRETIZE, VF_COARSE_GALERKIN = 0, 1
 VF_COARSEST_JACOBI, VF_COARSEST_CHOLESKY = 0, 1
 VF_SOLVE_DEVICE_PTRS = 1
 VF_OMEGA_FIXED, VF_OMEGA_AUTO = 0, 1
-VF_FINE_MODAL, VF_FINE_GATHER = 0, 1
+VF_FINE_MODAL, VF_FINE_GATHER, VF_FINE_MODAL_CPASYNC = 0, 1, 2
 STENCIL_STORAGE = {"sym_half": 0, "sym": 1, "full": 2}
 MIXED_MODES = {"reliable": 0, "restart": 1}
 

@@ -135,6 +135,7 @@ struct OpArgs {
   int dot_slot;           // which reduction finalizes (see vf_reduce.cuh)
   const double* ke_tab;   // HOST pointer: [KE(nu) | K_lam | K_mu], 3 x 576 doubles
   const double* omega_dev;  // device: damping of this level (overrides omega when set)
+  int* err;                 // device error flag (bounded waits that expired), or nullptr
 };
 template <typename T> void launch_fine_op(const Grid& g, int epi, const OpArgs& a, cudaStream_t st);
 
@@ -145,6 +146,11 @@ ModalConst modal_constants(double nu, bool lame);
 template <typename T> void launch_modal_op(const Grid& g, int epi, const OpArgs& a, const ModalConst& mc, int ty,
                                            int zchunk, cudaStream_t st);
 template <typename T> int fine_op_grid_blocks(const Grid& g);
+// vf_modal_tma.cu -- the modal operator with TMA staging (default form);
+// returns false without launching when a tensor map cannot be built
+template <typename T> bool launch_modal_tma(const Grid& g, int epi, const OpArgs& a, const ModalConst& mc, int zchunk,
+                                            cudaStream_t st);
+bool modal_tma_supported();
 
 // vf_stencil.cu -- assembled 27-point block stencils (Galerkin levels)
 template <typename T> void launch_stencil_op(const Grid& g, int epi, const OpArgs& a, const T* stencil, cudaStream_t st);

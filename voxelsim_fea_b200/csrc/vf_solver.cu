@@ -157,6 +157,7 @@ struct vf_solver {
   int nn_level = 1;
   bool nn_on = false;
   double* d_nn_eref = nullptr;  // [0] max voxel modulus, [1..] reduction scratch
+  int* d_err = nullptr;         // kernels' error flag (expired bounded waits)
   double* d_omega = nullptr;    // damping per level (read by the smoothers)
   double* d_lambda = nullptr;   // lambda_max(D^-1 A_l) estimates (VF_OMEGA_AUTO)
   std::vector<double> h_omega, h_lambda;
@@ -253,11 +254,17 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
   a.ks = ks;
   a.dot_slot = slot;
   a.ke_tab = s->tab;
+  a.err = s->d_err;
   if (l.galerkin) {
     if (s->o.coarse_storage == VF_STENCIL_FULL) launch_stencil_op<T>(l.g, epi, a, Sel<T>::st(l), s->st);
     else level_sym_op<T>(s, l, epi, a);
-  } else if (s->o.fine_kernel == VF_FINE_GATHER) launch_fine_op<T>(l.g, epi, a, s->st);
-  else launch_modal_op<T>(l.g, epi, a, s->lame ? s->mc_lame : s->mc, 8, l.zchunk, s->st);
+  } else if (s->o.fine_kernel == VF_FINE_GATHER) {
+    launch_fine_op<T>(l.g, epi, a, s->st);
+  } else {
+    const ModalConst& mc = s->lame ? s->mc_lame : s->mc;
+    if (s->o.fine_kernel == VF_FINE_MODAL_CPASYNC || !launch_modal_tma<T>(l.g, epi, a, mc, l.zchunk, s->st))
+      launch_modal_op<T>(l.g, epi, a, mc, 8, l.zchunk, s->st);
+  }
 }
 
 // `sweeps` damped-Jacobi sweeps on x (in place, through tmp); from_zero uses
@@ -556,6 +563,7 @@ int build_levels(vf_solver* s) {
   VF_ALLOC(s->d_info, 1);
   VF_ALLOC(s->d_omega, 16);
   VF_ALLOC(s->d_nn_eref, 148 * 4 + 1);
+  VF_ALLOC(s->d_err, 1);
   VF_ALLOC(s->d_lambda, 16);
   VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
   memset(s->h_ks, 0, sizeof(KrylovState));
@@ -885,7 +893,7 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
   if (o.precision < 0 || o.precision > 2 || o.method < 0 || o.method > 1 || o.coarse_op < 0 || o.coarse_op > 1 ||
       o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0 ||
       o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0 ||
-      o.fine_kernel < 0 || o.fine_kernel > 1 || o.modal_zchunk < 0 || o.coarse_storage < 0 ||
+      o.fine_kernel < 0 || o.fine_kernel > 2 || o.modal_zchunk < 0 || o.coarse_storage < 0 ||
       o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 1) {
     g_last_error = "invalid vf_options field";
     return VF_ERR_ARG;
@@ -1355,6 +1363,14 @@ extern "C" int vf_solve_cb(vf_solver* s, const double* f, const double* x0, doub
   VF_TRY(cudaEventRecord(s->ev1, s->st));
   VF_TRY(cudaEventSynchronize(s->ev1));
   inf.true_resid = fnorm > 0.0 ? s->h_ks->resid : 0.0;
+  {
+    int kerr = 0;
+    VF_TRY(cudaMemcpy(&kerr, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (kerr) {
+      s->err = "a kernel's bounded wait on its TMA pipeline expired (results invalid)";
+      return VF_ERR_CUDA;
+    }
+  }
   float ms = 0.f;
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   inf.device_ms = ms;
@@ -1787,6 +1803,7 @@ int make_child(vf_solver* m, vf_solver** out) {
     VF_ALLOC(s->ks, 1);
     VF_ALLOC(s->d_partials, 148 * 64);
     VF_ALLOC(s->d_info, 1);
+    VF_ALLOC(s->d_err, 1);
     VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
     memset(s->h_ks, 0, sizeof(KrylovState));
     int rc = ensure_hist(s, 4096);

@@ -47,7 +47,7 @@ class SolverOptions:
     omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
     omega_rel: float = 0.8
     power_iters: int = 20
-    fine_kernel: str = "modal"       # "modal" (z-marching, default) | "gather" (27-neighbour)
+    fine_kernel: str = "modal"       # "modal" (z-marching, TMA) | "modal_cpasync" | "gather" (27-neighbour)
     modal_zchunk: int = 0            # z-planes per CTA of the modal kernel (0 = automatic)
     coarse_storage: str = "sym_half"  # Galerkin stencils: "sym_half" | "sym" | "full"
 
@@ -142,7 +142,8 @@ class MGSolver:
         o.omega_mode = {"fixed": _lib.VF_OMEGA_FIXED, "auto": _lib.VF_OMEGA_AUTO}[self.options.omega_mode]
         o.omega_rel = float(self.options.omega_rel)
         o.power_iters = int(self.options.power_iters)
-        o.fine_kernel = {"modal": _lib.VF_FINE_MODAL, "gather": _lib.VF_FINE_GATHER}[self.options.fine_kernel]
+        o.fine_kernel = {"modal": _lib.VF_FINE_MODAL, "gather": _lib.VF_FINE_GATHER,
+                         "modal_cpasync": _lib.VF_FINE_MODAL_CPASYNC}[self.options.fine_kernel]
         o.modal_zchunk = int(self.options.modal_zchunk)
         o.coarse_storage = _lib.STENCIL_STORAGE[self.options.coarse_storage]
         o.mixed_mode = _lib.MIXED_MODES[self.options.mixed_mode]
