@@ -421,9 +421,8 @@ def run_b200(args):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = sweep_bytes / (kms.value / 1e3) / 1e9
     # DRAM traffic of one launch from the ncu capture summarised in
-    # profiles/k_modal_op_smooth_fp32_bracket256.md (read + write, same workload;
-    # the TMA-staged form reads the same arrays once per tile)
-    traffic = 188.54e6 + 34.62e6
+    # profiles/k_modal_tma_smooth_fp32_bracket256.md (read + write, same workload)
+    traffic = 184.44e6 + 34.92e6
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "traffic_unit": "B per launch (ncu)",
                 "kernel": "k_modal_tma<float, SMOOTH> (fused damped-Jacobi sweep, level 0, TMA-staged)",
