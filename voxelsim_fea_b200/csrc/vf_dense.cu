@@ -271,8 +271,7 @@ void dense_prepare_smem(int n) {
 template <typename T>
 void launch_dense_solve(const Grid& c, const double* Ainv, int n, const T* b, T* x, const KrylovState* ks,
                         cudaStream_t st) {
-  int blocks = (n + 7) / 8;
-  if (blocks > 148 * 2) blocks = 148 * 2;
+  int blocks = (n + 7) / 8;   // one row per warp: every row's stream in flight at once
   launch_k(k_dense_solve<T>, blocks, 256, sizeof(double) * n, st, c, Ainv, n, b, x, ks);
 }
 template void launch_dense_solve<double>(const Grid&, const double*, int, const double*, double*, const KrylovState*, cudaStream_t);

@@ -267,9 +267,11 @@ __global__ void __launch_bounds__(TX * TY, 2) k_modal_op(Grid g, OpArgs a, Modal
                 const T u2 = O::lane(Sp.u[2][ty][tx], l);
                 const T d0 = O::lane(Sp.d[0][dy][tx], l), d1 = O::lane(Sp.d[1][dy][tx], l);
                 const T d2 = O::lane(Sp.d[2][dy][tx], l);
-                out[p3] = u0 + ((m8 & 1) ? w * (d0 * (b0 - k0)) : (T)0);
-                out[p3 + 1] = u1 + ((m8 & 2) ? w * (d1 * (b1 - k1)) : (T)0);
-                out[p3 + 2] = u2 + ((m8 & 4) ? w * (d2 * (b2 - k2)) : (T)0);
+                const T o0 = u0 + ((m8 & 1) ? w * (d0 * (b0 - k0)) : (T)0);
+                const T o1 = u1 + ((m8 & 2) ? w * (d1 * (b1 - k1)) : (T)0);
+                const T o2 = u2 + ((m8 & 4) ? w * (d2 * (b2 - k2)) : (T)0);
+                out[p3] = o0; out[p3 + 1] = o1; out[p3 + 2] = o2;
+                if (a.dot_partials) dot += (double)b0 * (double)o0 + (double)b1 * (double)o1 + (double)b2 * (double)o2;
               } else {
                 out[p3] = b0 - k0; out[p3 + 1] = b1 - k1; out[p3 + 2] = b2 - k2;
               }
@@ -300,7 +302,9 @@ __global__ void __launch_bounds__(TX * TY, 2) k_modal_op(Grid g, OpArgs a, Modal
       for (int m = 0; m < 4; ++m) Fb[c][m] = Fa[c][m];
   }
   cp_async_wait<0>();
-  if (EPI == EPI_APPLY && a.dot_partials && ks) reduce_and_finalize(dot, a.dot_partials, ks, a.dot_slot, nullptr);
+  // APPLY: u.y (p.Ap); SMOOTH: b.u' (the V-cycle's last sweep: r.z)
+  if ((EPI == EPI_APPLY || EPI == EPI_SMOOTH) && a.dot_partials && ks)
+    reduce_and_finalize(dot, a.dot_partials, ks, a.dot_slot, nullptr);
 }
 
 template <typename T, int TY, bool LAME, int EPI>

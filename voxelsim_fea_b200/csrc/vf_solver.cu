@@ -269,8 +269,10 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
 
 // `sweeps` damped-Jacobi sweeps on x (in place, through tmp); from_zero uses
 // the exact first sweep x = w*Minv*b.
+// dot_slot >= 0: the last sweep also reduces b.x into that slot (modal kernels)
 template <typename T>
-void smooth(vf_solver* s, int li, T* x, T* tmp, const T* b, int sweeps, bool from_zero, KrylovState* ks) {
+void smooth(vf_solver* s, int li, T* x, T* tmp, const T* b, int sweeps, bool from_zero, KrylovState* ks,
+            int dot_slot = -1) {
   Level& l = s->L[li];
   if (sweeps <= 0) {
     if (from_zero) cudaMemsetAsync(x, 0, sizeof(T) * 3 * (size_t)l.g.n, s->st);
@@ -289,7 +291,8 @@ void smooth(vf_solver* s, int li, T* x, T* tmp, const T* b, int sweeps, bool fro
   }
   for (int k = 0; k < rest; ++k) {
     T* nxt = (cur == x) ? tmp : x;
-    level_op<T>(s, li, EPI_SMOOTH, cur, nxt, b, ks, nullptr, 0);
+    const bool last_dot = dot_slot >= 0 && k + 1 == rest;
+    level_op<T>(s, li, EPI_SMOOTH, cur, nxt, b, ks, last_dot ? s->d_partials : nullptr, last_dot ? dot_slot : 0);
     cur = nxt;
   }
   if (cur != x) launch_copy_vec<T>(l.g, cur, x, ks, s->st);
@@ -305,9 +308,10 @@ void coarse_solve(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
   }
 }
 
-// x = V-cycle(b) on level li (core/multigrid.py:426-436).
+// x = V-cycle(b) on level li (core/multigrid.py:426-436); dot_slot >= 0: the
+// last sweep on this level also reduces b.x (r.z of the PCG) into that slot.
 template <typename T>
-void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
+void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks, int dot_slot = -1) {
   Level& l = s->L[li];
   if (li == (int)s->L.size() - 1) {
     coarse_solve<T>(s, li, b, x, ks);
@@ -321,7 +325,7 @@ void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
   launch_restrict<T>(l.g, res, c.g, c.mask, Sel<T>::w(c, 3), ks, s->st);
   vcycle<T>(s, li + 1, Sel<T>::w(c, 3), Sel<T>::w(c, 0), ks);
   launch_prolong_add<T>(c.g, Sel<T>::w(c, 0), l.g, l.mask, x, ks, s->st);
-  smooth<T>(s, li, x, tmp, b, s->o.n_smooth, false, ks);
+  smooth<T>(s, li, x, tmp, b, s->o.n_smooth, false, ks, dot_slot);
 }
 
 template <typename T> T** kvec(vf_solver* s);
@@ -368,10 +372,17 @@ void learned_stage(vf_solver* s, const T* r, T* z, KrylovState* ks) {
   launch_axpy_gamma<T>(l0.g, z, c, kk, skip, s->st);
 }
 
+// PCG's r.z can come out of the V-cycle's last fine sweep (its rhs is r, its
+// output z): modal fine kernels, a fixed preconditioner, at least one sweep.
+bool fused_rz(const vf_solver* s) {
+  return use_mg(s) && !flexible(s) && s->o.n_smooth >= 1 && s->L.size() > 1 &&
+         (s->o.fine_kernel == VF_FINE_MODAL || s->o.fine_kernel == VF_FINE_MODAL_CPASYNC);
+}
+
 template <typename T>
-void precondition(vf_solver* s, const T* r, T* z, KrylovState* ks) {
+void precondition(vf_solver* s, const T* r, T* z, KrylovState* ks, int dot_slot = -1) {
   if (use_mg(s)) {
-    vcycle<T>(s, 0, r, z, ks);
+    vcycle<T>(s, 0, r, z, ks, dot_slot);
     if (s->nn_on) learned_stage<T>(s, r, z, ks);
   } else {
     launch_jacobi_precond<T>(s->L[0].g, r, Sel<T>::minv(s->L[0]), s->L[0].mask, z, ks, s->st);
@@ -379,11 +390,12 @@ void precondition(vf_solver* s, const T* r, T* z, KrylovState* ks) {
 }
 
 // After z = M r: the beta reduction (PCG r.z, or flexible (r.z, z.Ap)) and p = z + beta p.
+// (with fused_rz the PCG r.z was reduced by the V-cycle's last sweep)
 template <typename T>
 void update_direction(vf_solver* s, const T* r, const T* z, T* p, const T* Ap) {
   const Grid& g = s->L[0].g;
   if (flexible(s)) launch_dot_fcg<T>(g, r, z, Ap, s->d_partials, s->ks, s->st);
-  else launch_dot<T>(g, r, z, s->d_partials, s->ks, SLOT_RZ, s->st);
+  else if (!fused_rz(s)) launch_dot<T>(g, r, z, s->d_partials, s->ks, SLOT_RZ, s->st);
   launch_p_update<T>(g, p, z, s->ks, s->st);
 }
 
@@ -396,7 +408,7 @@ void pcg_iteration(vf_solver* s) {
   // the fine operator (level 0), masked, fused with p.Ap -> alpha
   level_op<T>(s, 0, EPI_APPLY, p, Ap, nullptr, s->ks, s->d_partials, SLOT_PAP);
   launch_cg_update<T>(g, x, p, r, Ap, s->d_partials, s->ks, s->d_hist, s->st);
-  precondition<T>(s, r, z, s->ks);
+  precondition<T>(s, r, z, s->ks, fused_rz(s) ? SLOT_RZ : -1);
   update_direction<T>(s, r, z, p, Ap);
 }
 
@@ -508,6 +520,20 @@ int map_status(int ks) {
 // ---------------------------------------------------------------------------
 // set-up
 // ---------------------------------------------------------------------------
+// Partial sums of the fused reductions: one (or two) doubles per CTA of the
+// largest grid any reducing kernel can get -- the marching kernels at the
+// smallest z-chunk the autotuner may pick, or the fixed vector grid.
+size_t partials_needed(const vf_solver* s) {
+  size_t m = 2 * (size_t)kVecBlocks;
+  for (const auto& l : s->L) {
+    const size_t planes = (size_t)l.g.lz + 1;
+    const size_t modal = (size_t)((l.g.lx + 31) / 31) * ((l.g.ly + 7) / 7) * planes;
+    const size_t sym = (size_t)((l.g.lx + 32) / 32) * ((l.g.ly + 8) / 8) * planes;
+    m = std::max(m, std::max(modal, sym));
+  }
+  return std::max<size_t>(m, 148 * 64);
+}
+
 int build_levels(vf_solver* s) {
   auto dims = level_dims(s->nx, s->ny, s->nz, s->o.min_elems, s->o.max_levels);
   if (s->o.method != VF_METHOD_MG) dims.resize(1);
@@ -559,7 +585,7 @@ int build_levels(vf_solver* s) {
   VF_ALLOC(s->d_active_pad, (size_t)g0.n);
   VF_ALLOC(s->d_allfree, (size_t)g0.n);
   VF_ALLOC(s->ks, 1);
-  VF_ALLOC(s->d_partials, 148 * 64);
+  VF_ALLOC(s->d_partials, partials_needed(s));
   VF_ALLOC(s->d_info, 1);
   VF_ALLOC(s->d_omega, 16);
   VF_ALLOC(s->d_nn_eref, 148 * 4 + 1);
@@ -1190,7 +1216,7 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
     } else {
       // the chunk stopped inside an iteration, right after r was updated: finish
       // that iteration on the replaced residual (z = M r, beta, p = z + beta p)
-      precondition<float>(s, v[1], v[2], s->ks);
+      precondition<float>(s, v[1], v[2], s->ks, fused_rz(s) ? SLOT_RZ : -1);
       update_direction<float>(s, v[1], v[2], v[3], v[4]);
     }
     VF_CHECK_LAUNCH();
@@ -1801,7 +1827,7 @@ int make_child(vf_solver* m, vf_solver** out) {
     VF_ALLOC(s->d_ref_b, nref);
     VF_ALLOC(s->d_ref_c, nref);
     VF_ALLOC(s->ks, 1);
-    VF_ALLOC(s->d_partials, 148 * 64);
+    VF_ALLOC(s->d_partials, partials_needed(s));
     VF_ALLOC(s->d_info, 1);
     VF_ALLOC(s->d_err, 1);
     VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
