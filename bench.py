@@ -368,6 +368,7 @@ def run_b200(args):
 
     sampler = ClockSampler(local) if rank == 0 else None
     ms, (iters, true_resid, outer), clocks, launches = timed(fast, args.steps, args.warmup, sampler)
+    setup_ms = float(info.setup_ms) if K == 1 else None   # set-up part of the last timed step
     if not (true_resid < TOL):
         # a solve that did not reach the tolerance is not a time-to-solution
         raise SystemExit(f"bench: solve did not reach tol={TOL:g} (true residual {true_resid:.3e}, "
@@ -468,6 +469,7 @@ def run_b200(args):
                        "tol": TOL, "l2": "working set > 126 MB L2 (vectors 54-107 MB each)",
                        "parallelism": f"replicas x{world}"},
             "iterations": iters, "outer_iterations": outer, "true_resid": true_resid,
+            "setup_ms_per_step": setup_ms,
             "time_to_solution_s": ms / 1e3,
             "plain_fp64": plain,
             "learned_mixed": learned,

@@ -147,8 +147,14 @@ __global__ void k_trsm_update(const double* A, double* Y, int n, int k, int nb, 
 }
 
 // Ainv = Y^T Y (Y lower triangular): Ainv[i][j] = sum_{l >= max(i,j)} Y[l][i] Y[l][j].
+// A^-1 = Y^T Y is symmetric: one CTA per 32x32 tile of the lower triangle
+// (blockIdx.x enumerates the pairs bi >= bj), written to both triangles.
 __global__ void k_yty(const double* Y, double* Ainv, int n) {
-  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  int bi = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
+  while ((bi + 1) * (bi + 2) / 2 <= (int)blockIdx.x) ++bi;
+  while (bi * (bi + 1) / 2 > (int)blockIdx.x) --bi;
+  const int bj = (int)blockIdx.x - bi * (bi + 1) / 2;
+  const int i0 = bi * 32, j0 = bj * 32;
   __shared__ double Yi[32][33], Yj[32][33];
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
   double acc[4] = {0, 0, 0, 0};
@@ -170,7 +176,10 @@ __global__ void k_yty(const double* Y, double* Ainv, int n) {
   }
   for (int q = 0; q < 4; ++q) {
     const int i = i0 + ty + 8 * q, j = j0 + tx;
-    if (i < n && j < n) Ainv[(long long)i * n + j] = acc[q];
+    if (i < n && j < n) {
+      Ainv[(long long)i * n + j] = acc[q];
+      Ainv[(long long)j * n + i] = acc[q];
+    }
   }
 }
 
@@ -252,9 +261,9 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
       launch_k(k_trsm_update, dim3((ncol + 31) / 32, (rest + 31) / 32), 256, 0, st, A, work, n, k, nb, ncol);
     }
   }
-  // A <- Y^T Y
+  // A <- Y^T Y (lower-triangle tiles, mirrored)
   const int tiles = (n + 31) / 32;
-  launch_k(k_yty, dim3(tiles, tiles), 256, 0, st, work, A, n);
+  launch_k(k_yty, dim3(tiles * (tiles + 1) / 2), 256, 0, st, work, A, n);
   return 0;
 }
 
