@@ -107,6 +107,8 @@ template <> struct Sel<float> {
 struct vf_solver {
   int device = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;   // set-up work that overlaps the main stream (coarsest factorization)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   vf_options o{};
   double nu = 0.3;
   int nx = 0, ny = 0, nz = 0;
@@ -589,6 +591,19 @@ int build_levels(vf_solver* s) {
   VF_ALLOC(s->d_info, 1);
   VF_ALLOC(s->d_omega, 16);
   VF_ALLOC(s->d_nn_eref, 148 * 4 + 1);
+  // coarsest dense factor: allocated (and zeroed on st) here, because it is
+  // built on the second set-up stream, which does not wait for st's memsets
+  if (use_mg(s) && s->o.coarsest == VF_COARSEST_CHOLESKY) {
+    Level& lc = s->L.back();
+    const int n = 3 * lc.g.nodes_ref();
+    if (n <= 16384) {
+      VF_ALLOC(s->d_Ainv, (size_t)n * n);
+      VF_ALLOC(s->d_dense_work, (size_t)n * n);
+      s->dense_n = n;
+      dense_prepare_smem(n);
+      if (!lc.galerkin && !lc.st64) VF_ALLOC(lc.st64, 243 * (size_t)lc.g.n);
+    }
+  }
   VF_ALLOC(s->d_err, 1);
   VF_ALLOC(s->d_lambda, 16);
   VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
@@ -757,12 +772,21 @@ int set_level_omegas(vf_solver* s) {
     launch_power_omega(s->ks, s->o.omega_rel, 1.1, s->d_omega + li, s->d_lambda + li, s->st);
   }
   VF_CHECK_LAUNCH();
+  return VF_OK;   // h_omega / h_lambda are read back by fetch_level_omegas (a blocking copy)
+}
+
+int fetch_level_omegas(vf_solver* s) {
+  const int nl = (int)s->h_omega.size();
+  if (s->o.omega_mode != VF_OMEGA_AUTO || !use_mg(s) || nl == 0) return VF_OK;
   VF_TRY(cudaMemcpyAsync(s->h_omega.data(), s->d_omega, sizeof(double) * nl, cudaMemcpyDeviceToHost, s->st));
   VF_TRY(cudaMemcpyAsync(s->h_lambda.data(), s->d_lambda, sizeof(double) * nl, cudaMemcpyDeviceToHost, s->st));
   return VF_OK;
 }
 
+// Runs on s->st2 (the coarsest stencil is final when it starts; see
+// vf_set_material), so the factorization overlaps the damping estimates.
 int build_dense_coarsest(vf_solver* s) {
+  cudaStream_t sd = s->st2 ? s->st2 : s->st;
   Level& lc = s->L.back();
   const int n = 3 * lc.g.nodes_ref();
   if (n > 16384) {
@@ -782,14 +806,14 @@ int build_dense_coarsest(vf_solver* s) {
     if (!lc.st64) VF_ALLOC(lc.st64, 243 * (size_t)lc.g.n);
     st = lc.st64;
     launch_stencil_from_elements(lc.g, lc.E64, s->lame ? lc.mu64 : nullptr, lc.mask, st,
-                                 s->lame ? s->d_Ktab_lame : s->d_Ktab, s->lame ? 1 : 0, s->st);
+                                 s->lame ? s->d_Ktab_lame : s->d_Ktab, s->lame ? 1 : 0, sd);
   }
-  dense_assemble(lc.g, st, lc.mask, s->d_Ainv, n, s->st);
-  dense_cholesky_inverse(s->d_Ainv, s->d_dense_work, n, s->d_info, s->st);
+  dense_assemble(lc.g, st, lc.mask, s->d_Ainv, n, sd);
+  dense_cholesky_inverse(s->d_Ainv, s->d_dense_work, n, s->d_info, sd);
   VF_CHECK_LAUNCH();
   int info = 0;
-  VF_TRY(cudaMemcpyAsync(&info, s->d_info, sizeof(int), cudaMemcpyDeviceToHost, s->st));
-  VF_TRY(cudaStreamSynchronize(s->st));
+  VF_TRY(cudaMemcpyAsync(&info, s->d_info, sizeof(int), cudaMemcpyDeviceToHost, sd));
+  VF_TRY(cudaStreamSynchronize(sd));
   if (info != 0) {
     s->err = "coarsest-level Cholesky: non-positive pivot at row " + std::to_string(info - 1) +
              " (singular coarse operator: is the part supported?)";
@@ -900,6 +924,9 @@ int vf_destroy(vf_solver* s) {
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->ev2) cudaEventDestroy(s->ev2);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->st2) { cudaStreamSynchronize(s->st2); cudaStreamDestroy(s->st2); }
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
   return VF_OK;
@@ -939,10 +966,16 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
     return code;
   };
   if (cudaSetDevice(s->device) != cudaSuccess) { s->err = "cudaSetDevice failed"; return fail(VF_ERR_CUDA); }
-  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) { s->err = "stream"; return fail(VF_ERR_CUDA); }
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking) != cudaSuccess) {
+    s->err = "stream";
+    return fail(VF_ERR_CUDA);
+  }
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
   cudaEventCreate(&s->ev2);
+  cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming);
   if ((rc = build_levels(s))) return fail(rc);
   if ((rc = upload_tables(s))) return fail(rc);
   s->h_mask_ref.assign((size_t)s->L[0].g.nodes_ref(), kFreeAll);
@@ -1075,12 +1108,24 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
     launch_convert<double, float>(l.minv64, l.minv32, 3 * n, s->st);
   }
   VF_CHECK_LAUNCH();
+  // the coarsest factorization (second stream) overlaps the damping estimates
+  const bool dense = use_mg(s) && s->o.coarsest == VF_COARSEST_CHOLESKY;
+  if (dense) {
+    VF_TRY(cudaEventRecord(s->ev_fork, s->st));
+    VF_TRY(cudaStreamWaitEvent(s->st2, s->ev_fork, 0));
+  }
   {
     int rc = set_level_omegas(s);
     if (rc) return rc;
   }
-  if (use_mg(s) && s->o.coarsest == VF_COARSEST_CHOLESKY) {
-    int rc = build_dense_coarsest(s);
+  if (dense) {
+    int rc = build_dense_coarsest(s);   // synchronises st2 (pivot check) while st keeps running
+    if (rc) return rc;
+    VF_TRY(cudaEventRecord(s->ev_join, s->st2));
+    VF_TRY(cudaStreamWaitEvent(s->st, s->ev_join, 0));
+  }
+  {
+    int rc = fetch_level_omegas(s);
     if (rc) return rc;
   }
   if (s->nn) nn_refresh_features(s);
