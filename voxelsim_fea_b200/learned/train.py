@@ -187,7 +187,15 @@ def eval_configs():
             ("learned_mixed", SolverOptions.fast(), True))
 
 
-def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None):
+def headline_configs():
+    """The comparison BASELINE names: plain FP64 GMG-PCG, mixed, learned + mixed."""
+    from ..multigrid import SolverOptions
+    return (("plain_fp64", SolverOptions.robust(), False),
+            ("mixed", SolverOptions.fast(), False),
+            ("learned_mixed", SolverOptions.fast(), True))
+
+
+def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None, max_cg=None):
     """Solve held-out parts without and with the learned stage (FP64 and
     mixed precision); per-part iterations and device times."""
     from ..multigrid import MGSolver
@@ -203,8 +211,8 @@ def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None):
             m.set_density(part["E"], nu_elem=part["nu"])
             if use:
                 stage.configure(m, params, level, True)
-            m.solve(part["E"], part["f"], tol=tol, nu_elem=part["nu"])   # warm (graph capture)
-            m.solve(part["E"], part["f"], tol=tol, nu_elem=part["nu"])
+            m.solve(part["E"], part["f"], tol=tol, nu_elem=part["nu"], max_cg=max_cg)   # warm (graph capture)
+            m.solve(part["E"], part["f"], tol=tol, nu_elem=part["nu"], max_cg=max_cg)
             inf = m.last_info
             row[name] = {"iters": int(inf.iters), "solve_ms": float(inf.device_ms),
                          "true_resid": float(inf.true_resid), "converged": bool(inf.converged)}
@@ -230,8 +238,24 @@ def main():
     ap.add_argument("--eval", type=int, default=0, help="held-out parts to evaluate")
     ap.add_argument("--eval-size", type=int, default=192)
     ap.add_argument("--eval-json", type=str, default=None)
+    ap.add_argument("--eval-only", action="store_true", help="evaluate the packaged weights, no training")
+    ap.add_argument("--max-cg", type=int, default=3000)
     args = ap.parse_args()
     from . import stage
+    if args.eval_only:
+        params, level = stage.load_weights()
+        seeds = [9_000_000 + 7919 * i for i in range(args.eval)]
+        e = args.eval_size
+        rows = evaluate(params, level, seeds, (e, e, e), configs=headline_configs(), max_cg=args.max_cg)
+        summary = {k: {"iters_mean": float(np.mean([r[k]["iters"] for r in rows])),
+                       "solve_ms_mean": float(np.mean([r[k]["solve_ms"] for r in rows])),
+                       "converged": int(sum(r[k]["converged"] for r in rows))}
+                   for k, _, _ in headline_configs()}
+        print(json.dumps(summary), flush=True)
+        if args.eval_json:
+            with open(args.eval_json, "w") as fh:
+                json.dump({"rows": rows, "summary": summary}, fh, indent=1)
+        return
     sizes = tuple(int(v) for v in args.sizes.split(","))
     snaps = tuple(int(v) for v in args.snapshots.split(","))
     net, hist, secs = train(args.parts, args.level, snaps, args.steps_per_part, lr=args.lr, seed=args.seed,
