@@ -302,6 +302,27 @@ int vf_solve_batch(vf_solver* const* solvers, int32_t n, const double* const* E,
                    const double* const* nu_elem, const double* const* F, double tol,
                    int32_t max_it, uint32_t flags, double* const* U, vf_solve_info* infos);
 
+/* Per-element displacement field of the result views (core/solve_worker.py:374-388):
+ * disp_out[e] = mean over the 8 corners of |u_node| (FP32, element order
+ * iz-fastest); u: 3 values per node, reference node order (host arrays). */
+int vf_element_displacement(int32_t nx, int32_t ny, int32_t nz, const double* u, float* disp_out);
+
+/* ---- voxelization: point-in-mesh inside test ------------------------------------
+ * The reference's parity ray cast (core/inside_worker.py:_inside_mask_numpy,
+ * lines 105-147) on the device with its FP64 arithmetic in its evaluation order:
+ * the masks are the reference's bit for bit.  verts (nv x 3), faces (nf x 3,
+ * indices checked), dir3 = the ray direction (the reference's default is
+ * (1, 0.0073301, 0.0031337) normalised).  Host arrays; out: one byte per point. */
+int vf_inside_points(const double* verts, int64_t nv, const int64_t* faces, int64_t nf,
+                     const double* points, int64_t npts, const double* dir3, uint8_t* out);
+/* The same for the voxel centers (target 0, element order iz-fastest) or the
+ * grid nodes (target 1, node order x-fastest) of a dims3 grid at origin3 with
+ * voxel size vsize (inside_worker.py:voxel_centers / node_coords), the points
+ * generated on the device. */
+int vf_inside_grid(const double* verts, int64_t nv, const int64_t* faces, int64_t nf,
+                   const int32_t* dims3, const double* origin3, double vsize, int32_t target,
+                   const double* dir3, uint8_t* out);
+
 /* ---- learned preconditioner stage: BF16 tensor-core 3x3x3 convolutions --------
  * No counterpart in the reference (its solver has no learned part).  Building
  * blocks of the U-Net trained by voxelsim_fea_b200.learned and run inside the

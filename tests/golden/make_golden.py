@@ -106,6 +106,107 @@ def _islands_case(fea):
             "n_removed": n_removed}
 
 
+def box_mesh(lo, hi):
+    """Closed triangulated axis-aligned box (12 outward triangles)."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], dtype=float)
+    f = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4],
+                  [1, 2, 6], [1, 6, 5], [2, 3, 7], [2, 7, 6], [3, 0, 4], [3, 4, 7]], dtype=np.int64)
+    return v, f
+
+
+def torus_mesh(R, r, nu_, nv_, center):
+    """Closed triangulated torus around z (a part with a through-hole)."""
+    a = np.linspace(0, 2 * np.pi, nu_, endpoint=False)
+    b = np.linspace(0, 2 * np.pi, nv_, endpoint=False)
+    A, B = np.meshgrid(a, b, indexing="ij")
+    v = np.stack([(R + r * np.cos(B)) * np.cos(A), (R + r * np.cos(B)) * np.sin(A), r * np.sin(B)], -1).reshape(-1, 3)
+    v = v + np.asarray(center, dtype=float)
+    f = []
+    for i in range(nu_):
+        for j in range(nv_):
+            p, q = i * nv_ + j, ((i + 1) % nu_) * nv_ + j
+            p2, q2 = i * nv_ + (j + 1) % nv_, ((i + 1) % nu_) * nv_ + (j + 1) % nv_
+            f += [[p, q, q2], [p, q2, p2]]
+    return v, np.asarray(f, dtype=np.int64)
+
+
+def _inside_case(ref):
+    """Voxelization: the reference's parity ray cast on three closed meshes,
+    for random points, voxel centers and grid nodes (inside_worker.py)."""
+    from core import inside_worker as iw
+    rng = np.random.default_rng(31)
+    out = {}
+    meshes = {"box": box_mesh((0.013, 0.021, 0.017), (0.91, 0.57, 0.43)),
+              "torus": torus_mesh(0.31, 0.11, 24, 12, (0.5, 0.5, 0.25)),
+              "tilted": None}
+    v, f = box_mesh((0.1, 0.1, 0.1), (0.7, 0.5, 0.4))
+    th = 0.37
+    rot = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1.0]])
+    meshes["tilted"] = (v @ rot.T + np.array([0.2, 0.05, 0.03]), f)
+    dims, origin, vsize = (23, 17, 11), np.array([-0.031, -0.017, -0.009]), 0.047
+    centers = iw.voxel_centers(dims, origin, vsize)
+    nodes = iw.node_coords(dims, origin, vsize)
+    for name, (v, f) in meshes.items():
+        pts = rng.uniform(-0.1, 1.1, size=(3000, 3))
+        out[f"{name}_verts"] = v
+        out[f"{name}_faces"] = f
+        out[f"{name}_points"] = pts
+        out[f"{name}_in_points"] = iw._inside_mask_numpy(v, f, pts)
+        out[f"{name}_in_centers"] = iw._inside_mask_numpy(v, f, centers)
+        out[f"{name}_in_nodes"] = iw._inside_mask_numpy(v, f, nodes)
+    out["dims"] = np.array(dims)
+    out["origin"] = origin
+    out["vsize"] = np.array(vsize)
+    out["centers"] = centers
+    out["nodes"] = nodes
+    out["ray_dir"] = iw._RAY_DIR
+    return out
+
+
+def _worker_job():
+    """A complete solve job in the reference's job.pkl format: a 28x10x8 grid,
+    a box part with a box exclusion, a bearing box at x = 0 clamping x/y/z, a
+    load box at x = max with 1 kN in -z."""
+    vsize = 0.002
+    dims = (28, 10, 8)
+    origin = np.array([0.0, 0.0, 0.0])
+    part = box_mesh((0.0005, 0.0005, 0.0005), (0.0555, 0.0195, 0.0155))
+    excl = box_mesh((0.020, -0.01, 0.009), (0.030, 0.03, 0.02))
+    bearing = box_mesh((-0.001, -0.001, -0.001), (0.0015, 0.021, 0.017))
+    load = box_mesh((0.0545, -0.001, -0.001), (0.0575, 0.021, 0.017))
+    qs = [(part, "centers"), (excl, "centers"), (bearing, "nodes"), (load, "nodes")]
+    return {"grid": {"dims": dims, "origin": origin, "vsize": vsize}, "direction": None,
+            "queries": [{"verts": v, "faces": f, "target": t} for (v, f), t in qs],
+            "descr": [("build", None), ("exclude", None), ("bearing", (True, True, True)),
+                      ("load", (0.0, 0.0, -1000.0))],
+            "material": {"youngs_modulus": 200e9, "poisson": 0.3, "yield_strength": 250e6},
+            "compute_mode": "CPU"}
+
+
+def _worker_case(ref):
+    """The reference worker end to end (job.pkl -> final.pkl)."""
+    import pickle
+    import tempfile
+    from core import solve_worker
+    job = _worker_job()
+    with tempfile.TemporaryDirectory() as d:
+        jp = os.path.join(d, "job.pkl")
+        with open(jp, "wb") as fh:
+            pickle.dump(job, fh)
+        solve_worker._worker_main(jp, d)
+        with open(os.path.join(d, "final.pkl"), "rb") as fh:
+            final = pickle.load(fh)
+    keep = {}
+    for k, v in final.items():
+        if v is None or isinstance(v, str):
+            continue
+        keep[k] = np.asarray(v)
+    return keep
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -131,6 +232,8 @@ def main():
                         n_levels=c6["n_levels"], u_tip=c6["u"][2::3].min())
     np.savez_compressed(os.path.join(HERE, "noise_32x16x16_jacobi.npz"), **_noise_case(fea, multigrid))
     np.savez_compressed(os.path.join(HERE, "islands_12x10x8.npz"), **_islands_case(fea))
+    np.savez_compressed(os.path.join(HERE, "inside_cases.npz"), **_inside_case(args.ref))
+    np.savez_compressed(os.path.join(HERE, "worker_28x10x8.npz"), **_worker_case(args.ref))
     print("cantilever L3 iters", c3["iters"], "L6 iters", c6["iters"],
           "max vm", c3["vm"].max())
 

@@ -65,3 +65,23 @@ def test_create_rejects_bad_args(lib):
     o.struct_size = 3
     assert lib.vf_create(4, 4, 4, 0.3, ctypes.byref(o), ctypes.byref(h)) == _lib.VF_ERR_ARG
     assert not h.value
+
+
+def test_grid_assembly_matches_reference_semantics():
+    """solve_worker.assemble (host bookkeeping) on role masks: active = build &
+    ~exclude, fixed DOFs per bearing axis flags, load split evenly over the
+    load nodes (solve_worker.py:242-270)."""
+    from voxelsim_fea_b200.solve_worker import assemble
+    dims = (2, 1, 1)
+    nn = 3 * 2 * 2
+    build = np.array([True, True])
+    excl = np.array([False, True])
+    bearing = np.zeros(nn, dtype=bool)
+    bearing[[0, 3]] = True
+    load = np.zeros(nn, dtype=bool)
+    load[[2, 5, 11]] = True
+    descr = [("build", None), ("exclude", None), ("bearing", (True, False, True)), ("load", (3.0, 0.0, -6.0))]
+    active, fixed, f = assemble(descr, [build, excl, bearing, load], dims)
+    np.testing.assert_array_equal(active, [True, False])
+    np.testing.assert_array_equal(fixed, [0, 2, 9, 11])
+    assert f[3 * 2] == 1.0 and f[3 * 5 + 2] == -2.0 and f[3 * 11] == 1.0 and abs(f.sum() - (-3.0)) < 1e-15

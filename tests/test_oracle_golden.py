@@ -93,3 +93,18 @@ def test_galerkin_oracle_equals_rediscretization_for_uniform_E():
     A1 = hier[1][0]
     K1 = galerkin.fine_matrix(4, 2, 2, np.full(16, 3.0 * 2.0))
     assert abs(A1 - K1).max() < 1e-12 * abs(K1).max()
+
+
+def test_voxelize_oracle_matches_reference():
+    """oracle/voxelize.py against the reference's own parity ray cast
+    (inside_worker._inside_mask_numpy, voxel_centers, node_coords)."""
+    from oracle import voxelize
+    g = golden("inside_cases.npz")
+    dims, origin, vsize = tuple(int(v) for v in g["dims"]), g["origin"], float(g["vsize"])
+    np.testing.assert_array_equal(voxelize.voxel_centers(dims, origin, vsize), g["centers"])
+    np.testing.assert_array_equal(voxelize.node_coords(dims, origin, vsize), g["nodes"])
+    np.testing.assert_array_equal(voxelize.RAY_DIR, g["ray_dir"])
+    for name in ("box", "torus", "tilted"):
+        v, f = g[f"{name}_verts"], g[f"{name}_faces"]
+        for key, pts in (("points", g[f"{name}_points"]), ("centers", g["centers"]), ("nodes", g["nodes"])):
+            np.testing.assert_array_equal(voxelize.inside_mask(v, f, pts), g[f"{name}_in_{key}"], err_msg=f"{name}/{key}")

@@ -50,7 +50,7 @@ EXPORTS = (
     "vf_nn_conv3d_forward", "vf_nn_conv3d_backward_data", "vf_nn_conv3d_backward_weight",
     "vf_nn_wgrad_workspace", "vf_learned_param_count", "vf_learned_configure", "vf_learned_info",
     "vf_learned_input", "vf_learned_apply", "vf_level_mask", "vf_mg_propagate", "vf_solve_block",
-    "vf_solve_batch",
+    "vf_solve_batch", "vf_inside_points", "vf_inside_grid", "vf_element_displacement",
 )
 
 
@@ -152,6 +152,10 @@ def _declare(L):
                                           ctypes.POINTER(VfSolveInfo)]),
         "vf_solve_batch": (ctypes.c_int, [_P, _I32, _P, _P, _P, ctypes.c_double, _I32, ctypes.c_uint32, _P,
                                           ctypes.POINTER(VfSolveInfo)]),
+        "vf_inside_points": (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_int64, _P, ctypes.c_int64, _P, _P]),
+        "vf_element_displacement": (ctypes.c_int, [_I32, _I32, _I32, _P, _P]),
+        "vf_inside_grid": (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_int64, _P, _P, ctypes.c_double, _I32,
+                                          _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

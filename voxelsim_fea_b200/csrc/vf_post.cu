@@ -3,6 +3,7 @@
 //   * element strain energy u_e^T KE u_e  (core/fea.py:595-602)
 // and the pre-step that drops voxel islands not connected to a support
 // (core/fea.py:165-227) as an in-place 6-connected flood fill.
+#include "../../include/voxfea.h"
 #include "vf_common.cuh"
 
 namespace vf {
@@ -166,3 +167,52 @@ int flood_fill_islands(int nx, int ny, int nz, const uint8_t* d_active, const ui
 }
 
 }  // namespace vf
+
+// ---------------------------------------------------------------------------
+// Per-element displacement field of the result views (solve_worker.py:374-388):
+// each voxel gets the mean of its 8 corner nodes' displacement magnitude.
+// Reference node / element orders; host arrays in, FP32 field out.
+// ---------------------------------------------------------------------------
+namespace vf {
+namespace {
+__global__ void k_elem_disp(int nx, int ny, int nz, const double* __restrict__ u, float* __restrict__ out) {
+  const long long ne = (long long)nx * ny * nz;
+  const int nx1 = nx + 1, ny1 = ny + 1;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne; e += (long long)gridDim.x * blockDim.x) {
+    const int iz = (int)(e % nz), iy = (int)((e / nz) % ny), ix = (int)(e / ((long long)nz * ny));
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {   // corner order of build_edof (fea.py:33-36)
+      const int ox = (k == 1 || k == 2 || k == 5 || k == 6), oy = (k == 2 || k == 3 || k == 6 || k == 7), oz = k >= 4;
+      const long long n = (ix + ox) + (long long)nx1 * ((iy + oy) + (long long)ny1 * (iz + oz));
+      const double a = u[3 * n], b = u[3 * n + 1], c = u[3 * n + 2];
+      s += sqrt(a * a + b * b + c * c);
+    }
+    out[e] = (float)(s / 8.0);
+  }
+}
+}  // namespace
+}  // namespace vf
+
+extern "C" int vf_element_displacement(int32_t nx, int32_t ny, int32_t nz, const double* u, float* disp_out) {
+  if (nx < 1 || ny < 1 || nz < 1 || !u || !disp_out) return VF_ERR_ARG;
+  const size_t ndof = 3 * (size_t)(nx + 1) * (ny + 1) * (nz + 1), ne = (size_t)nx * ny * nz;
+  cudaStream_t st = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return VF_ERR_CUDA;
+  double* d_u = nullptr;
+  float* d_o = nullptr;
+  int rc = VF_OK;
+  if (cudaMalloc(&d_u, sizeof(double) * ndof) != cudaSuccess || cudaMalloc(&d_o, sizeof(float) * ne) != cudaSuccess) {
+    rc = VF_ERR_NOMEM;
+  } else {
+    cudaMemcpyAsync(d_u, u, sizeof(double) * ndof, cudaMemcpyHostToDevice, st);
+    const long long b = ((long long)ne + 255) / 256;
+    vf::launch_k(vf::k_elem_disp, (int)(b < 148 * 16 ? b : 148 * 16), 256, 0, st, nx, ny, nz, (const double*)d_u, d_o);
+    cudaMemcpyAsync(disp_out, d_o, sizeof(float) * ne, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = VF_ERR_CUDA;
+  }
+  cudaFree(d_u);
+  cudaFree(d_o);
+  cudaStreamDestroy(st);
+  return rc;
+}
