@@ -509,7 +509,7 @@ def main():
     ap.add_argument("--kernel-precision", choices=("fp32", "fp64"), default="fp32")
     ap.add_argument("--modal-zchunk", type=int, default=0, help="z-planes per CTA of the modal kernel (0 = auto)")
     ap.add_argument("--kernel-iters", type=int, default=3, help="launches timed by --kernel-profile")
-    ap.add_argument("--mixed-mode", choices=("reliable", "restart"), default="reliable")
+    ap.add_argument("--mixed-mode", choices=("reliable", "restart", "outer64"), default="reliable")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed: residual reduction between FP64 corrections (solver default if unset)")
     args = ap.parse_args()

@@ -104,7 +104,10 @@ typedef struct vf_options {
                               residual is replaced by the FP64 true residual (and the FP32
                               increment folded into the FP64 solution) each time it has
                               dropped by inner_tol; VF_MIXED_RESTART: iterative refinement,
-                              a fresh FP32 PCG per outer step */
+                              a fresh FP32 PCG per outer step; VF_MIXED_OUTER64: FP64 PCG
+                              (x, r, p, A p, dots and the fine operator of A p in FP64)
+                              preconditioned by the FP32 V-cycle -- the FP64 Krylov space,
+                              so the iteration count of the FP64 solve on hard problems */
   int32_t flexible;        /* 1: flexible CG (Notay's FCG(1): beta = -z.Ap / p.Ap), which
                               stays correct for a preconditioner that varies between
                               iterations; always on while a learned stage is enabled */
@@ -119,7 +122,7 @@ enum { VF_FINE_MODAL = 0,     /* modal z-marching kernel, TMA-staged (vf_modal_t
        VF_FINE_GATHER = 1,    /* node-centric 27-neighbour gather (vf_matvec.cu) */
        VF_FINE_MODAL_CPASYNC = 2 };  /* modal z-marching kernel, cp.async-staged (vf_modal.cu) */
 enum { VF_STENCIL_SYM_HALF = 0, VF_STENCIL_SYM = 1, VF_STENCIL_FULL = 2 };
-enum { VF_MIXED_RELIABLE = 0, VF_MIXED_RESTART = 1 };
+enum { VF_MIXED_RELIABLE = 0, VF_MIXED_RESTART = 1, VF_MIXED_OUTER64 = 2 };
 
 typedef struct vf_solve_info {
   int32_t iters;           /* PCG iterations (all inner iterations for MIXED);

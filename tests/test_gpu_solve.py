@@ -52,12 +52,13 @@ def test_cantilever_default_levels(gpu):
     assert abs(u[2::3].min() / float(g6["u_tip"]) - 1) < 1e-9
 
 
-@pytest.mark.parametrize("preset", ["robust", "fast", "fp32"])
+@pytest.mark.parametrize("preset", ["robust", "fast", "outer64", "fp32"])
 def test_cantilever_b200_solvers(gpu, preset):
     from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
     g = golden("cantilever_64x16x16_L3.npz")
     p = _cantilever()
     opts = {"robust": SolverOptions.robust(), "fast": SolverOptions.fast(),
+            "outer64": SolverOptions.fast(mixed_mode="outer64"),
             "fp32": SolverOptions(precision="fp32", coarse="galerkin", coarsest="cholesky")}[preset]
     tol = 1e-5 if preset == "fp32" else 1e-10
     m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"], options=opts)
@@ -144,7 +145,7 @@ def test_set_fixed_required(gpu):
         v.solve(np.ones(64), np.zeros(375))
 
 
-@pytest.mark.parametrize("preset", ["robust", "fast"])
+@pytest.mark.parametrize("preset", ["robust", "fast", "outer64"])
 def test_noise_bracket_converges(gpu, preset):
     """The reference's rediscretized MG does not converge on noise geometry;
     the Galerkin hierarchy with per-level damping must reach 1e-8 quickly, with
@@ -155,7 +156,8 @@ def test_noise_bracket_converges(gpu, preset):
     p = generators.bracket(shape=(64, 32, 32), seed=0, sigma=4.0, load_n=5000.0, patch=16)
     nx, ny, nz = p["dims"]
     E_mg = np.where(p["active"], p["E_stiff"], p["E_stiff"] * 1e-9)
-    opts = SolverOptions.robust() if preset == "robust" else SolverOptions.fast()
+    opts = {"robust": SolverOptions.robust(), "fast": SolverOptions.fast(),
+            "outer64": SolverOptions.fast(mixed_mode="outer64")}[preset]
     m = MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=4, options=opts)
     u = m.solve(E_mg, p["f"], tol=1e-8)
     assert m.last_converged
@@ -165,3 +167,27 @@ def test_noise_bracket_converges(gpu, preset):
         assert 2.0 < lam < 8.0 and abs(w * lam - 1.6) < 1e-12
     r = true_residual(nx, ny, nz, E_mg, p["fixed_dofs"], p["f"], u, nu=p["nu"])
     assert r < 1e-8, r
+
+
+@pytest.mark.parametrize("flexible", [False, True])
+def test_outer64_tracks_fp64_iterations(gpu, flexible):
+    """FP64 PCG preconditioned by the FP32 V-cycle keeps the FP64 Krylov
+    space: on a two-material part (1000:1 moduli, per-voxel Poisson ratio)
+    that needs a few hundred FP64 iterations it converges in about the same
+    count, with the true FP64 residual below tol and the FP64 solution."""
+    from voxelsim_fea_b200.learned.train import make_part
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    part = make_part(9_015_838, shape=(48, 48, 48))
+    nx, ny, nz = part["dims"]
+    res = {}
+    for name, opts in (("fp64", SolverOptions.robust(flexible=flexible)),
+                       ("outer64", SolverOptions.fast(mixed_mode="outer64", flexible=flexible))):
+        m = MGSolver(nx, ny, nz, part["fixed"], nu=0.3, options=opts)
+        u = m.solve(part["E"], part["f"], tol=1e-8, nu_elem=part["nu"], max_cg=3000)
+        res[name] = (u, m.last_iters, m.last_converged, m.last_info.true_resid)
+        m.close()
+    (u64, it64, c64, _), (u32, it32, c32, r32) = res["fp64"], res["outer64"]
+    assert c64 and c32
+    assert r32 < 1e-8
+    assert it32 <= int(1.1 * it64) + 5, (it32, it64)
+    assert np.abs(u32 - u64).max() <= 1e-5 * np.abs(u64).max()

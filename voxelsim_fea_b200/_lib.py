@@ -32,7 +32,7 @@ VF_SOLVE_DEVICE_PTRS = 1
 VF_OMEGA_FIXED, VF_OMEGA_AUTO = 0, 1
 VF_FINE_MODAL, VF_FINE_GATHER, VF_FINE_MODAL_CPASYNC = 0, 1, 2
 STENCIL_STORAGE = {"sym_half": 0, "sym": 1, "full": 2}
-MIXED_MODES = {"reliable": 0, "restart": 1}
+MIXED_MODES = {"reliable": 0, "restart": 1, "outer64": 2}
 
 PRECISIONS = {"fp64": VF_PREC_FP64, "mixed": VF_PREC_MIXED, "fp32": VF_PREC_FP32}
 COARSE_OPS = {"rediscretize": VF_COARSE_REDISCRETIZE, "galerkin": VF_COARSE_GALERKIN}

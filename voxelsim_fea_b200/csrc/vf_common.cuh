@@ -201,6 +201,12 @@ void launch_norm2_f64(const Grid& g, const double* v, double* partials, KrylovSt
 void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState* ks, cudaStream_t st);
 void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const KrylovState* ks, cudaStream_t st);
 void launch_ir_replace(const Grid& g, const double* r64, float* r32, const KrylovState* ks, cudaStream_t st);
+void launch_cg_update_split(const Grid& g, double* x, const double* p, double* r, const double* Ap, float* r32,
+                            double* partials, KrylovState* ks, double* hist, cudaStream_t st);
+void launch_p_update_split(const Grid& g, double* p, const float* z, KrylovState* ks, cudaStream_t st);
+void launch_dot_fcg_split(const Grid& g, const float* r, const float* z, const double* Ap, double* partials,
+                          KrylovState* ks, cudaStream_t st);
+void launch_scale64(const Grid& g, const double* x, double* y, double sc, cudaStream_t st);
 void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st);
 template <typename T> void launch_sub_inplace(const Grid& g, T* y, const T* x, cudaStream_t st);
 template <typename T> void launch_axpy_gamma(const Grid& g, T* z, const T* c, const KrylovState* ks, const int* skip,

@@ -149,8 +149,9 @@ struct vf_solver {
   double* d_ref_c = nullptr;
   uint8_t* d_ref_u8 = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
-  cudaGraphExec_t chunk[3] = {nullptr, nullptr, nullptr};   // FP64 MG / FP32 MG / Jacobi
-  unsigned long long chunk_kernels[3] = {0, 0, 0};
+  // FP64 MG / FP32 MG / Jacobi / FP64 PCG with the FP32 V-cycle
+  cudaGraphExec_t chunk[4] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned long long chunk_kernels[4] = {0, 0, 0, 0};
   std::vector<void*> allocs;
   double last_setup_ms = 0.0;
   double last_best = 0.0;       // stall guard: best ratio of the last solve
@@ -414,18 +415,33 @@ void pcg_iteration(vf_solver* s) {
   update_direction<T>(s, r, z, p, Ap);
 }
 
-int graph_slot(const vf_solver* s, bool fp32) { return use_mg(s) ? (fp32 ? 1 : 0) : 2; }
+// One iteration of the FP64 PCG preconditioned by the FP32 V-cycle
+// (VF_MIXED_OUTER64): the iteration of pcg_iteration<double>, with the
+// residual handed to the V-cycle as an FP32 copy and z widened in p = z + beta p.
+void pcg_iteration_outer64(vf_solver* s) {
+  double *x = s->k64[0], *r = s->k64[1], *p = s->k64[3], *Ap = s->k64[4];
+  float *r32 = s->k32[1], *z32 = s->k32[2];
+  const Grid& g = s->L[0].g;
+  level_op<double>(s, 0, EPI_APPLY, p, Ap, nullptr, s->ks, s->d_partials, SLOT_PAP);
+  launch_cg_update_split(g, x, p, r, Ap, r32, s->d_partials, s->ks, s->d_hist, s->st);
+  precondition<float>(s, r32, z32, s->ks, fused_rz(s) ? SLOT_RZ : -1);
+  if (flexible(s)) launch_dot_fcg_split(g, r32, z32, Ap, s->d_partials, s->ks, s->st);
+  else if (!fused_rz(s)) launch_dot<float>(g, r32, z32, s->d_partials, s->ks, SLOT_RZ, s->st);
+  launch_p_update_split(g, p, z32, s->ks, s->st);
+}
 
-// Run PCG chunks until the device says done.  Host callbacks see each new
-// history entry.
-template <typename T>
-int run_chunks(vf_solver* s, void (*progress)(int, double, double, void*), void* user, double tol) {
+int graph_slot(const vf_solver* s, bool fp32) { return use_mg(s) ? (fp32 ? 1 : 0) : 2; }
+constexpr int kSlotOuter64 = 3;
+
+// Run PCG chunks of `iteration` until the device says done.  Host callbacks
+// see each new history entry.
+int run_chunks(vf_solver* s, void (*iteration)(vf_solver*), int gslot,
+               void (*progress)(int, double, double, void*), void* user, double tol) {
   const int K = std::max(1, s->o.check_every);
-  const int gslot = graph_slot(s, sizeof(T) == 4);
   if (s->o.use_graphs && !s->chunk[gslot]) {
     cudaGraph_t graph = nullptr;
     VF_TRY(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < K; ++k) pcg_iteration<T>(s);
+    for (int k = 0; k < K; ++k) iteration(s);
     cudaError_t e = cudaStreamEndCapture(s->st, &graph);
     if (e != cudaSuccess) { s->err = std::string("graph capture: ") + cudaGetErrorString(e); return VF_ERR_CUDA; }
     e = cudaGraphInstantiate(&s->chunk[gslot], graph, 0);
@@ -447,7 +463,7 @@ int run_chunks(vf_solver* s, void (*progress)(int, double, double, void*), void*
       VF_TRY(cudaGraphLaunch(s->chunk[gslot], s->st));
       g_launches += s->chunk_kernels[gslot];
     } else {
-      for (int k = 0; k < K; ++k) pcg_iteration<T>(s);
+      for (int k = 0; k < K; ++k) iteration(s);
       VF_CHECK_LAUNCH();
     }
     VF_TRY(cudaMemcpyAsync(s->h_ks, s->ks, sizeof(KrylovState), cudaMemcpyDeviceToHost, s->st));
@@ -508,7 +524,7 @@ int pcg_solve(vf_solver* s, double tol, int max_it, int stall_guard, int it_base
   launch_copy_vec<T>(g, v[2], v[3], nullptr, s->st);
   VF_CHECK_LAUNCH();
   if (max_it <= 0) return VF_OK;
-  return run_chunks<T>(s, progress, user, tol_report);
+  return run_chunks(s, pcg_iteration<T>, graph_slot(s, sizeof(T) == 4), progress, user, tol_report);
 }
 
 int map_status(int ks) {
@@ -661,12 +677,18 @@ int autotune_levels(vf_solver* s) {
                                     : (long long)((l.g.lx + 31) / 31) * ((l.g.ly + 7) / 7);
     auto ctas = [&](int c) { return tiles * ((planes + c - 1) / c); };
     const long long floor_ctas = std::min<long long>(148, ctas(modal ? 2 : 1));
+    // every distinct z-chunk ceil(planes / n) for n = 1..64 z-ranges: the
+    // last wave of CTAs can be anywhere from nearly empty to full, and which
+    // split fills it best depends on the tile count and the residency
     std::vector<int> cand;
     const int base = stencil ? sym_zchunk(l.g) : auto_zchunk(l.g, 0);
-    for (int c : {base, 1, 2, 3, 4, 6, 8, 12, 16, 22, 33, 48, 65})
-      if (c >= 1 && c <= planes && (modal ? c >= 2 : true) && ctas(c) >= floor_ctas &&
+    cand.push_back(base);
+    for (int n = 1; n <= 64; ++n) {
+      const int c = (planes + n - 1) / n;
+      if (c >= 1 && (modal ? c >= 2 : true) && ctas(c) >= floor_ctas &&
           std::find(cand.begin(), cand.end(), c) == cand.end())
         cand.push_back(c);
+    }
     // two passes, minimum per candidate: the first pass also brings the
     // clocks up after the set-up, which would otherwise favour late candidates
     std::vector<float> tmin(cand.size(), 1e30f);
@@ -947,7 +969,7 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
       o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0 ||
       o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0 ||
       o.fine_kernel < 0 || o.fine_kernel > 2 || o.modal_zchunk < 0 || o.coarse_storage < 0 ||
-      o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 1) {
+      o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 2) {
     g_last_error = "invalid vf_options field";
     return VF_ERR_ARG;
   }
@@ -1220,7 +1242,7 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
   const int max_updates = std::max(1, s->o.max_outer) * 8;
   int cycle_start = 0, longest = 0;
   for (;;) {
-    int rc = run_chunks<float>(s, progress, user, tol);
+    int rc = run_chunks(s, pcg_iteration<float>, graph_slot(s, true), progress, user, tol);
     if (rc) return rc;
     const int kst = s->h_ks->status;
     const int it = s->h_ks->it;
@@ -1267,6 +1289,50 @@ int mixed_reliable(vf_solver* s, bool have_x0, double tol, int max_it, double fn
     VF_CHECK_LAUNCH();
   }
   s->history.resize(inf.iters);
+  return VF_OK;
+}
+
+// FP64 PCG preconditioned by the FP32 V-cycle (VF_MIXED_OUTER64).  The
+// system is solved scaled by 1 / ||f|| (A x~ = f / ||f||, x = ||f|| x~), so
+// the FP32 residual copies and corrections stay O(1) -> far from FP32's range
+// limits whatever the units of E and f; the relative residual, the stall
+// guard and the history are those of the FP64 solve.
+int mixed_outer64(vf_solver* s, bool have_x0, double tol, int max_it, double fnorm,
+                  void (*progress)(int, double, double, void*), void* user, vf_solve_info& inf, int& status) {
+  Level& l0 = s->L[0];
+  const Grid& g = l0.g;
+  double** v = s->k64;
+  float** w = s->k32;
+  const double inv = 1.0 / fnorm;
+  launch_scale64(g, s->f64, v[1], inv, s->st);                       // r~ = f~
+  if (have_x0) {
+    launch_pack_vec<double>(g, s->d_ref_b, v[0], l0.mask, s->st);
+    launch_scale64(g, v[0], v[0], inv, s->st);                       // x~0 = x0 / ||f||
+    level_op<double>(s, 0, EPI_APPLY, v[0], s->r64, nullptr, nullptr, nullptr, 0);
+    launch_sub_inplace<double>(g, v[1], s->r64, s->st);              // r~ = f~ - A x~0
+  } else {
+    cudaMemsetAsync(v[0], 0, sizeof(double) * 3 * (size_t)g.n, s->st);
+  }
+  init_ks(*s->h_ks, tol, max_it, use_mg(s) ? s->o.stall_guard : 0, 0, 1.0);
+  s->h_ks->fnorm = 1.0;
+  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  launch_convert<double, float>(v[1], w[1], 3LL * g.n, s->st);
+  precondition<float>(s, w[1], w[2], nullptr);
+  launch_dot<float>(g, w[1], w[2], s->d_partials, s->ks, SLOT_RZ_INIT, s->st);
+  launch_convert<float, double>(w[2], v[3], 3LL * g.n, s->st);      // p = z
+  VF_CHECK_LAUNCH();
+  if (max_it > 0) {
+    int rc = run_chunks(s, pcg_iteration_outer64, kSlotOuter64, progress, user, tol);
+    if (rc) return rc;
+  }
+  launch_scale64(g, v[0], v[0], fnorm, s->st);                       // x = ||f|| x~
+  VF_CHECK_LAUNCH();
+  inf.iters = s->h_ks->it;
+  inf.outer_iters = 0;
+  inf.converged = s->h_ks->status == KS_CONVERGED;
+  inf.resid_ratio = s->h_ks->it > 0 ? s->h_ks->resid : std::numeric_limits<double>::quiet_NaN();
+  status = map_status(s->h_ks->status);
+  s->last_best = s->h_ks->best;
   return VF_OK;
 }
 
@@ -1373,6 +1439,9 @@ extern "C" int vf_solve_cb(vf_solver* s, const double* f, const double* x0, doub
     status = map_status(s->h_ks->status);
   } else if (s->o.mixed_mode == VF_MIXED_RELIABLE) {
     int rc = mixed_reliable(s, x0 != nullptr, tol, max_it, fnorm, progress, user, inf, status);
+    if (rc) return rc;
+  } else if (s->o.mixed_mode == VF_MIXED_OUTER64) {
+    int rc = mixed_outer64(s, x0 != nullptr, tol, max_it, fnorm, progress, user, inf, status);
     if (rc) return rc;
   } else {
     // ---- mixed precision iterative refinement ----
@@ -1913,7 +1982,7 @@ int vf_solve_block(vf_solver* s, const double* F, int32_t k, double tol, int32_t
   std::vector<vf_solver*> solvers{s};
   for (int j = 0; j + 1 < k; ++j) {
     vf_solver* c = s->children[j];
-    const bool had_graphs = c->chunk[0] || c->chunk[1] || c->chunk[2];
+    const bool had_graphs = c->chunk[0] || c->chunk[1] || c->chunk[2] || c->chunk[3];
     const double* oldA = c->d_Ainv;
     share_operator(c, s);
     // graphs hold operator pointers and option-dependent launch sequences: re-capture on change

@@ -195,6 +195,17 @@ def headline_configs():
             ("learned_mixed", SolverOptions.fast(), True))
 
 
+def modes_configs():
+    """Plain FP64 against the mixed-precision forms: FP32 CG with residual
+    replacement, FP64 PCG around the FP32 V-cycle, and the latter with the
+    learned stage."""
+    from ..multigrid import SolverOptions
+    return (("plain_fp64", SolverOptions.robust(), False),
+            ("mixed", SolverOptions.fast(), False),
+            ("outer64", SolverOptions.fast(mixed_mode="outer64"), False),
+            ("learned_outer64", SolverOptions.fast(mixed_mode="outer64"), True))
+
+
 def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None, max_cg=None):
     """Solve held-out parts without and with the learned stage (FP64 and
     mixed precision); per-part iterations and device times."""
@@ -240,17 +251,19 @@ def main():
     ap.add_argument("--eval-json", type=str, default=None)
     ap.add_argument("--eval-only", action="store_true", help="evaluate the packaged weights, no training")
     ap.add_argument("--max-cg", type=int, default=3000)
+    ap.add_argument("--configs", choices=("headline", "modes"), default="headline")
     args = ap.parse_args()
     from . import stage
     if args.eval_only:
         params, level = stage.load_weights()
         seeds = [9_000_000 + 7919 * i for i in range(args.eval)]
         e = args.eval_size
-        rows = evaluate(params, level, seeds, (e, e, e), configs=headline_configs(), max_cg=args.max_cg)
+        cfgs = headline_configs() if args.configs == "headline" else modes_configs()
+        rows = evaluate(params, level, seeds, (e, e, e), configs=cfgs, max_cg=args.max_cg)
         summary = {k: {"iters_mean": float(np.mean([r[k]["iters"] for r in rows])),
                        "solve_ms_mean": float(np.mean([r[k]["solve_ms"] for r in rows])),
                        "converged": int(sum(r[k]["converged"] for r in rows))}
-                   for k, _, _ in headline_configs()}
+                   for k, _, _ in cfgs}
         print(json.dumps(summary), flush=True)
         if args.eval_json:
             with open(args.eval_json, "w") as fh:

@@ -41,7 +41,9 @@ class SolverOptions:
     device: int = 0
     inner_tol: float = 1e-2          # mixed: residual reduction between FP64 corrections
     max_outer: int = 20              # mixed: cap on FP64 corrections
-    mixed_mode: str = "reliable"     # mixed: "reliable" (residual replacement) | "restart" (refinement)
+    # mixed: "reliable" (FP32 CG, residual replacement) | "restart" (refinement) |
+    # "outer64" (FP64 PCG, FP32 V-cycle)
+    mixed_mode: str = "reliable"
     flexible: bool = False           # flexible CG (automatic with a learned stage)
     autotune: bool = True            # time z-chunk candidates of the marching kernels at set-up
     omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
