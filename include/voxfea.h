@@ -94,7 +94,9 @@ typedef struct vf_options {
   double  omega_rel;       /* VF_OMEGA_AUTO: fraction of the stability limit (0.8) */
   int32_t fine_kernel;     /* VF_FINE_MODAL (default) | VF_FINE_GATHER: kernel of the
                               element-operator levels (same operator, different form) */
-  int32_t modal_zchunk;    /* z-planes per CTA of the modal kernel; 0 = automatic */
+  int32_t modal_zchunk;    /* z-planes per CTA of the modal kernel; 0 = automatic;
+                              -1 = one resident wave of CTAs sharing the (tile, plane)
+                              units evenly (TMA form) */
   int32_t coarse_storage;  /* Galerkin stencils as applied in the V-cycle:
                               VF_STENCIL_SYM_HALF (default): symmetric, diagonally
                               scaled, FP16 values for the FP32 V-cycle and FP64 for FP64;

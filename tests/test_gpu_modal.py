@@ -32,7 +32,7 @@ def _problem(nx, ny, nz, seed, lame=False):
     return rng, E, fixed, nu, ndof
 
 
-@pytest.mark.parametrize("zchunk", [0, 1, 2, 5, 64])
+@pytest.mark.parametrize("zchunk", [-1, 0, 1, 2, 5, 64])
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_modal_apply_matches_oracle(gpu, zchunk, prec):
     from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
@@ -86,3 +86,31 @@ def test_modal_solve_matches_gather_solve(gpu):
     ub, ib = out["gather"]
     assert abs(ia - ib) <= 2
     assert np.abs(ua - ub).max() < 1e-7 * np.abs(ub).max()
+
+
+@pytest.mark.parametrize("dims", [(64, 48, 40), (120, 60, 50), (200, 13, 3)])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_modal_even_wave_is_bitwise_chunked(gpu, dims, prec):
+    """The one-wave split (z-chunk -1: CTAs share the (tile, plane) units
+    evenly, a range crossing a tile boundary marched as a second segment, the
+    staging ring carried across segments) does each node's arithmetic exactly
+    as the per-chunk grid does: bitwise equal apply and Jacobi sweeps, with a
+    per-voxel Poisson ratio, on grids with several units per CTA."""
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    nx, ny, nz = dims
+    rng, E, fixed, nu, ndof = _problem(nx, ny, nz, 5, lame=True)
+    ms = {}
+    for zc in (-1, 3):
+        ms[zc] = MGSolver(nx, ny, nz, fixed, nu=0.3, max_levels=1,
+                          options=SolverOptions(fine_kernel="modal", modal_zchunk=zc, autotune=False))
+        ms[zc].set_density(E, nu_elem=nu)
+    free = ms[3].levels[0]["free"]
+    u = rng.standard_normal(ndof) * free
+    rhs = rng.standard_normal(ndof) * free
+    a, b = ms[-1], ms[3]
+    np.testing.assert_array_equal(a._apply(0, u, precision=prec), b._apply(0, u, precision=prec))
+    np.testing.assert_array_equal(a._smooth(0, u, rhs, 2, precision=prec), b._smooth(0, u, rhs, 2, precision=prec))
+    if prec == "fp64":
+        lam, mu = hex8.lame(E, nu)
+        ref = hex8.element_apply_lame(u, lam, mu, hex8.build_edof(nx, ny, nz), ndof) * free
+        _close(a._apply(0, u, precision=prec), ref, RTOL[prec])

@@ -19,6 +19,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -123,26 +124,29 @@ __global__ void __launch_bounds__(TX * TY, 2)
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const bool leader = (tx == 0 && ty == 0);
-  const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TY - 1);
-  const int Xc = X0 - 1 + tx, Yc = Y0 - 1 + ty;
-  const int zb = blockIdx.z * zchunk;
-  const int ze = min(zb + zchunk, g.lz + 1);
-  const int H = (ze - zb + L - 1) / L;
-  const int sz = g.px * g.py;
-  const bool col_in = (Xc + 1 < g.px) && (Yc + 1 < g.py);
-  const int colbase = col_in ? (Yc + 1) * g.px + (Xc + 1) : 0;
-  const bool out_col = tx >= 1 && ty >= 1 && Xc <= g.lx && Yc <= g.ly;
-  // box origins (storage coordinates; x rounded down to 16 bytes) and remainders
-  const int xu = (3 * X0) & ~(AL - 1), ou = 3 * X0 - xu;
-  const int xe = X0 & ~(AL - 1), oe = X0 - xe;
-
-  int z0[L], oend[L];
-#pragma unroll
-  for (int l = 0; l < L; ++l) {
-    z0[l] = zb + l * H - 1;
-    oend[l] = min(min(zb + l * H + H, ze), g.lz + 1);
+  // Work of this CTA: a range [ub, ue) of (tile, output plane) units, tile-
+  // major, NP planes per tile.  zchunk > 0: one tile and z-chunk per CTA
+  // (x tiles fastest, then y tiles, then chunks); zchunk <= 0: the units split
+  // evenly over the grid (one resident wave), a range crossing into the next
+  // tile marched as a second segment.
+  const int ntx = (g.lx + TX - 1) / (TX - 1), nty = (g.ly + TY - 1) / (TY - 1);
+  const int NP = g.lz + 1;
+  long long ub, ue;
+  if (zchunk > 0) {
+    const int ntile = ntx * nty;
+    const int tile = (int)(blockIdx.x % ntile), ch = (int)(blockIdx.x / ntile);
+    ub = (long long)tile * NP + (long long)ch * zchunk;
+    ue = (long long)tile * NP + min((long long)(ch + 1) * zchunk, (long long)NP);
+  } else {
+    const long long U = (long long)ntx * nty * NP;
+    ub = U * blockIdx.x / gridDim.x;
+    ue = U * (blockIdx.x + 1) / gridDim.x;
   }
-  const int nsteps = H + 2;
+  const int sz = g.px * g.py;
+  // per-segment geometry (set at the top of each segment)
+  int X0 = 0, Y0 = 0, Xc = 0, Yc = 0, colbase = 0, xu = 0, ou = 0, xe = 0, oe = 0, nsteps = 0, gbase = 0;
+  bool out_col = false;
+  int z0[L], oend[L];
 
   if (leader) {
 #pragma unroll
@@ -151,8 +155,9 @@ __global__ void __launch_bounds__(TX * TY, 2)
   }
   __syncthreads();
 
+  // stages and mbarrier phases follow the CTA's running step count gbase + s
   auto issue = [&](int s) {   // leader only
-    const int st = s % NSTAGE;
+    const int st = (gbase + s) % NSTAGE;
     unsigned char* base = smem + st * Lay::STAGE;
     mbar_expect_tx(&bar[st], Lay::TXB);
 #pragma unroll
@@ -185,15 +190,12 @@ __global__ void __launch_bounds__(TX * TY, 2)
   };
 
   P hiPrev[3][4];
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int m = 0; m < 4; ++m) hiPrev[c][m] = O::zero();
   double dot = 0.0;
 
   auto step = [&](const int s, P (&Fc)[3][4], const P (&Fp)[3][4]) {
-    const int st = s % NSTAGE, sp = (s + NSTAGE - 1) % NSTAGE;
-    wait_stage(&bar[st], (unsigned)((s / NSTAGE) & 1), a.err);
+    const int gs = gbase + s;
+    const int st = gs % NSTAGE, sp = (gs + NSTAGE - 1) % NSTAGE;
+    wait_stage(&bar[st], (unsigned)((gs / NSTAGE) & 1), a.err);
     __syncthreads();                         // step s-1 done everywhere: stage (s+2) is free
     if (leader && s + 2 < nsteps) issue(s + 2);
     uint8_t mk[L];
@@ -294,22 +296,52 @@ __global__ void __launch_bounds__(TX * TY, 2)
     }
   };
 
-  if (leader) {
-    issue(0);
-    if (1 < nsteps) issue(1);
-  }
   P Fa[3][4], Fb[3][4];
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int m = 0; m < 4; ++m) { Fa[c][m] = O::zero(); Fb[c][m] = O::zero(); }
+  // Segments: a new segment's first two loads go to the stages of steps
+  // gbase-4 and gbase-3, whose last readers (steps gbase-3 and gbase-2) every
+  // thread has left once the leader is past step gbase-1's first barrier.
 #pragma unroll 1
-  for (int s = 0; s < nsteps; ++s) {
-    step(s, Fa, Fb);
+  for (long long u0 = ub; u0 < ue;) {
+    const int tile = (int)(u0 / NP);
+    const int zb = (int)(u0 - (long long)tile * NP);
+    const int ze = (int)min((long long)NP, (long long)zb + (ue - u0));
+    u0 = (long long)tile * NP + ze;
+    X0 = (tile % ntx) * (TX - 1);
+    Y0 = (tile / ntx) * (TY - 1);
+    Xc = X0 - 1 + tx;
+    Yc = Y0 - 1 + ty;
+    const bool col_in = (Xc + 1 < g.px) && (Yc + 1 < g.py);
+    colbase = col_in ? (Yc + 1) * g.px + (Xc + 1) : 0;
+    out_col = tx >= 1 && ty >= 1 && Xc <= g.lx && Yc <= g.ly;
+    // box origins (storage coordinates; x rounded down to 16 bytes) and remainders
+    xu = (3 * X0) & ~(AL - 1);
+    ou = 3 * X0 - xu;
+    xe = X0 & ~(AL - 1);
+    oe = X0 - xe;
+    const int H = (ze - zb + L - 1) / L;
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      z0[l] = zb + l * H - 1;
+      oend[l] = min(min(zb + l * H + H, ze), g.lz + 1);
+    }
+    nsteps = H + 2;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int m = 0; m < 4; ++m) Fb[c][m] = Fa[c][m];
+      for (int m = 0; m < 4; ++m) { hiPrev[c][m] = O::zero(); Fa[c][m] = O::zero(); Fb[c][m] = O::zero(); }
+    if (leader) {
+      issue(0);
+      issue(1);
+    }
+#pragma unroll 1
+    for (int s = 0; s < nsteps; ++s) {
+      step(s, Fa, Fb);
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) Fb[c][m] = Fa[c][m];
+    }
+    gbase += nsteps;
   }
   // APPLY: u.y (p.Ap); SMOOTH: b.u' (the V-cycle's last sweep: r.z)
   if ((EPI == EPI_APPLY || EPI == EPI_SMOOTH) && a.dot_partials && ks)
@@ -363,12 +395,15 @@ bool tensor_map(const void* ptr, const Grid& g, int kind, CUtensorMap* out) {
 
 bool modal_tma_supported() { return encode_fn(); }
 
-// Launch geometry as launch_modal_op: (ceil((lx+1)/31), ceil((ly+1)/7), ceil((lz+1)/zchunk)).
+// Launch geometry: zchunk > 0 (0: the whole column): one CTA per 31 x 7 tile
+// and z-chunk, ceil((lx+1)/31) * ceil((ly+1)/7) * ceil((lz+1)/zchunk) CTAs;
+// zchunk < 0: one resident wave (SMs x CTAs per SM, at most one per unit)
+// sharing the (tile, plane) units evenly.
 // Returns false (nothing launched) when a tensor map cannot be built.
 template <typename T>
 bool launch_modal_tma(const Grid& g, int epi, const OpArgs& a, const ModalConst& mc, int zchunk, cudaStream_t st) {
   const bool lame = a.mu != nullptr;
-  if (zchunk < 1) zchunk = g.lz + 1;
+  if (zchunk == 0) zchunk = g.lz + 1;
   CUtensorMap mu, me, mm, mb, md;
   if (!tensor_map<T>(a.u, g, 0, &mu) || !tensor_map<T>(a.E, g, 2, &me)) return false;
   mm = me;
@@ -377,19 +412,30 @@ bool launch_modal_tma(const Grid& g, int epi, const OpArgs& a, const ModalConst&
   if (lame && !tensor_map<T>(a.mu, g, 2, &mm)) return false;
   if (epi != EPI_APPLY && !tensor_map<T>(a.b, g, 1, &mb)) return false;
   if (epi == EPI_SMOOTH && !tensor_map<T>(a.minv, g, 1, &md)) return false;
-  const int gz = (g.lz + 1 + zchunk - 1) / zchunk;
-  const dim3 grid((g.lx + 1 + TX - 2) / (TX - 1), (g.ly + 1 + TY - 2) / (TY - 1), gz);
+  const long long tiles = (long long)((g.lx + TX - 1) / (TX - 1)) * ((g.ly + TY - 1) / (TY - 1));
+  const long long units = tiles * (g.lz + 1);
   const dim3 block(TX, TY);
 #define VF_TMA_ONE(LM, EP)                                                                    \
   do {                                                                                        \
     auto kern = k_modal_tma<T, LM, EP>;                                                       \
     constexpr size_t smem = Layout<T, LM, EP>::total();                                       \
-    static std::atomic<bool> attr{false};                                                     \
-    if (!attr.load()) {                                                                       \
+    static std::atomic<int> per_sm{0};                                                        \
+    if (per_sm.load() == 0) {                                                                 \
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
-      attr.store(true);                                                                       \
+      int o = 0;                                                                              \
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, TX * TY, smem) != cudaSuccess || o < 1) o = 1; \
+      per_sm.store(o);                                                                        \
     }                                                                                         \
-    launch_k(kern, grid, block, smem, st, g, a, mc, zchunk, mu, me, mm, mb, md);              \
+    long long nb;                                                                             \
+    if (zchunk > 0) {                                                                         \
+      nb = tiles * ((g.lz + 1 + zchunk - 1) / zchunk);                                        \
+    } else {                                                                                  \
+      int dev = 0, sms = 148;                                                                 \
+      cudaGetDevice(&dev);                                                                    \
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);                      \
+      nb = std::min<long long>((long long)sms * per_sm.load(), units);                        \
+    }                                                                                         \
+    launch_k(kern, dim3((unsigned)nb), block, smem, st, g, a, mc, zchunk, mu, me, mm, mb, md); \
   } while (0)
   if (lame) {
     if (epi == EPI_APPLY) VF_TMA_ONE(true, EPI_APPLY);

@@ -73,7 +73,7 @@ unsigned long long graph_kernel_nodes(cudaGraph_t g) {
 
 struct Level {
   Grid g{};
-  int zchunk = 0;          // modal kernel: z-planes per CTA
+  int zchunk = 0;          // modal kernel: z-planes per CTA (< 0: one even wave)
   int szchunk = 0;         // marching stencil kernel: z-planes per CTA
   uint8_t* mask = nullptr;
   bool galerkin = false;   // operator is the assembled stencil
@@ -241,6 +241,8 @@ template <> void level_sym_op<float>(vf_solver* s, Level& l, int epi, const OpAr
   else launch_stencil_sym_op<float, float>(l.g, epi, a, l.sym32, l.sq32, l.szchunk, s->st);
 }
 
+int auto_zchunk(const Grid& g, int requested);
+
 template <typename T>
 void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, KrylovState* ks, double* partials,
               int slot) {
@@ -266,7 +268,7 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
   } else {
     const ModalConst& mc = s->lame ? s->mc_lame : s->mc;
     if (s->o.fine_kernel == VF_FINE_MODAL_CPASYNC || !launch_modal_tma<T>(l.g, epi, a, mc, l.zchunk, s->st))
-      launch_modal_op<T>(l.g, epi, a, mc, 8, l.zchunk, s->st);
+      launch_modal_op<T>(l.g, epi, a, mc, 8, l.zchunk > 0 ? l.zchunk : auto_zchunk(l.g, 0), s->st);
   }
 }
 
@@ -660,7 +662,7 @@ int autotune_levels(vf_solver* s) {
     const bool stencil = l.galerkin && s->o.coarse_storage != VF_STENCIL_FULL;
     const bool modal = !l.galerkin && s->o.fine_kernel == VF_FINE_MODAL;
     if (!stencil && !modal) continue;
-    if (modal && s->o.modal_zchunk > 0) continue;   // fixed by the caller
+    if (modal && s->o.modal_zchunk != 0) continue;   // fixed by the caller
     const auto key = std::make_tuple(l.g.lx, l.g.ly, l.g.lz, stencil ? 1 + s->o.coarse_storage : 0);
     {
       std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -683,6 +685,8 @@ int autotune_levels(vf_solver* s) {
     std::vector<int> cand;
     const int base = stencil ? sym_zchunk(l.g) : auto_zchunk(l.g, 0);
     cand.push_back(base);
+    // the TMA modal kernel's even one-wave split (z-chunk -1)
+    if (modal && s->o.fine_kernel == VF_FINE_MODAL) cand.push_back(-1);
     for (int n = 1; n <= 64; ++n) {
       const int c = (planes + n - 1) / n;
       if (c >= 1 && (modal ? c >= 2 : true) && ctas(c) >= floor_ctas &&
@@ -718,7 +722,7 @@ int autotune_levels(vf_solver* s) {
 }
 
 int auto_zchunk(const Grid& g, int requested) {
-  if (requested > 0) return requested;
+  if (requested != 0) return requested;
   const long long tiles = (long long)((g.lx + 1 + 30) / 31) * ((g.ly + 1 + 6) / 7);
   long long nz = (4LL * 148 + tiles - 1) / tiles;
   if (nz < 1) nz = 1;
@@ -968,7 +972,7 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
   if (o.precision < 0 || o.precision > 2 || o.method < 0 || o.method > 1 || o.coarse_op < 0 || o.coarse_op > 1 ||
       o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0 ||
       o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0 ||
-      o.fine_kernel < 0 || o.fine_kernel > 2 || o.modal_zchunk < 0 || o.coarse_storage < 0 ||
+      o.fine_kernel < 0 || o.fine_kernel > 2 || o.modal_zchunk < -1 || o.coarse_storage < 0 ||
       o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 2) {
     g_last_error = "invalid vf_options field";
     return VF_ERR_ARG;

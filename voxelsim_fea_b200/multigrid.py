@@ -50,7 +50,7 @@ class SolverOptions:
     omega_rel: float = 0.8
     power_iters: int = 20
     fine_kernel: str = "modal"       # "modal" (z-marching, TMA) | "modal_cpasync" | "gather" (27-neighbour)
-    modal_zchunk: int = 0            # z-planes per CTA of the modal kernel (0 = automatic)
+    modal_zchunk: int = 0            # z-planes per CTA of the modal kernel (0 = automatic, -1 = one even wave)
     coarse_storage: str = "sym_half"  # Galerkin stencils: "sym_half" | "sym" | "full"
 
     @classmethod
