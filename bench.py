@@ -242,7 +242,9 @@ def run_batch(args):
         raise SystemExit(f"bench: a batch part missed tol={TOL:g} (true residual {worst:.3e})")
     line = {"metric": METRIC, "value": ndof / (ms / 1e3) / 1e6, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (FP64 dots, refinement residual, coarsest solve)",
+            "vs_baseline": None,
+            "dtype": ("f32 V-cycle, f64 Krylov (FP64 fine operator for A p, dots, coarsest solve)"
+                      if args.mixed_mode == "outer64" else "f32 (FP64 dots, refinement residual, coarsest solve)"),
             "data": "synthetic (seeded generator)",
             "config": {"workload": f"batch{args.batch}_parts_32-128", "dof": ndof, "parts": args.batch,
                        "iterations_max": max(s.last_iters for s in solvers), "timing": "host clock, synchronous call"}}
@@ -465,7 +467,7 @@ def run_b200(args):
             "config": {"workload": args.workload + (f"_block{K}" if K > 1 else ""), "dof": ndof,
                        "rhs_per_step": K, "active_voxels": int(p["active"].sum()),
                        "levels": w["levels"], "solver": "mixed-precision GMG-PCG, Galerkin coarse ops, "
-                                                        "FP64 Cholesky coarsest",
+                                                        "FP64 Cholesky coarsest", "mixed_mode": args.mixed_mode,
                        "tol": TOL, "l2": "working set > 126 MB L2 (vectors 54-107 MB each)",
                        "parallelism": f"replicas x{world}"},
             "iterations": iters, "outer_iterations": outer, "true_resid": true_resid,
@@ -509,7 +511,7 @@ def main():
     ap.add_argument("--kernel-precision", choices=("fp32", "fp64"), default="fp32")
     ap.add_argument("--modal-zchunk", type=int, default=0, help="z-planes per CTA of the modal kernel (0 = auto)")
     ap.add_argument("--kernel-iters", type=int, default=3, help="launches timed by --kernel-profile")
-    ap.add_argument("--mixed-mode", choices=("reliable", "restart", "outer64"), default="reliable")
+    ap.add_argument("--mixed-mode", choices=("outer64", "reliable", "restart"), default="outer64")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed: residual reduction between FP64 corrections (solver default if unset)")
     args = ap.parse_args()

@@ -102,11 +102,11 @@ typedef struct vf_options {
                               scaled, FP16 values for the FP32 V-cycle and FP64 for FP64;
                               VF_STENCIL_SYM: symmetric scaled FP32 / FP64;
                               VF_STENCIL_FULL: all 27 blocks, unscaled */
-  int32_t mixed_mode;      /* VF_PREC_MIXED: VF_MIXED_RELIABLE (default): one FP32 CG whose
+  int32_t mixed_mode;      /* VF_PREC_MIXED: VF_MIXED_RELIABLE: one FP32 CG whose
                               residual is replaced by the FP64 true residual (and the FP32
                               increment folded into the FP64 solution) each time it has
                               dropped by inner_tol; VF_MIXED_RESTART: iterative refinement,
-                              a fresh FP32 PCG per outer step; VF_MIXED_OUTER64: FP64 PCG
+                              a fresh FP32 PCG per outer step; VF_MIXED_OUTER64 (default): FP64 PCG
                               (x, r, p, A p, dots and the fine operator of A p in FP64)
                               preconditioned by the FP32 V-cycle -- the FP64 Krylov space,
                               so the iteration count of the FP64 solve on hard problems */

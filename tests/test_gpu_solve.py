@@ -52,13 +52,13 @@ def test_cantilever_default_levels(gpu):
     assert abs(u[2::3].min() / float(g6["u_tip"]) - 1) < 1e-9
 
 
-@pytest.mark.parametrize("preset", ["robust", "fast", "outer64", "fp32"])
+@pytest.mark.parametrize("preset", ["robust", "fast", "reliable", "fp32"])
 def test_cantilever_b200_solvers(gpu, preset):
     from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
     g = golden("cantilever_64x16x16_L3.npz")
     p = _cantilever()
     opts = {"robust": SolverOptions.robust(), "fast": SolverOptions.fast(),
-            "outer64": SolverOptions.fast(mixed_mode="outer64"),
+            "reliable": SolverOptions.fast(mixed_mode="reliable"),
             "fp32": SolverOptions(precision="fp32", coarse="galerkin", coarsest="cholesky")}[preset]
     tol = 1e-5 if preset == "fp32" else 1e-10
     m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"], options=opts)
@@ -145,7 +145,7 @@ def test_set_fixed_required(gpu):
         v.solve(np.ones(64), np.zeros(375))
 
 
-@pytest.mark.parametrize("preset", ["robust", "fast", "outer64"])
+@pytest.mark.parametrize("preset", ["robust", "fast", "reliable"])
 def test_noise_bracket_converges(gpu, preset):
     """The reference's rediscretized MG does not converge on noise geometry;
     the Galerkin hierarchy with per-level damping must reach 1e-8 quickly, with
@@ -157,7 +157,7 @@ def test_noise_bracket_converges(gpu, preset):
     nx, ny, nz = p["dims"]
     E_mg = np.where(p["active"], p["E_stiff"], p["E_stiff"] * 1e-9)
     opts = {"robust": SolverOptions.robust(), "fast": SolverOptions.fast(),
-            "outer64": SolverOptions.fast(mixed_mode="outer64")}[preset]
+            "reliable": SolverOptions.fast(mixed_mode="reliable")}[preset]
     m = MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=4, options=opts)
     u = m.solve(E_mg, p["f"], tol=1e-8)
     assert m.last_converged
@@ -181,7 +181,7 @@ def test_outer64_tracks_fp64_iterations(gpu, flexible):
     nx, ny, nz = part["dims"]
     res = {}
     for name, opts in (("fp64", SolverOptions.robust(flexible=flexible)),
-                       ("outer64", SolverOptions.fast(mixed_mode="outer64", flexible=flexible))):
+                       ("outer64", SolverOptions.fast(flexible=flexible))):
         m = MGSolver(nx, ny, nz, part["fixed"], nu=0.3, options=opts)
         u = m.solve(part["E"], part["f"], tol=1e-8, nu_elem=part["nu"], max_cg=3000)
         res[name] = (u, m.last_iters, m.last_converged, m.last_info.true_resid)

@@ -932,7 +932,7 @@ void vf_options_default(vf_options* o) {
   o->fine_kernel = VF_FINE_MODAL;
   o->modal_zchunk = 0;
   o->coarse_storage = VF_STENCIL_SYM_HALF;
-  o->mixed_mode = VF_MIXED_RELIABLE;
+  o->mixed_mode = VF_MIXED_OUTER64;
   o->autotune = 1;
 }
 

@@ -182,6 +182,7 @@ def eval_configs():
     return (("plain_fp64", SolverOptions.robust(), False),
             ("learned_fp64", SolverOptions.robust(), True),
             ("mixed", SolverOptions.fast(), False),
+            ("mixed_reliable", SolverOptions.fast(mixed_mode="reliable"), False),
             ("mixed_restart", SolverOptions.fast(mixed_mode="restart", inner_tol=1e-4), False),
             ("learned_mixed_restart", SolverOptions.fast(mixed_mode="restart", inner_tol=1e-4), True),
             ("learned_mixed", SolverOptions.fast(), True))
@@ -201,7 +202,7 @@ def modes_configs():
     learned stage."""
     from ..multigrid import SolverOptions
     return (("plain_fp64", SolverOptions.robust(), False),
-            ("mixed", SolverOptions.fast(), False),
+            ("mixed_reliable", SolverOptions.fast(mixed_mode="reliable"), False),
             ("outer64", SolverOptions.fast(mixed_mode="outer64"), False),
             ("learned_outer64", SolverOptions.fast(mixed_mode="outer64"), True))
 

@@ -41,9 +41,9 @@ class SolverOptions:
     device: int = 0
     inner_tol: float = 1e-2          # mixed: residual reduction between FP64 corrections
     max_outer: int = 20              # mixed: cap on FP64 corrections
-    # mixed: "reliable" (FP32 CG, residual replacement) | "restart" (refinement) |
-    # "outer64" (FP64 PCG, FP32 V-cycle)
-    mixed_mode: str = "reliable"
+    # mixed: "outer64" (FP64 PCG, FP32 V-cycle) | "reliable" (FP32 CG, residual
+    # replacement) | "restart" (refinement)
+    mixed_mode: str = "outer64"
     flexible: bool = False           # flexible CG (automatic with a learned stage)
     autotune: bool = True            # time z-chunk candidates of the marching kernels at set-up
     omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
@@ -72,7 +72,8 @@ class SolverOptions:
 
     @classmethod
     def fast(cls, **kw):
-        """Galerkin hierarchy, mixed precision with FP64 refinement."""
+        """Galerkin hierarchy, mixed precision: by default FP64 PCG preconditioned by
+        the FP32 V-cycle (``mixed_mode="outer64"``)."""
         base = dict(coarse="galerkin", coarsest="cholesky", precision="mixed", omega_mode="auto",
                     stall_guard=False)
         base.update(kw)

@@ -11,6 +11,11 @@ bookkeeping, solve_worker.py:242-287); the unsupported-island removal, the
 solve and the von Mises stress on the device (VoxelFEA); the per-element
 displacement / safety-factor fields and the summary numbers as in
 solve_worker.py:356-431.
+
+One job key beyond the reference's: ``"solver": "reference"`` runs the
+reference's own multigrid algorithm (rediscretized levels, omega 0.6) instead
+of the default robust hierarchy; the solution is the same to the solver
+tolerance, the iteration count and history are then the reference's.
 """
 
 import json
@@ -197,6 +202,7 @@ def assemble(descr, masks, dims):
 def _worker_main(job_path, work_dir):
     from . import fea, inside
     from .fea import VoxelFEA
+    from .multigrid import SolverOptions
 
     status_path = os.path.join(work_dir, "status.json")
 
@@ -251,8 +257,10 @@ def _worker_main(job_path, work_dir):
     yield_strength = float(mat.get("yield_strength") or 0.0)
     active3d = active.reshape(nx, ny, nz)
     nelem = nx * ny * nz
+    mg_options = SolverOptions() if job.get("solver") == "reference" else None
     vfea = VoxelFEA(nx, ny, nz, nu=nu, active_elems=active3d, compute_mode=job.get("compute_mode", "AUTO"),
-                    cpu_threads=int(job.get("cpu_threads", 0)), verbose=bool(job.get("verbose", False)))
+                    cpu_threads=int(job.get("cpu_threads", 0)), verbose=bool(job.get("verbose", False)),
+                    mg_options=mg_options)
     last = [0.0]
 
     def _cg_progress(it, resid_ratio, tol):
