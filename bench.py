@@ -462,7 +462,9 @@ def run_b200(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (FP64 dots, refinement residual, coarsest solve)",
+            "vs_baseline": None,
+            "dtype": ("f32 V-cycle, f64 Krylov (FP64 fine operator for A p, dots, coarsest solve)"
+                      if args.mixed_mode == "outer64" else "f32 (FP64 dots, refinement residual, coarsest solve)"),
             "data": "synthetic (seeded generator)",
             "config": {"workload": args.workload + (f"_block{K}" if K > 1 else ""), "dof": ndof,
                        "rhs_per_step": K, "active_voxels": int(p["active"].sum()),
