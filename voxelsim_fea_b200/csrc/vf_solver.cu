@@ -685,8 +685,10 @@ int autotune_levels(vf_solver* s) {
     std::vector<int> cand;
     const int base = stencil ? sym_zchunk(l.g) : auto_zchunk(l.g, 0);
     cand.push_back(base);
-    // the TMA modal kernel's even one-wave split (z-chunk -1)
-    if (modal && s->o.fine_kernel == VF_FINE_MODAL) cand.push_back(-1);
+    // (the TMA modal kernel's one-wave split, z-chunk -1, is not a candidate:
+    // it is ~3 % faster on the 256x128x128 level but its CTAs march
+    // neighbouring tiles at different z, so the tile halos miss L2 and the
+    // DRAM traffic grows from 219 to 336 MB per sweep)
     for (int n = 1; n <= 64; ++n) {
       const int c = (planes + n - 1) / n;
       if (c >= 1 && (modal ? c >= 2 : true) && ctas(c) >= floor_ctas &&
