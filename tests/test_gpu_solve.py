@@ -191,3 +191,29 @@ def test_outer64_tracks_fp64_iterations(gpu, flexible):
     assert r32 < 1e-8
     assert it32 <= int(1.1 * it64) + 5, (it32, it64)
     assert np.abs(u32 - u64).max() <= 1e-5 * np.abs(u64).max()
+
+
+@pytest.mark.parametrize("dims", [(10, 6, 5), (16, 8, 8), (20, 12, 9)])
+def test_dense_coarsest_is_exact_inverse(gpu, dims):
+    """One level, coarsest solve = the dense FP64 Cholesky inverse: the
+    preconditioner is A^-1 up to rounding, so PCG converges in one to three
+    iterations, to the oracle's residual.  n = 1386, 4131 and 8190 DOFs (not
+    multiples of the 64-row tiles of the factorization kernels), a 1000:1
+    modulus contrast."""
+    from oracle import hex8
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    nx, ny, nz = dims
+    rng = np.random.default_rng(3)
+    ne = nx * ny * nz
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    E = np.where(rng.random(ne) < 0.5, 1.0, 1e-3) * 7e4
+    fixed = np.arange(3 * (nx + 1) * (ny + 1))            # z = 0 face clamped
+    f = np.zeros(ndof)
+    f[-3 * (nx + 1) * (ny + 1) + 2::3] = -1.0             # z = max face, -z
+    m = MGSolver(nx, ny, nz, fixed, nu=0.3, max_levels=1, options=SolverOptions.robust())
+    u = m.solve(E, f, tol=1e-12)
+    assert m.last_converged and m.last_iters <= 3, m.last_iters
+    free = np.ones(ndof, bool)
+    free[fixed] = False
+    r = f * free - hex8.element_apply(u, E, hex8.build_edof(nx, ny, nz), hex8.hex8_ke(1.0, 0.3), ndof) * free
+    assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(f)

@@ -86,26 +86,47 @@ __global__ void k_trsm_panel(double* A, int n, int k, int nb) {
   for (int j = 0; j < nb; ++j) A[(long long)i * n + k + j] = x[j];
 }
 
+// The three O(n^3) phases (trailing update, the update of Y = L^-1, Y^T Y)
+// run on 64 x 64 output tiles per CTA of 256 threads, each thread holding a
+// 4 x 4 register block (rows ty + 16a, columns tx + 16b): per inner index one
+// shared-memory load of 4 + 4 values feeds 16 FMAs.
+constexpr int TB = 64;
+
 // Trailing update (lower triangle): A[i][j] -= sum_l A[i][k+l] A[j][k+l].
-__global__ void k_syrk_update(double* A, int n, int k, int nb) {
+// Grid: one CTA per 64 x 64 tile pair bi >= bj of the trailing matrix.
+__global__ void __launch_bounds__(256) k_syrk_update(double* A, int n, int k, int nb) {
   const int t0 = k + nb;
   const int bi = blockIdx.y, bj = blockIdx.x;
   if (bj > bi) return;
-  const int i0 = t0 + bi * 32, j0 = t0 + bj * 32;
-  __shared__ double Pi[32][NB + 1], Pj[32][NB + 1];
-  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;   // 256 threads: ty 0..7
-  for (int r = ty; r < 32; r += 8) {
-    Pi[r][tx] = (i0 + r < n && tx < nb) ? A[(long long)(i0 + r) * n + k + tx] : 0.0;
-    Pj[r][tx] = (j0 + r < n && tx < nb) ? A[(long long)(j0 + r) * n + k + tx] : 0.0;
+  const int i0 = t0 + bi * TB, j0 = t0 + bj * TB;
+  __shared__ double Pi[TB][NB + 1], Pj[TB][NB + 1];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < TB * NB; e += 256) {
+    const int r = e / NB, l = e % NB;
+    Pi[r][l] = (i0 + r < n && l < nb) ? A[(long long)(i0 + r) * n + k + l] : 0.0;
+    Pj[r][l] = (j0 + r < n && l < nb) ? A[(long long)(j0 + r) * n + k + l] : 0.0;
   }
   __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    const int i = i0 + r, j = j0 + tx;
-    if (i >= n || j >= n || j > i) continue;
-    double s = 0.0;
-    for (int l = 0; l < nb; ++l) s += Pi[r][l] * Pj[tx][l];
-    A[(long long)i * n + j] -= s;
+  const int tx = tid % 16, ty = tid / 16;
+  double acc[4][4] = {};
+  for (int l = 0; l < nb; ++l) {
+    double pi[4], pj[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) pi[a] = Pi[ty + 16 * a][l];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) pj[b] = Pj[tx + 16 * b][l];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(pi[a], pj[b], acc[a][b]);
   }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      if (i < n && j <= i) A[(long long)i * n + j] -= acc[a][b];
+    }
 }
 
 // Forward substitution block: Y[k:k+nb, 0:ncol] <- L_kk^{-1} Y[k:k+nb, 0:ncol].
@@ -128,59 +149,86 @@ __global__ void k_trsv_block_rows(const double* A, double* Y, int n, int k, int 
 }
 
 // Y[i, 0:ncol] -= sum_l L[i][k+l] Y[k+l, 0:ncol] for i >= k+nb.
-__global__ void k_trsm_update(const double* A, double* Y, int n, int k, int nb, int ncol) {
-  const int i0 = k + nb + blockIdx.y * 32, c0 = blockIdx.x * 32;
-  __shared__ double Li[32][NB + 1], Yk[NB][33];
-  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
-  for (int r = ty; r < 32; r += 8) {
-    Li[r][tx] = (i0 + r < n && tx < nb) ? A[(long long)(i0 + r) * n + k + tx] : 0.0;
-    Yk[r][tx] = (r < nb && c0 + tx < ncol) ? Y[(long long)(k + r) * n + c0 + tx] : 0.0;
+// Grid: (column tiles of 64, row tiles of 64 below the block).
+__global__ void __launch_bounds__(256) k_trsm_update(const double* A, double* Y, int n, int k, int nb, int ncol) {
+  const int i0 = k + nb + blockIdx.y * TB, c0 = blockIdx.x * TB;
+  __shared__ double Li[TB][NB + 1], Yk[NB][TB + 1];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < TB * NB; e += 256) {
+    const int r = e / NB, l = e % NB;
+    Li[r][l] = (i0 + r < n && l < nb) ? A[(long long)(i0 + r) * n + k + l] : 0.0;
+    const int lr = e / TB, c = e % TB;
+    Yk[lr][c] = (lr < nb && c0 + c < ncol) ? Y[(long long)(k + lr) * n + c0 + c] : 0.0;
   }
   __syncthreads();
-  for (int r = ty; r < 32; r += 8) {
-    const int i = i0 + r, c = c0 + tx;
-    if (i >= n || c >= ncol) continue;
-    double s = 0.0;
-    for (int l = 0; l < nb; ++l) s += Li[r][l] * Yk[l][tx];
-    Y[(long long)i * n + c] -= s;
+  const int tx = tid % 16, ty = tid / 16;
+  double acc[4][4] = {};
+  for (int l = 0; l < nb; ++l) {
+    double li[4], yk[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) li[a] = Li[ty + 16 * a][l];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) yk[b] = Yk[l][tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(li[a], yk[b], acc[a][b]);
   }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + ty + 16 * a, c = c0 + tx + 16 * b;
+      if (i < n && c < ncol) Y[(long long)i * n + c] -= acc[a][b];
+    }
 }
 
 // Ainv = Y^T Y (Y lower triangular): Ainv[i][j] = sum_{l >= max(i,j)} Y[l][i] Y[l][j].
-// A^-1 = Y^T Y is symmetric: one CTA per 32x32 tile of the lower triangle
+// A^-1 = Y^T Y is symmetric: one CTA per 64x64 tile of the lower triangle
 // (blockIdx.x enumerates the pairs bi >= bj), written to both triangles.
-__global__ void k_yty(const double* Y, double* Ainv, int n) {
+__global__ void __launch_bounds__(256) k_yty(const double* Y, double* Ainv, int n) {
   int bi = (int)((sqrt(8.0 * blockIdx.x + 1.0) - 1.0) * 0.5);
   while ((bi + 1) * (bi + 2) / 2 <= (int)blockIdx.x) ++bi;
   while (bi * (bi + 1) / 2 > (int)blockIdx.x) --bi;
   const int bj = (int)blockIdx.x - bi * (bi + 1) / 2;
-  const int i0 = bi * 32, j0 = bj * 32;
-  __shared__ double Yi[32][33], Yj[32][33];
-  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
-  double acc[4] = {0, 0, 0, 0};
+  const int i0 = bi * TB, j0 = bj * TB;
+  constexpr int LC = 32;   // inner-index chunk
+  __shared__ double Yi[LC][TB + 1], Yj[LC][TB + 1];
+  const int tid = threadIdx.x;
+  const int tx = tid % 16, ty = tid / 16;
+  double acc[4][4] = {};
   const int lstart = (i0 > j0 ? i0 : j0);
-  for (int l0 = lstart; l0 < n; l0 += 32) {
-    for (int r = ty; r < 32; r += 8) {
+  for (int l0 = lstart; l0 < n; l0 += LC) {
+    for (int e = tid; e < LC * TB; e += 256) {
+      const int r = e / TB, c = e % TB;
       const int l = l0 + r;
-      Yi[r][tx] = (l < n && i0 + tx < n) ? Y[(long long)l * n + i0 + tx] : 0.0;
-      Yj[r][tx] = (l < n && j0 + tx < n) ? Y[(long long)l * n + j0 + tx] : 0.0;
+      Yi[r][c] = (l < n && i0 + c < n) ? Y[(long long)l * n + i0 + c] : 0.0;
+      Yj[r][c] = (l < n && j0 + c < n) ? Y[(long long)l * n + j0 + c] : 0.0;
     }
     __syncthreads();
-    for (int q = 0; q < 4; ++q) {
-      const int r = ty + 8 * q;
-      double s = 0.0;
-      for (int l = 0; l < 32; ++l) s += Yi[l][r] * Yj[l][tx];
-      acc[q] += s;
+    for (int l = 0; l < LC; ++l) {
+      double yi[4], yj[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) yi[a] = Yi[l][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) yj[b] = Yj[l][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(yi[a], yj[b], acc[a][b]);
     }
     __syncthreads();
   }
-  for (int q = 0; q < 4; ++q) {
-    const int i = i0 + ty + 8 * q, j = j0 + tx;
-    if (i < n && j < n) {
-      Ainv[(long long)i * n + j] = acc[q];
-      Ainv[(long long)j * n + i] = acc[q];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      if (i < n && j < n) {
+        Ainv[(long long)i * n + j] = acc[a][b];
+        Ainv[(long long)j * n + i] = acc[a][b];
+      }
     }
-  }
 }
 
 __global__ void k_set_identity(double* Y, int n) {
@@ -246,7 +294,7 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
     const int rest = n - k - nb;
     if (rest > 0) {
       launch_k(k_trsm_panel, (rest + 127) / 128, 128, 0, st, A, n, k, nb);
-      const int tiles = (rest + 31) / 32;
+      const int tiles = (rest + TB - 1) / TB;
       launch_k(k_syrk_update, dim3(tiles, tiles), 256, 0, st, A, n, k, nb);
     }
   }
@@ -258,11 +306,11 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
     launch_k(k_trsv_block_rows, (ncol + 127) / 128, 128, 0, st, A, work, n, k, nb, ncol);
     const int rest = n - k - nb;
     if (rest > 0) {
-      launch_k(k_trsm_update, dim3((ncol + 31) / 32, (rest + 31) / 32), 256, 0, st, A, work, n, k, nb, ncol);
+      launch_k(k_trsm_update, dim3((ncol + TB - 1) / TB, (rest + TB - 1) / TB), 256, 0, st, A, work, n, k, nb, ncol);
     }
   }
   // A <- Y^T Y (lower-triangle tiles, mirrored)
-  const int tiles = (n + 31) / 32;
+  const int tiles = (n + TB - 1) / TB;
   launch_k(k_yty, dim3(tiles * (tiles + 1) / 2), 256, 0, st, work, A, n);
   return 0;
 }
