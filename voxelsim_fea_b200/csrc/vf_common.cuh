@@ -212,9 +212,11 @@ template <typename T> void launch_sub_inplace(const Grid& g, T* y, const T* x, c
 template <typename T> void launch_axpy_gamma(const Grid& g, T* z, const T* c, const KrylovState* ks, const int* skip,
                                              cudaStream_t st);
 // power iteration on D^-1 A (per-level damping)
-void launch_power_init(const Grid& g, double* x, const uint8_t* mask, cudaStream_t st);
-void launch_power_scale(const Grid& g, double* y, const double* minv3, double* partials, KrylovState* ks, cudaStream_t st);
-void launch_power_normalize(const Grid& g, const double* y, double* x, const KrylovState* ks, cudaStream_t st);
+template <typename T> void launch_power_init(const Grid& g, T* x, const uint8_t* mask, cudaStream_t st);
+template <typename T>
+void launch_power_scale(const Grid& g, T* y, const T* minv3, double* partials, KrylovState* ks, cudaStream_t st);
+template <typename T>
+void launch_power_normalize(const Grid& g, const T* y, T* x, const KrylovState* ks, cudaStream_t st);
 void launch_power_omega(const KrylovState* ks, double omega_rel, double safety, double* omega_out, double* lambda_out, cudaStream_t st);
 
 // vf_post.cu -- post-processing and the island pre-step

@@ -257,33 +257,35 @@ __global__ void k_sub_from(long long n3, const double* __restrict__ f, double* _
 }
 
 // Power iteration on D^-1 A: x_0 = deterministic pseudo-random free vector.
-__global__ void k_power_init(long long n, double* __restrict__ x, const uint8_t* __restrict__ mask) {
+template <typename T>
+__global__ void k_power_init(long long n, T* __restrict__ x, const uint8_t* __restrict__ mask) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
     const uint8_t m = mask[p];
     for (int c = 0; c < 3; ++c) {
       unsigned long long h = (unsigned long long)(3 * p + c) * 0x9E3779B97F4A7C15ULL;
       h ^= h >> 31; h *= 0xBF58476D1CE4E5B9ULL; h ^= h >> 29;
       const double v = (double)(h >> 11) * (1.0 / 9007199254740992.0) - 0.5;
-      x[3 * p + c] = ((m >> c) & 1) ? v : 0.0;
+      x[3 * p + c] = ((m >> c) & 1) ? (T)v : (T)0;
     }
   }
 }
 
-__global__ void __launch_bounds__(kVecThreads) k_power_scale(long long n, double* __restrict__ y,
-                                                             const double* __restrict__ minv, double* partials,
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_power_scale(long long n, T* __restrict__ y,
+                                                             const T* __restrict__ minv, double* partials,
                                                              KrylovState* ks) {
   double s = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const double v = y[i] * minv[i];
+    const T v = y[i] * minv[i];
     y[i] = v;
-    s += v * v;
+    s += (double)v * (double)v;
   }
   reduce_and_finalize(s, partials, ks, SLOT_PLAIN, nullptr);
 }
 
-__global__ void k_power_normalize(long long n, const double* __restrict__ y, double* __restrict__ x,
-                                  const KrylovState* ks) {
-  const double inv = ks->rr > 0.0 ? 1.0 / sqrt(ks->rr) : 0.0;
+template <typename T>
+__global__ void k_power_normalize(long long n, const T* __restrict__ y, T* __restrict__ x, const KrylovState* ks) {
+  const T inv = ks->rr > 0.0 ? (T)(1.0 / sqrt(ks->rr)) : (T)0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     x[i] = y[i] * inv;
 }
@@ -298,16 +300,25 @@ __global__ void k_power_omega(const KrylovState* ks, double omega_rel, double sa
 
 }  // namespace
 
-void launch_power_init(const Grid& g, double* x, const uint8_t* mask, cudaStream_t st) {
-  launch_k(k_power_init, kVecBlocks, kVecThreads, 0, st, (long long)g.n, x, mask);
+template <typename T>
+void launch_power_init(const Grid& g, T* x, const uint8_t* mask, cudaStream_t st) {
+  launch_k(k_power_init<T>, kVecBlocks, kVecThreads, 0, st, (long long)g.n, x, mask);
 }
-void launch_power_scale(const Grid& g, double* y, const double* minv3, double* partials, KrylovState* ks,
-                        cudaStream_t st) {
-  launch_k(k_power_scale, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, y, minv3, partials, ks);
+template <typename T>
+void launch_power_scale(const Grid& g, T* y, const T* minv3, double* partials, KrylovState* ks, cudaStream_t st) {
+  launch_k(k_power_scale<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, y, minv3, partials, ks);
 }
-void launch_power_normalize(const Grid& g, const double* y, double* x, const KrylovState* ks, cudaStream_t st) {
-  launch_k(k_power_normalize, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, y, x, ks);
+template <typename T>
+void launch_power_normalize(const Grid& g, const T* y, T* x, const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_power_normalize<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, y, x, ks);
 }
+#define VF_INST_POWER(T)                                                                                   \
+  template void launch_power_init<T>(const Grid&, T*, const uint8_t*, cudaStream_t);                       \
+  template void launch_power_scale<T>(const Grid&, T*, const T*, double*, KrylovState*, cudaStream_t);     \
+  template void launch_power_normalize<T>(const Grid&, const T*, T*, const KrylovState*, cudaStream_t);
+VF_INST_POWER(double)
+VF_INST_POWER(float)
+#undef VF_INST_POWER
 void launch_power_omega(const KrylovState* ks, double omega_rel, double safety, double* omega_out,
                         double* lambda_out, cudaStream_t st) {
   launch_k(k_power_omega, 1, 1, 0, st, ks, omega_rel, safety, omega_out, lambda_out);

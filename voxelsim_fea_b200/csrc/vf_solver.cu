@@ -789,13 +789,16 @@ int set_level_omegas(vf_solver* s) {
   }
   init_ks(*s->h_ks, 1.0, 1, 0, 0, 1.0);
   VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  // in FP32 on the V-cycle's FP32 operators (half-precision scaled stencils
+  // on Galerkin levels): lambda is needed to a few percent (it is padded by
+  // the 1.1 safety factor), and the FP32 sweeps cost half the FP64 ones
   for (int li = 0; li < nl; ++li) {
     Level& l = s->L[li];
-    launch_power_init(l.g, l.w64[0], l.mask, s->st);
+    launch_power_init<float>(l.g, l.w32[0], l.mask, s->st);
     for (int k = 0; k < std::max(2, s->o.power_iters); ++k) {
-      level_op<double>(s, li, EPI_APPLY, l.w64[0], l.w64[1], nullptr, nullptr, nullptr, 0);
-      launch_power_scale(l.g, l.w64[1], l.minv64, s->d_partials, s->ks, s->st);
-      launch_power_normalize(l.g, l.w64[1], l.w64[0], s->ks, s->st);
+      level_op<float>(s, li, EPI_APPLY, l.w32[0], l.w32[1], nullptr, nullptr, nullptr, 0);
+      launch_power_scale<float>(l.g, l.w32[1], l.minv32, s->d_partials, s->ks, s->st);
+      launch_power_normalize<float>(l.g, l.w32[1], l.w32[0], s->ks, s->st);
     }
     launch_power_omega(s->ks, s->o.omega_rel, 1.1, s->d_omega + li, s->d_lambda + li, s->st);
   }
