@@ -185,6 +185,7 @@ template <typename T> void launch_jacobi_from_zero(const Grid& g, const T* b, co
 // vf_dense.cu -- coarsest-level dense FP64 direct solve
 int dense_assemble(const Grid& c, const double* stencil, const uint8_t* cmask, double* A, int n, cudaStream_t st);
 int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStream_t st);
+size_t dense_work_count(int n);
 template <typename T> void launch_dense_solve(const Grid& c, const double* Ainv, int n, const T* b, T* x, const KrylovState* ks, cudaStream_t st);
 
 // vf_krylov.cu -- fused PCG vector kernels with deterministic FP64 reductions

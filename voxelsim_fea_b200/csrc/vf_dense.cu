@@ -39,14 +39,18 @@ __global__ void k_dense_assemble(Grid c, const double* __restrict__ st, const ui
   }
 }
 
-// Factor the nb x nb diagonal block at (k, k) (rows already updated).
-__global__ void k_potrf_diag(double* A, int n, int k, int nb, int* info) {
-  __shared__ double L[NB][NB + 1];
-  const int t = threadIdx.x;
-  for (int j = 0; j < nb; ++j) L[t][j] = (t < nb) ? A[(long long)(k + t) * n + k + j] : 0.0;
+// Factor the nb x nb diagonal block at (k, k) (rows already updated) and
+// invert it: L_kk -> A's lower block, L_kk^-1 -> linv (NB x NB, zero padded).
+// 1024 threads, one per (row t, column c) of the block; the panel solve and
+// the block-row solve of the inverse phase then multiply by linv instead of
+// substituting row by row.
+__global__ void __launch_bounds__(NB * NB) k_potrf_diag(double* A, int n, int k, int nb, int* info, double* linv) {
+  __shared__ double L[NB][NB + 1], X[NB][NB + 1];
+  const int c = threadIdx.x % NB, t = threadIdx.x / NB;
+  L[t][c] = (t < nb && c <= t) ? A[(long long)(k + t) * n + k + c] : 0.0;
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
-    if (t == j) {
+    if (t == j && c == j) {
       const double d = L[j][j];
       if (!(d > 0.0)) {
         if (*info == 0) *info = k + j + 1;
@@ -56,34 +60,43 @@ __global__ void k_potrf_diag(double* A, int n, int k, int nb, int* info) {
       }
     }
     __syncthreads();
-    const double piv = L[j][j];
-    if (t > j && t < nb) L[t][j] /= piv;
+    if (c == j && t > j && t < nb) L[t][j] /= L[j][j];
     __syncthreads();
-    if (t > j && t < nb)
-      for (int l = j + 1; l <= t; ++l) L[t][l] -= L[t][j] * L[l][j];
+    if (t > j && t < nb && c > j && c <= t) L[t][c] -= L[t][j] * L[c][j];
     __syncthreads();
   }
-  if (t < nb)
-    for (int j = 0; j <= t; ++j) A[(long long)(k + t) * n + k + j] = L[t][j];
+  // X = L^-1, one row per step (all columns at once): X[r][c] for c <= r
+  for (int r = 0; r < nb; ++r) {
+    if (t == r) {
+      double v = (r == c) ? 1.0 : 0.0;
+      for (int l = c; l < r; ++l) v -= L[r][l] * X[l][c];
+      X[r][c] = (c <= r) ? v / L[r][r] : 0.0;
+    }
+    __syncthreads();
+  }
+  if (t < nb && c <= t) A[(long long)(k + t) * n + k + c] = L[t][c];
+  linv[t * NB + c] = (t < nb && c < nb) ? X[t][c] : 0.0;
 }
 
-// Rows i >= k+nb: A[i, k:k+nb] <- A[i, k:k+nb] L_kk^{-T}.
-__global__ void k_trsm_panel(double* A, int n, int k, int nb) {
-  __shared__ double L[NB][NB + 1];
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, j = e % nb;
-    L[i][j] = (j <= i) ? A[(long long)(k + i) * n + k + j] : 0.0;
+// Rows i >= k+nb: A[i, k:k+nb] <- A[i, k:k+nb] L_kk^-T, i.e.
+// X[i][j] = sum_{l <= j} A[i][k+l] linv[j][l].  64 rows per CTA.
+__global__ void __launch_bounds__(256) k_trsm_panel(double* A, int n, int k, int nb, const double* linv) {
+  __shared__ double P[64][NB + 1], Li[NB][NB + 1];
+  const int tid = threadIdx.x;
+  const int i0 = k + nb + blockIdx.x * 64;
+  for (int e = tid; e < NB * NB; e += 256) Li[e / NB][e % NB] = linv[e];
+  for (int e = tid; e < 64 * NB; e += 256) {
+    const int r = e / NB, l = e % NB;
+    P[r][l] = (i0 + r < n && l < nb) ? A[(long long)(i0 + r) * n + k + l] : 0.0;
   }
   __syncthreads();
-  const int i = k + nb + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double x[NB];
-  for (int j = 0; j < nb; ++j) {
-    double v = A[(long long)i * n + k + j];
-    for (int l = 0; l < j; ++l) v -= x[l] * L[j][l];
-    x[j] = v / L[j][j];
+  const int c = tid % NB, r0 = tid / NB;
+  for (int a = 0; a < 8; ++a) {
+    const int r = r0 + 8 * a;
+    double v = 0.0;
+    for (int l = 0; l <= c; ++l) v = fma(P[r][l], Li[c][l], v);
+    if (i0 + r < n && c < nb) A[(long long)(i0 + r) * n + k + c] = v;
   }
-  for (int j = 0; j < nb; ++j) A[(long long)i * n + k + j] = x[j];
 }
 
 // The three O(n^3) phases (trailing update, the update of Y = L^-1, Y^T Y)
@@ -129,23 +142,26 @@ __global__ void __launch_bounds__(256) k_syrk_update(double* A, int n, int k, in
     }
 }
 
-// Forward substitution block: Y[k:k+nb, 0:ncol] <- L_kk^{-1} Y[k:k+nb, 0:ncol].
-__global__ void k_trsv_block_rows(const double* A, double* Y, int n, int k, int nb, int ncol) {
-  __shared__ double L[NB][NB + 1];
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, j = e % nb;
-    L[i][j] = (j <= i) ? A[(long long)(k + i) * n + k + j] : 0.0;
+// Diagonal block of Y: Y[k:k+nb, 0:ncol] <- L_kk^{-1} Y[k:k+nb, 0:ncol]
+// (a product with linv; each CTA owns 64 columns, read whole before written).
+__global__ void __launch_bounds__(256) k_trsv_block_rows(const double* linv, double* Y, int n, int k, int nb,
+                                                         int ncol) {
+  __shared__ double Li[NB][NB + 1], Yb[NB][64 + 1];
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * 64;
+  for (int e = tid; e < NB * NB; e += 256) Li[e / NB][e % NB] = linv[e];
+  for (int e = tid; e < NB * 64; e += 256) {
+    const int l = e / 64, c = e % 64;
+    Yb[l][c] = (l < nb && c0 + c < ncol) ? Y[(long long)(k + l) * n + c0 + c] : 0.0;
   }
   __syncthreads();
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= ncol) return;
-  double x[NB];
-  for (int i = 0; i < nb; ++i) {
-    double v = Y[(long long)(k + i) * n + col];
-    for (int l = 0; l < i; ++l) v -= L[i][l] * x[l];
-    x[i] = v / L[i][i];
+  const int c = tid % 64, ir = tid / 64;
+  for (int a = 0; a < NB / 4; ++a) {
+    const int i = ir + 4 * a;
+    double v = 0.0;
+    for (int l = 0; l <= i; ++l) v = fma(Li[i][l], Yb[l][c], v);
+    if (i < nb && c0 + c < ncol) Y[(long long)(k + i) * n + c0 + c] = v;
   }
-  for (int i = 0; i < nb; ++i) Y[(long long)(k + i) * n + col] = x[i];
 }
 
 // Y[i, 0:ncol] -= sum_l L[i][k+l] Y[k+l, 0:ncol] for i >= k+nb.
@@ -284,16 +300,23 @@ int dense_assemble(const Grid& c, const double* stencil, const uint8_t* cmask, d
   return 0;
 }
 
-// A (n x n, lower part) is overwritten by L; work (n x n) receives A^{-1}
-// ... then copied back into A.  d_info > 0 flags a non-positive pivot.
+// Doubles of the work buffer: Y = L^-1 (n x n) and the inverted diagonal
+// blocks (NB x NB each).
+size_t dense_work_count(int n) { return (size_t)n * n + (size_t)((n + NB - 1) / NB) * NB * NB; }
+
+// A (n x n, lower part) is overwritten by L; work (dense_work_count(n))
+// receives Y = L^-1 and the inverted diagonal blocks; A <- Y^T Y = A^-1.
+// d_info > 0 flags a non-positive pivot.
 int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStream_t st) {
   cudaMemsetAsync(d_info, 0, sizeof(int), st);
+  double* linv_all = work + (size_t)n * n;
   for (int k = 0; k < n; k += NB) {
     const int nb = (n - k < NB) ? (n - k) : NB;
-    launch_k(k_potrf_diag, 1, NB, 0, st, A, n, k, nb, d_info);
+    double* linv = linv_all + (size_t)(k / NB) * NB * NB;
+    launch_k(k_potrf_diag, 1, NB * NB, 0, st, A, n, k, nb, d_info, linv);
     const int rest = n - k - nb;
     if (rest > 0) {
-      launch_k(k_trsm_panel, (rest + 127) / 128, 128, 0, st, A, n, k, nb);
+      launch_k(k_trsm_panel, (rest + 63) / 64, 256, 0, st, A, n, k, nb, (const double*)linv);
       const int tiles = (rest + TB - 1) / TB;
       launch_k(k_syrk_update, dim3(tiles, tiles), 256, 0, st, A, n, k, nb);
     }
@@ -303,7 +326,8 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
   for (int k = 0; k < n; k += NB) {
     const int nb = (n - k < NB) ? (n - k) : NB;
     const int ncol = k + nb;
-    launch_k(k_trsv_block_rows, (ncol + 127) / 128, 128, 0, st, A, work, n, k, nb, ncol);
+    const double* linv = linv_all + (size_t)(k / NB) * NB * NB;
+    launch_k(k_trsv_block_rows, (ncol + 63) / 64, 256, 0, st, linv, work, n, k, nb, ncol);
     const int rest = n - k - nb;
     if (rest > 0) {
       launch_k(k_trsm_update, dim3((ncol + TB - 1) / TB, (rest + TB - 1) / TB), 256, 0, st, A, work, n, k, nb, ncol);

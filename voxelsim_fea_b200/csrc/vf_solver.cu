@@ -616,7 +616,7 @@ int build_levels(vf_solver* s) {
     const int n = 3 * lc.g.nodes_ref();
     if (n <= 16384) {
       VF_ALLOC(s->d_Ainv, (size_t)n * n);
-      VF_ALLOC(s->d_dense_work, (size_t)n * n);
+      VF_ALLOC(s->d_dense_work, dense_work_count(n));
       s->dense_n = n;
       dense_prepare_smem(n);
       if (!lc.galerkin && !lc.st64) VF_ALLOC(lc.st64, 243 * (size_t)lc.g.n);
@@ -827,7 +827,7 @@ int build_dense_coarsest(vf_solver* s) {
   }
   if (s->dense_n != n) {
     VF_ALLOC(s->d_Ainv, (size_t)n * n);
-    VF_ALLOC(s->d_dense_work, (size_t)n * n);
+    VF_ALLOC(s->d_dense_work, dense_work_count(n));
     s->dense_n = n;
     dense_prepare_smem(n);
   }
