@@ -218,19 +218,26 @@ __global__ void __launch_bounds__(kThreads) k_galerkin_from_fine(Grid f, const d
   }
 }
 
-// Level l -> l+1 by stencil RAP (fine stencil already masked).
+// Level l -> l+1 by stencil RAP (fine stencil already masked).  One thread
+// per (coarse node, offset s) for the diagonal and the 13 upper offsets
+// s = 13..26 (consecutive threads: consecutive nodes of one offset); the 13
+// lower blocks are the transposed upper blocks of the neighbours
+// (k_stencil_mirror), so the coarse stencil is exactly symmetric.
 __global__ void __launch_bounds__(kThreads) k_galerkin_from_stencil(Grid f, const double* __restrict__ stf,
                                                                     Grid c, double* __restrict__ stc) {
   const int nx1 = c.lx + 1, ny1 = c.ly + 1;
-  const int nint = nx1 * ny1 * (c.lz + 1);
+  const long long nint = (long long)nx1 * ny1 * (c.lz + 1);
   const long long nf = f.n, nc = c.n;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
-    const int X = t % nx1;
-    const int rr = t / nx1;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 14 * nint;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = 13 + (int)(t / nint);
+    const int node = (int)(t % nint);
+    const int X = node % nx1;
+    const int rr = node / nx1;
     const int Y = rr % ny1;
     const int Z = rr / ny1;
     const int p = c.idx(X, Y, Z);
-    for (int s = 0; s < 27; ++s) {
+    {
       const int Dx = s % 3 - 1, Dy = (s / 3) % 3 - 1, Dz = s / 9 - 1;
       double acc[9];
 #pragma unroll
@@ -264,6 +271,32 @@ __global__ void __launch_bounds__(kThreads) k_galerkin_from_stencil(Grid f, cons
 #pragma unroll
       for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * nc + p] = acc[k];
     }
+  }
+}
+
+// Lower offsets s = 0..12 from the upper ones: block (s, p)[r][c] =
+// block (26 - s, p + off(s))[c][r] (zero where the neighbour is outside).
+__global__ void __launch_bounds__(kThreads) k_stencil_mirror(Grid c, double* __restrict__ stc) {
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1;
+  const long long nint = (long long)nx1 * ny1 * (c.lz + 1);
+  const long long nc = c.n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 13 * nint;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(t / nint);
+    const int node = (int)(t % nint);
+    const int X = node % nx1;
+    const int rr = node / nx1;
+    const int Y = rr % ny1;
+    const int Z = rr / ny1;
+    const int p = c.idx(X, Y, Z);
+    const int MX = X + s % 3 - 1, MY = Y + (s / 3) % 3 - 1, MZ = Z + s / 9 - 1;
+    const bool in = MX >= 0 && MX <= c.lx && MY >= 0 && MY <= c.ly && MZ >= 0 && MZ <= c.lz;
+    const long long q = in ? c.idx(MX, MY, MZ) : 0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+        stc[((long long)s * 9 + 3 * r + cc) * nc + p] = in ? stc[((long long)(26 - s) * 9 + 3 * cc + r) * nc + q] : 0.0;
   }
 }
 
@@ -401,7 +434,8 @@ void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu,
 void launch_galerkin_from_stencil(const Grid& f, const double* stencil_f, const Grid& c, double* stencil_c,
                                   cudaStream_t st) {
   long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
-  launch_k(k_galerkin_from_stencil, blocks_for(nint, kThreads), kThreads, 0, st, f, stencil_f, c, stencil_c);
+  launch_k(k_galerkin_from_stencil, blocks_for(14 * nint, kThreads), kThreads, 0, st, f, stencil_f, c, stencil_c);
+  launch_k(k_stencil_mirror, blocks_for(13 * nint, kThreads), kThreads, 0, st, c, stencil_c);
 }
 
 void launch_stencil_from_elements(const Grid& g, const double* E, const double* mu, const uint8_t* mask,
