@@ -34,34 +34,6 @@ inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
   kern<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
 }
 
-// Programmatic dependent launch for the kernels of the PCG iteration: the
-// kernel may be scheduled while its predecessor on the stream finishes (its
-// CTAs take the SM slots the predecessor's last wave frees).  Only kernels
-// that begin with pdl_enter() are launched this way: pdl_enter waits until
-// the predecessor grid has completed and its writes are visible, before the
-// kernel reads or writes anything, then lets its own dependents launch.
-template <typename... KArgs, typename... Args>
-inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                       Args&&... args) {
-  count_launch(st);
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
-}
-
-__device__ __forceinline__ void pdl_enter() {
-  asm volatile("griddepcontrol.wait;\n" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
-}
-
 struct Grid {
   int lx, ly, lz;   // voxels
   int px, py, pz;   // padded node box

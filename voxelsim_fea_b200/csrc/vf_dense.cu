@@ -257,7 +257,6 @@ __global__ void k_set_identity(double* Y, int n) {
 template <typename T>
 __global__ void k_dense_solve(Grid c, const double* __restrict__ Ainv, int n, const T* __restrict__ b,
                               T* __restrict__ x, const KrylovState* ks) {
-  pdl_enter();
   if (ks && ks->done) return;
   extern __shared__ double sb[];
   const int nx1 = c.lx + 1, ny1 = c.ly + 1;
@@ -354,7 +353,7 @@ template <typename T>
 void launch_dense_solve(const Grid& c, const double* Ainv, int n, const T* b, T* x, const KrylovState* ks,
                         cudaStream_t st) {
   int blocks = (n + 7) / 8;   // one row per warp: every row's stream in flight at once
-  launch_pdl(k_dense_solve<T>, blocks, 256, sizeof(double) * n, st, c, Ainv, n, b, x, ks);
+  launch_k(k_dense_solve<T>, blocks, 256, sizeof(double) * n, st, c, Ainv, n, b, x, ks);
 }
 template void launch_dense_solve<double>(const Grid&, const double*, int, const double*, double*, const KrylovState*, cudaStream_t);
 template void launch_dense_solve<float>(const Grid&, const double*, int, const float*, float*, const KrylovState*, cudaStream_t);

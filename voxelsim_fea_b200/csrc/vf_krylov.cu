@@ -33,7 +33,6 @@ template <> struct V16<double> {
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_dot(long long n3, const T* __restrict__ a, const T* __restrict__ b,
                                                      double* partials, KrylovState* ks, int slot) {
-  pdl_enter();
   if (ks->done && slot != SLOT_FNORM && slot != SLOT_RZ_INIT && slot != SLOT_OUTER && slot != SLOT_PLAIN) return;
   using H = V16<T>;
   using V = typename H::V;
@@ -50,7 +49,6 @@ template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_cg_update(long long n3, T* __restrict__ x, const T* __restrict__ p,
                                                            T* __restrict__ r, const T* __restrict__ Ap,
                                                            double* partials, KrylovState* ks, double* hist) {
-  pdl_enter();
   if (ks->done) return;
   using H = V16<T>;
   using V = typename H::V;
@@ -75,7 +73,6 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_update(long long n3, T* __re
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_dot_fcg(long long n3, const T* __restrict__ r, const T* __restrict__ z,
                                                          const T* __restrict__ Ap, double* partials, KrylovState* ks) {
-  pdl_enter();
   if (ks->done) return;
   using H = V16<T>;
   using V = typename H::V;
@@ -95,7 +92,6 @@ __global__ void __launch_bounds__(kVecThreads) k_dot_fcg(long long n3, const T* 
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_p_update(long long n3, T* __restrict__ p, const T* __restrict__ z,
                                                           const KrylovState* ks) {
-  pdl_enter();
   if (ks->done) return;
   using H = V16<T>;
   using V = typename H::V;
@@ -117,7 +113,6 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_update_split(long long n3, d
                                                                  const double* __restrict__ p, double* __restrict__ r,
                                                                  const double* __restrict__ Ap, float* __restrict__ r32,
                                                                  double* partials, KrylovState* ks, double* hist) {
-  pdl_enter();
   if (ks->done) return;
   const double alpha = ks->alpha;
   const long long n4 = n3 / 4;
@@ -147,7 +142,6 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_update_split(long long n3, d
 // p = z + beta p (p FP64, z FP32)
 __global__ void __launch_bounds__(kVecThreads) k_p_update_split(long long n3, double* __restrict__ p,
                                                                 const float* __restrict__ z, const KrylovState* ks) {
-  pdl_enter();
   if (ks->done) return;
   const bool restart = ks->restart != 0;
   const double beta = restart ? 0.0 : ks->beta;
@@ -168,7 +162,6 @@ __global__ void __launch_bounds__(kVecThreads) k_dot_fcg_split(long long n3, con
                                                                const float* __restrict__ z,
                                                                const double* __restrict__ Ap, double* partials,
                                                                KrylovState* ks) {
-  pdl_enter();
   if (ks->done) return;
   const long long n4 = n3 / 4;
   const float4* rv = reinterpret_cast<const float4*>(r);
@@ -205,7 +198,6 @@ __global__ void k_jacobi_precond(int n, const T* __restrict__ r, const T* __rest
 
 template <typename T>
 __global__ void k_copy(long long n3, const T* __restrict__ s, T* __restrict__ d, const KrylovState* ks) {
-  pdl_enter();
   if (ks && ks->done) return;
   const long long n16 = n3 * (long long)sizeof(T) / 16;   // 16-byte chunks
   const float4* sv = reinterpret_cast<const float4*>(s);
@@ -334,16 +326,16 @@ void launch_power_omega(const KrylovState* ks, double omega_rel, double safety, 
 
 template <typename T>
 void launch_dot(const Grid& g, const T* a, const T* b, double* partials, KrylovState* ks, int slot, cudaStream_t st) {
-  launch_pdl(k_dot<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, a, b, partials, ks, slot);
+  launch_k(k_dot<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, a, b, partials, ks, slot);
 }
 template <typename T>
 void launch_cg_update(const Grid& g, T* x, const T* p, T* r, const T* Ap, double* partials, KrylovState* ks,
                       double* hist, cudaStream_t st) {
-  launch_pdl(k_cg_update<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, p, r, Ap, partials, ks, hist);
+  launch_k(k_cg_update<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, p, r, Ap, partials, ks, hist);
 }
 template <typename T>
 void launch_p_update(const Grid& g, T* p, const T* z, KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_p_update<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, p, z, ks);
+  launch_k(k_p_update<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, p, z, ks);
 }
 template <typename T>
 void launch_jacobi_precond(const Grid& g, const T* r, const T* minv3, const uint8_t* mask, T* z,
@@ -352,10 +344,10 @@ void launch_jacobi_precond(const Grid& g, const T* r, const T* minv3, const uint
 }
 template <typename T>
 void launch_copy_vec(const Grid& g, const T* src, T* dst, const KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_copy<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, src, dst, ks);
+  launch_k(k_copy<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, src, dst, ks);
 }
 void launch_norm2_f64(const Grid& g, const double* v, double* partials, KrylovState* ks, int slot, cudaStream_t st) {
-  launch_pdl(k_dot<double>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, v, v, partials, ks, slot);
+  launch_k(k_dot<double>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, v, v, partials, ks, slot);
 }
 void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState* ks, cudaStream_t st) {
   launch_k(k_ir_prepare, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r64, r32, ks);
@@ -385,14 +377,14 @@ void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st)
 
 void launch_cg_update_split(const Grid& g, double* x, const double* p, double* r, const double* Ap, float* r32,
                             double* partials, KrylovState* ks, double* hist, cudaStream_t st) {
-  launch_pdl(k_cg_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, p, r, Ap, r32, partials, ks, hist);
+  launch_k(k_cg_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, p, r, Ap, r32, partials, ks, hist);
 }
 void launch_p_update_split(const Grid& g, double* p, const float* z, KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_p_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, p, z, (const KrylovState*)ks);
+  launch_k(k_p_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, p, z, (const KrylovState*)ks);
 }
 void launch_dot_fcg_split(const Grid& g, const float* r, const float* z, const double* Ap, double* partials,
                           KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_dot_fcg_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r, z, Ap, partials, ks);
+  launch_k(k_dot_fcg_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r, z, Ap, partials, ks);
 }
 void launch_scale64(const Grid& g, const double* x, double* y, double sc, cudaStream_t st) {
   launch_k(k_scale64, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, y, sc);
@@ -401,7 +393,7 @@ void launch_scale64(const Grid& g, const double* x, double* y, double sc, cudaSt
 template <typename T>
 void launch_dot_fcg(const Grid& g, const T* r, const T* z, const T* Ap, double* partials, KrylovState* ks,
                     cudaStream_t st) {
-  launch_pdl(k_dot_fcg<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r, z, Ap, partials, ks);
+  launch_k(k_dot_fcg<T>, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r, z, Ap, partials, ks);
 }
 
 #define VF_INST(T)                                                                                            \

@@ -105,7 +105,6 @@ __global__ void __launch_bounds__(TX * TY, 2)
     k_modal_tma(Grid g, OpArgs a, ModalConst mc, int zchunk, const __grid_constant__ CUtensorMap tm_u,
                 const __grid_constant__ CUtensorMap tm_e, const __grid_constant__ CUtensorMap tm_m,
                 const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_d) {
-  pdl_enter();
   using O = Pack<T>;
   using P = typename O::P;
   using Lay = Layout<T, LAME, EPI>;
@@ -436,7 +435,7 @@ bool launch_modal_tma(const Grid& g, int epi, const OpArgs& a, const ModalConst&
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);                      \
       nb = std::min<long long>((long long)sms * per_sm.load(), units);                        \
     }                                                                                         \
-    launch_pdl(kern, dim3((unsigned)nb), block, smem, st, g, a, mc, zchunk, mu, me, mm, mb, md); \
+    launch_k(kern, dim3((unsigned)nb), block, smem, st, g, a, mc, zchunk, mu, me, mm, mb, md); \
   } while (0)
   if (lame) {
     if (epi == EPI_APPLY) VF_TMA_ONE(true, EPI_APPLY);

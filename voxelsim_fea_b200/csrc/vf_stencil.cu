@@ -564,7 +564,6 @@ constexpr int SX = 32, SY = 8;   // node tile of the marching stencil kernel
 template <typename T, typename S, int EPI>
 __global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, const S* __restrict__ stc,
                                                            const T* __restrict__ sqd, int zchunk) {
-  pdl_enter();
   using Lay = SymLayout<S>;
   using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
   constexpr int VPC = Lay::VPC;
@@ -727,9 +726,9 @@ void launch_stencil_sym_op(const Grid& g, int epi, const OpArgs& a, const S* stc
   if (zchunk < 1) zchunk = sym_zchunk(g);
   const dim3 grid((g.lx + 1 + SX - 1) / SX, (g.ly + 1 + SY - 1) / SY, (g.lz + 1 + zchunk - 1) / zchunk);
   const dim3 block(SX, SY);
-  if (epi == EPI_APPLY) launch_pdl(k_sym_march<T, S, EPI_APPLY>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
-  else if (epi == EPI_SMOOTH) launch_pdl(k_sym_march<T, S, EPI_SMOOTH>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
-  else launch_pdl(k_sym_march<T, S, EPI_RESID>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
+  if (epi == EPI_APPLY) launch_k(k_sym_march<T, S, EPI_APPLY>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
+  else if (epi == EPI_SMOOTH) launch_k(k_sym_march<T, S, EPI_SMOOTH>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
+  else launch_k(k_sym_march<T, S, EPI_RESID>, grid, block, 0, st, g, a, stc, sqrtd, zchunk);
 }
 template void launch_stencil_sym_op<float, __half>(const Grid&, int, const OpArgs&, const __half*, const float*, int, cudaStream_t);
 template void launch_stencil_sym_op<float, float>(const Grid&, int, const OpArgs&, const float*, const float*, int, cudaStream_t);

@@ -17,7 +17,6 @@ namespace {
 __global__ void __launch_bounds__(256) k_restrict_d(Grid f, const double* __restrict__ rf, Grid c,
                                                     const uint8_t* __restrict__ cm, double* __restrict__ rc,
                                                     const KrylovState* ks) {
-  pdl_enter();
   if (ks && ks->done) return;
   const int nx1 = c.lx + 1, ny1 = c.ly + 1, nint = nx1 * ny1 * (c.lz + 1);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
@@ -44,7 +43,6 @@ __global__ void __launch_bounds__(256) k_restrict_d(Grid f, const double* __rest
 __global__ void __launch_bounds__(256) k_restrict_f(Grid f, const float* __restrict__ rf, Grid c,
                                                     const uint8_t* __restrict__ cm, float* __restrict__ rc,
                                                     const KrylovState* ks) {
-  pdl_enter();
   if (ks && ks->done) return;
   const int nx1 = c.lx + 1, ny1 = c.ly + 1, nint = nx1 * ny1 * (c.lz + 1);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
@@ -138,7 +136,6 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_prolong_add4(Grid c, const T* __restrict__ ec, Grid f,
                                                       const uint8_t* __restrict__ fm, T* __restrict__ uf,
                                                       const KrylovState* ks) {
-  pdl_enter();
   if (ks && ks->done) return;
   const int gpr = f.px / 4;                        // 4-node groups per storage row
   const long long ngroups = (long long)gpr * (f.ly + 1) * (f.lz + 1);
@@ -185,7 +182,6 @@ template <typename T>
 __global__ void k_jacobi_from_zero(Grid g, const T* __restrict__ b, const T* __restrict__ minv,
                                    const uint8_t* __restrict__ mask, T w0, const double* __restrict__ wdev,
                                    T* __restrict__ u, const KrylovState* ks) {
-  pdl_enter();
   if (ks && ks->done) return;
   const T w = wdev ? (T)(*wdev) : w0;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
@@ -208,25 +204,25 @@ inline int blocks_for(long long n) {
 template <>
 void launch_restrict<double>(const Grid& f, const double* rf, const Grid& c, const uint8_t* cmask, double* rc,
                              const KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_restrict_d, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c, cmask, rc, ks);
+  launch_k(k_restrict_d, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c, cmask, rc, ks);
 }
 template <>
 void launch_restrict<float>(const Grid& f, const float* rf, const Grid& c, const uint8_t* cmask, float* rc,
                             const KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_restrict_f, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c, cmask, rc, ks);
+  launch_k(k_restrict_f, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c, cmask, rc, ks);
 }
 
 template <typename T>
 void launch_prolong_add(const Grid& c, const T* ec, const Grid& f, const uint8_t* fmask, T* uf,
                         const KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_prolong_add4<T>, blocks_for((long long)(f.px / 4) * (f.ly + 1) * (f.lz + 1)), 256, 0, st, c, ec, f, fmask,
+  launch_k(k_prolong_add4<T>, blocks_for((long long)(f.px / 4) * (f.ly + 1) * (f.lz + 1)), 256, 0, st, c, ec, f, fmask,
            uf, ks);
 }
 
 template <typename T>
 void launch_jacobi_from_zero(const Grid& g, const T* b, const T* minv3, const uint8_t* mask, double omega,
                              const double* omega_dev, T* u, const KrylovState* ks, cudaStream_t st) {
-  launch_pdl(k_jacobi_from_zero<T>, blocks_for(g.n), 256, 0, st, g, b, minv3, mask, (T)omega, omega_dev, u, ks);
+  launch_k(k_jacobi_from_zero<T>, blocks_for(g.n), 256, 0, st, g, b, minv3, mask, (T)omega, omega_dev, u, ks);
 }
 
 template void launch_prolong_add<double>(const Grid&, const double*, const Grid&, const uint8_t*, double*, const KrylovState*, cudaStream_t);
