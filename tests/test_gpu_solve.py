@@ -217,3 +217,19 @@ def test_dense_coarsest_is_exact_inverse(gpu, dims):
     free[fixed] = False
     r = f * free - hex8.element_apply(u, E, hex8.build_edof(nx, ny, nz), hex8.hex8_ke(1.0, 0.3), ndof) * free
     assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(f)
+
+
+def test_solve_into_out_buffer(gpu):
+    """``out=``: the displacement lands in the caller's array (returned as
+    is), bitwise the same as a solve that allocates; bad buffers are refused."""
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    p = _cantilever()
+    m = MGSolver(*p["dims"], p["fixed_dofs"], nu=p["nu"], options=SolverOptions.fast())
+    u0 = m.solve(p["E_stiff"], p["f"], tol=1e-10)
+    buf = np.full(m.ndof, np.nan)
+    u1 = m.solve(p["E_stiff"], p["f"], tol=1e-10, out=buf)
+    assert u1 is buf
+    np.testing.assert_array_equal(u1, u0)
+    with pytest.raises(ValueError):
+        m.solve(p["E_stiff"], p["f"], tol=1e-10, out=np.empty(m.ndof, dtype=np.float32))
+    m.close()

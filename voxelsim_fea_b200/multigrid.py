@@ -280,10 +280,13 @@ class MGSolver:
         return out
 
     # -- public solve ------------------------------------------------------------
-    def solve(self, Evec_full, f, tol=1e-4, max_cg=None, x0=None, progress_cb=None, nu_elem=None):
+    def solve(self, Evec_full, f, tol=1e-4, max_cg=None, x0=None, progress_cb=None, nu_elem=None, out=None):
         """PCG with the V-cycle preconditioner; returns a fresh numpy u
         (core/multigrid.py:439-583).  ``progress_cb(it, resid_ratio, tol)`` is
-        called once per iteration, in order (bursts at graph-chunk ends)."""
+        called once per iteration, in order (bursts at graph-chunk ends).
+        ``out`` (B200 extension): a C-contiguous float64 array of ndof values
+        that receives u and is returned (e.g. page-locked host memory, which
+        the device writes at full PCIe / C2C speed)."""
         self.resid_history = []
         t0 = time.perf_counter()
         self.set_density(Evec_full, nu_elem=nu_elem)
@@ -291,7 +294,13 @@ class MGSolver:
         if f.size != self.ndof:
             raise ValueError(f"f has {f.size} entries, expected {self.ndof}")
         x0a = None if x0 is None else _lib.f64(np.asarray(x0, dtype=float).ravel())
-        u = np.empty(self.ndof)
+        if out is not None:
+            if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.size != self.ndof
+                    or not out.flags.c_contiguous):
+                raise ValueError(f"out must be a C-contiguous float64 array of {self.ndof} values")
+            u = out.reshape(-1)
+        else:
+            u = np.empty(self.ndof)
         info = _lib.VfSolveInfo()
         cb_error = []
 
@@ -311,7 +320,8 @@ class MGSolver:
         if rc not in (_lib.VF_OK, _lib.VF_ERR_STALLED):
             _lib.check(rc, self._h, "solve")
         if info.iters < 0:
-            return np.zeros(self.ndof)   # zero load (multigrid.py:471-473)
+            u[:] = 0.0                   # zero load (multigrid.py:471-473)
+            return u
         n = ctypes.c_int32()
         L.vf_resid_history(self._h, None, 0, ctypes.byref(n))
         hist = np.empty(n.value)
