@@ -95,7 +95,8 @@ struct KrylovState {
   int stall_guard;
   int restart;      // beta := 0 (rz == 0, multigrid.py:534-545)
   int it_trigger;   // > 0: stop the chunk (KS_RELIABLE) once it reaches it
-  unsigned int counter[12];  // last-block-done counters of the reductions
+  int x_it;         // split-precision PCG: iterations whose alpha p is already in x
+  unsigned int counter[12];  // last-block-done counters (reductions; [11]: x_it)
 };
 
 enum KState { KS_RUNNING = 0, KS_CONVERGED = 1, KS_MAXIT = 2, KS_STALLED = 3,
@@ -202,9 +203,9 @@ void launch_norm2_f64(const Grid& g, const double* v, double* partials, KrylovSt
 void launch_ir_prepare(const Grid& g, const double* r64, float* r32, KrylovState* ks, cudaStream_t st);
 void launch_ir_accumulate(const Grid& g, double* x64, const float* d32, const KrylovState* ks, cudaStream_t st);
 void launch_ir_replace(const Grid& g, const double* r64, float* r32, const KrylovState* ks, cudaStream_t st);
-void launch_cg_update_split(const Grid& g, double* x, const double* p, double* r, const double* Ap, float* r32,
-                            double* partials, KrylovState* ks, double* hist, cudaStream_t st);
-void launch_p_update_split(const Grid& g, double* p, const float* z, KrylovState* ks, cudaStream_t st);
+void launch_cg_update_split(const Grid& g, double* r, const double* Ap, float* r32, double* partials,
+                            KrylovState* ks, double* hist, cudaStream_t st);
+void launch_p_update_split(const Grid& g, double* x, double* p, const float* z, KrylovState* ks, cudaStream_t st);
 void launch_dot_fcg_split(const Grid& g, const float* r, const float* z, const double* Ap, double* partials,
                           KrylovState* ks, cudaStream_t st);
 void launch_scale64(const Grid& g, const double* x, double* y, double sc, cudaStream_t st);

@@ -107,31 +107,25 @@ __global__ void __launch_bounds__(kVecThreads) k_p_update(long long n3, T* __res
 // FP64 outer PCG around an FP32 preconditioner: the FP64 recurrences of x,
 // r, p keep the Krylov space of the FP64 solve; the V-cycle reads an FP32
 // copy of r (written by the update pass) and returns z in FP32, which the
-// direction update widens.  Four values per thread step (n3 is a multiple of
-// 12): two double2 and one float4 access per vector.
-__global__ void __launch_bounds__(kVecThreads) k_cg_update_split(long long n3, double* __restrict__ x,
-                                                                 const double* __restrict__ p, double* __restrict__ r,
+// direction update widens.  x += alpha p is deferred to the direction update
+// (which reads p anyway), so p is read once per iteration, not twice.  Four
+// values per thread step (n3 is a multiple of 12): two double2 and one
+// float4 access per vector.
+__global__ void __launch_bounds__(kVecThreads) k_cg_update_split(long long n3, double* __restrict__ r,
                                                                  const double* __restrict__ Ap, float* __restrict__ r32,
                                                                  double* partials, KrylovState* ks, double* hist) {
   if (ks->done) return;
   const double alpha = ks->alpha;
   const long long n4 = n3 / 4;
-  double2* xv = reinterpret_cast<double2*>(x);
   double2* rv = reinterpret_cast<double2*>(r);
-  const double2* pv = reinterpret_cast<const double2*>(p);
   const double2* av = reinterpret_cast<const double2*>(Ap);
   float4* r4 = reinterpret_cast<float4*>(r32);
   double s = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
-    const double2 p0 = __ldg(pv + 2 * i), p1 = __ldg(pv + 2 * i + 1);
     const double2 a0 = __ldg(av + 2 * i), a1 = __ldg(av + 2 * i + 1);
-    double2 x0 = xv[2 * i], x1 = xv[2 * i + 1];
     double2 q0 = rv[2 * i], q1 = rv[2 * i + 1];
-    x0.x = fma(alpha, p0.x, x0.x); x0.y = fma(alpha, p0.y, x0.y);
-    x1.x = fma(alpha, p1.x, x1.x); x1.y = fma(alpha, p1.y, x1.y);
     q0.x = fma(-alpha, a0.x, q0.x); q0.y = fma(-alpha, a0.y, q0.y);
     q1.x = fma(-alpha, a1.x, q1.x); q1.y = fma(-alpha, a1.y, q1.y);
-    xv[2 * i] = x0; xv[2 * i + 1] = x1;
     rv[2 * i] = q0; rv[2 * i + 1] = q1;
     r4[i] = make_float4((float)q0.x, (float)q0.y, (float)q1.x, (float)q1.y);
     s += q0.x * q0.x + q0.y * q0.y + q1.x * q1.x + q1.y * q1.y;
@@ -139,21 +133,50 @@ __global__ void __launch_bounds__(kVecThreads) k_cg_update_split(long long n3, d
   reduce_and_finalize(s, partials, ks, SLOT_RR, hist);
 }
 
-// p = z + beta p (p FP64, z FP32)
-__global__ void __launch_bounds__(kVecThreads) k_p_update_split(long long n3, double* __restrict__ p,
-                                                                const float* __restrict__ z, const KrylovState* ks) {
-  if (ks->done) return;
+// x += alpha p (the iteration's deferred solution update), then p = z + beta p
+// (p FP64, z FP32).  The x update runs once per completed iteration -- also
+// the one whose residual test ended the solve, when p stays -- tracked by
+// ks->x_it, which the last CTA advances.
+__global__ void __launch_bounds__(kVecThreads) k_p_update_split(long long n3, double* __restrict__ x,
+                                                                double* __restrict__ p, const float* __restrict__ z,
+                                                                KrylovState* ks) {
+  const int it = ks->it;
+  const bool do_x = it > ks->x_it;
+  const bool do_p = !ks->done;
+  if (!do_x && !do_p) return;
+  const double alpha = do_x ? ks->alpha : 0.0;
   const bool restart = ks->restart != 0;
   const double beta = restart ? 0.0 : ks->beta;
   const long long n4 = n3 / 4;
+  double2* xv = reinterpret_cast<double2*>(x);
   double2* pv = reinterpret_cast<double2*>(p);
   const float4* zv = reinterpret_cast<const float4*>(z);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
-    const float4 zz = __ldg(zv + i);
     double2 p0 = pv[2 * i], p1 = pv[2 * i + 1];
-    p0.x = fma(beta, p0.x, (double)zz.x); p0.y = fma(beta, p0.y, (double)zz.y);
-    p1.x = fma(beta, p1.x, (double)zz.z); p1.y = fma(beta, p1.y, (double)zz.w);
-    pv[2 * i] = p0; pv[2 * i + 1] = p1;
+    if (do_x) {
+      double2 x0 = xv[2 * i], x1 = xv[2 * i + 1];
+      x0.x = fma(alpha, p0.x, x0.x); x0.y = fma(alpha, p0.y, x0.y);
+      x1.x = fma(alpha, p1.x, x1.x); x1.y = fma(alpha, p1.y, x1.y);
+      xv[2 * i] = x0; xv[2 * i + 1] = x1;
+    }
+    if (do_p) {
+      const float4 zz = __ldg(zv + i);
+      p0.x = fma(beta, p0.x, (double)zz.x); p0.y = fma(beta, p0.y, (double)zz.y);
+      p1.x = fma(beta, p1.x, (double)zz.z); p1.y = fma(beta, p1.y, (double)zz.w);
+      pv[2 * i] = p0; pv[2 * i + 1] = p1;
+    }
+  }
+  if (do_x) {   // last CTA: this iteration's alpha p is in x
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(&ks->counter[11], 1u);
+      if (prev == gridDim.x - 1) {
+        ks->x_it = it;
+        ks->counter[11] = 0u;
+        __threadfence();
+      }
+    }
   }
 }
 
@@ -375,12 +398,12 @@ void launch_sub_from(const Grid& g, const double* f, double* r, cudaStream_t st)
   launch_k(k_sub_from, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, f, r);
 }
 
-void launch_cg_update_split(const Grid& g, double* x, const double* p, double* r, const double* Ap, float* r32,
-                            double* partials, KrylovState* ks, double* hist, cudaStream_t st) {
-  launch_k(k_cg_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, p, r, Ap, r32, partials, ks, hist);
+void launch_cg_update_split(const Grid& g, double* r, const double* Ap, float* r32, double* partials,
+                            KrylovState* ks, double* hist, cudaStream_t st) {
+  launch_k(k_cg_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, r, Ap, r32, partials, ks, hist);
 }
-void launch_p_update_split(const Grid& g, double* p, const float* z, KrylovState* ks, cudaStream_t st) {
-  launch_k(k_p_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, p, z, (const KrylovState*)ks);
+void launch_p_update_split(const Grid& g, double* x, double* p, const float* z, KrylovState* ks, cudaStream_t st) {
+  launch_k(k_p_update_split, kVecBlocks, kVecThreads, 0, st, 3LL * g.n, x, p, z, ks);
 }
 void launch_dot_fcg_split(const Grid& g, const float* r, const float* z, const double* Ap, double* partials,
                           KrylovState* ks, cudaStream_t st) {

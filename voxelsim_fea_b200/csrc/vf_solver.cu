@@ -425,11 +425,11 @@ void pcg_iteration_outer64(vf_solver* s) {
   float *r32 = s->k32[1], *z32 = s->k32[2];
   const Grid& g = s->L[0].g;
   level_op<double>(s, 0, EPI_APPLY, p, Ap, nullptr, s->ks, s->d_partials, SLOT_PAP);
-  launch_cg_update_split(g, x, p, r, Ap, r32, s->d_partials, s->ks, s->d_hist, s->st);
+  launch_cg_update_split(g, r, Ap, r32, s->d_partials, s->ks, s->d_hist, s->st);
   precondition<float>(s, r32, z32, s->ks, fused_rz(s) ? SLOT_RZ : -1);
   if (flexible(s)) launch_dot_fcg_split(g, r32, z32, Ap, s->d_partials, s->ks, s->st);
   else if (!fused_rz(s)) launch_dot<float>(g, r32, z32, s->d_partials, s->ks, SLOT_RZ, s->st);
-  launch_p_update_split(g, p, z32, s->ks, s->st);
+  launch_p_update_split(g, x, p, z32, s->ks, s->st);
 }
 
 int graph_slot(const vf_solver* s, bool fp32) { return use_mg(s) ? (fp32 ? 1 : 0) : 2; }
