@@ -298,7 +298,7 @@ class MGSolver:
             if (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.size != self.ndof
                     or not out.flags.c_contiguous):
                 raise ValueError(f"out must be a C-contiguous float64 array of {self.ndof} values")
-            u = out.reshape(-1)
+            u = out if out.ndim == 1 else out.reshape(-1)   # a view of out either way
         else:
             u = np.empty(self.ndof)
         info = _lib.VfSolveInfo()
