@@ -34,6 +34,7 @@ def test_abi_and_options(lib):
     assert o.struct_size == ctypes.sizeof(_lib.VfOptions)
     assert (o.n_smooth, o.min_elems, o.max_levels, o.coarse_sweeps) == (2, 4, 6, 30)
     assert abs(o.omega - 0.6) < 1e-15
+    assert o.mixed_mode == _lib.MIXED_MODES["outer64"] and o.modal_zchunk == 0 and o.autotune == 1
     assert lib.vf_status_string(_lib.VF_ERR_STALLED) == b"MG-PCG stalled/diverged"
 
 
@@ -64,6 +65,12 @@ def test_create_rejects_bad_args(lib):
     o = _lib.default_options()
     o.struct_size = 3
     assert lib.vf_create(4, 4, 4, 0.3, ctypes.byref(o), ctypes.byref(h)) == _lib.VF_ERR_ARG
+    # option fields outside their enums are refused before any device call
+    for field, bad in (("mixed_mode", 3), ("mixed_mode", -1), ("modal_zchunk", -2), ("fine_kernel", 3),
+                       ("coarse_storage", 3), ("precision", 3)):
+        o = _lib.default_options()
+        setattr(o, field, bad)
+        assert lib.vf_create(4, 4, 4, 0.3, ctypes.byref(o), ctypes.byref(h)) == _lib.VF_ERR_ARG, field
     assert not h.value
 
 
