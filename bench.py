@@ -157,6 +157,32 @@ def cpu_sample_solve():
     return dt, 3 * (nx + 1) * (ny + 1) * (nz + 1), v.last_iters
 
 
+def cpu_matvec_full(dims, E, nu, u=None):
+    """One full-size element-by-element K u on the host cores with the oracle's
+    restatement of the reference's gather / GEMM / bincount apply
+    (core/multigrid.py:318-341), in x-slabs of elements to bound host memory;
+    returns (seconds, dof, K u)."""
+    from oracle import hex8
+    nx, ny, nz = dims
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    KE = hex8.hex8_ke(1.0, nu)
+    if u is None:
+        u = np.random.default_rng(1).standard_normal(ndof)
+    Ee = np.asarray(E, dtype=float).reshape(nx, ny, nz)
+    slab = max(1, (1 << 19) // (ny * nz))
+    t0 = time.perf_counter()
+    y = np.zeros(ndof)
+    for x0 in range(0, nx, slab):
+        x1 = min(nx, x0 + slab)
+        ex, ey, ez = np.meshgrid(np.arange(x0, x1), np.arange(ny), np.arange(nz), indexing="ij")
+        edof = np.empty((ex.size, 24), dtype=np.int64)
+        for k, (ox, oy, oz) in enumerate(hex8.CORNERS):
+            nid = hex8.node_id(ex.ravel() + ox, ey.ravel() + oy, ez.ravel() + oz, nx, ny)
+            edof[:, 3 * k:3 * k + 3] = 3 * nid[:, None] + np.arange(3)
+        y += hex8.element_apply(u, Ee[x0:x1].ravel(), edof, KE, ndof)
+    return time.perf_counter() - t0, ndof, y
+
+
 def cpu_cores():
     try:
         import threadpoolctl
@@ -168,9 +194,15 @@ def cpu_cores():
     return os.cpu_count() or 1
 
 
-def cpu_baseline_record():
+def cpu_baseline_record(full=None):
     dt, dof, it = cpu_sample_solve()
-    return {"value": dof / dt / 1e6, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
+    mv = None
+    if full is not None:
+        mt, mdof, _ = cpu_matvec_full(*full)
+        mv = {"seconds_per_apply": mt, "mdof_per_s": mdof / mt / 1e6, "dof": mdof,
+              "what": "one full-size FP64 element-by-element K u (gather, 24x24 GEMM, bincount scatter) of "
+                      "the bench workload, numpy restatement of the reference's apply, host cores"}
+    return {"value": dof / dt / 1e6, "unit": UNIT, "cores": cpu_cores(), "kind": "port", "matvec_full_size": mv,
             "sample": (f"numpy restatement of the reference's Jacobi-PCG (core/fea.py:497-593) to {TOL:g} "
                        f"on the seeded bracket generator at {CPU_SAMPLE['shape'][0]}x{CPU_SAMPLE['shape'][1]}x"
                        f"{CPU_SAMPLE['shape'][2]} ({dof} DOF, {it} iterations, {dt:.1f} s); the reference's "
@@ -466,7 +498,7 @@ def run_b200(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_record()
+        cpu = cpu_baseline_record(full=((nx, ny, nz), E_mg, nu_scalar))
 
     if rank == 0:
         line = {

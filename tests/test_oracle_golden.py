@@ -108,3 +108,23 @@ def test_voxelize_oracle_matches_reference():
         v, f = g[f"{name}_verts"], g[f"{name}_faces"]
         for key, pts in (("points", g[f"{name}_points"]), ("centers", g["centers"]), ("nodes", g["nodes"])):
             np.testing.assert_array_equal(voxelize.inside_mask(v, f, pts), g[f"{name}_in_{key}"], err_msg=f"{name}/{key}")
+
+
+def test_bench_cpu_matvec_slabs_match_oracle_apply():
+    """The CPU baseline's full-size K u (bench.py, x-slabs of elements) is the
+    oracle's element apply, on a grid that takes several slabs."""
+    import importlib.util
+    import os
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(os.path.dirname(__file__), "..", "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    from oracle import hex8
+    nx, ny, nz = 40, 30, 500
+    rng = np.random.default_rng(0)
+    E = rng.random(nx * ny * nz)
+    ndof = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    u = rng.standard_normal(ndof)
+    _, dof, y = bench.cpu_matvec_full((nx, ny, nz), E, 0.3, u=u)
+    yr = hex8.element_apply(u, E, hex8.build_edof(nx, ny, nz), hex8.hex8_ke(1.0, 0.3), ndof)
+    assert dof == ndof
+    assert np.abs(y - yr).max() <= 1e-14 * np.abs(yr).max()
