@@ -15,8 +15,11 @@ rediscretized coarse levels, injected Dirichlet masks, 30-sweep Jacobi coarse
 * ``coarse="galerkin"``  R A P coarse operators (robust on void/solid noise
   geometry, where the rediscretized hierarchy stops converging);
 * ``coarsest="cholesky"`` FP64 dense direct solve on the coarsest level;
-* ``precision="mixed"`` FP32 PCG + V-cycle inside FP64 iterative refinement
-  (FP64 dots, outer residual and coarsest solve); ``"fp32"`` without refinement.
+* ``precision="mixed"`` the FP32 V-cycle (matvec, smoother, transfers) inside
+  FP64 PCG (``mixed_mode="outer64"``, default: FP64 dots, A p, vector updates
+  and coarsest solve), or FP32 CG with FP64 residual replacement
+  (``"reliable"``) or iterative refinement (``"restart"``); ``"fp32"``: FP32
+  PCG without refinement.
 """
 
 import ctypes
