@@ -189,7 +189,7 @@ def eval_configs():
 
 
 def headline_configs():
-    """The comparison BASELINE names: plain FP64 GMG-PCG, mixed, learned + mixed."""
+    """The headline comparison: plain FP64 GMG-PCG, mixed, learned + mixed."""
     from ..multigrid import SolverOptions
     return (("plain_fp64", SolverOptions.robust(), False),
             ("mixed", SolverOptions.fast(), False),
