@@ -1,0 +1,65 @@
+"""Index arithmetic of the modal TMA kernel's work split, restated on the host
+(voxelsim_fea_b200/csrc/vf_modal_tma.cu: the (tile, plane) unit ranges of
+the per-chunk grid and of the one-wave split, the segments a range crosses,
+and the two z-lanes of a segment): every output plane of every tile is
+written by exactly one (CTA, lane, step), for grids with partial tiles,
+ranges that cross tile boundaries, and more CTAs than units."""
+
+import itertools
+
+import pytest
+
+TX, TY, L = 32, 8, 2   # CTA tile (threads) and z-lanes of the FP32 kernel
+
+
+def _ranges(lx, ly, lz, zchunk, nb_wave):
+    ntx, nty = (lx + TX - 1) // (TX - 1), (ly + TY - 1) // (TY - 1)
+    NP = lz + 1
+    U = ntx * nty * NP
+    if zchunk > 0:
+        ntile = ntx * nty
+        nb = ntile * ((NP + zchunk - 1) // zchunk)
+        for b in range(nb):
+            tile, ch = b % ntile, b // ntile
+            yield tile * NP + ch * zchunk, tile * NP + min((ch + 1) * zchunk, NP)
+    else:
+        nb = min(nb_wave, U)
+        for b in range(nb):
+            yield U * b // nb, U * (b + 1) // nb
+
+
+def _outputs(lx, ly, lz, zchunk, nb_wave=296):
+    NP = lz + 1
+    seen = {}
+    for ub, ue in _ranges(lx, ly, lz, zchunk, nb_wave):
+        assert ub < ue
+        u0 = ub
+        while u0 < ue:
+            tile = u0 // NP
+            zb = u0 - tile * NP
+            ze = min(NP, zb + (ue - u0))
+            u0 = tile * NP + ze
+            H = (ze - zb + L - 1) // L
+            for lane in range(L):
+                z0 = zb + lane * H - 1
+                oend = min(zb + lane * H + H, ze, lz + 1)
+                for s in range(H + 2):
+                    zs = z0 + s - 1
+                    if s >= 2 and zs < oend:
+                        key = (tile, zs)
+                        seen[key] = seen.get(key, 0) + 1
+    return seen
+
+
+@pytest.mark.parametrize("dims,zchunk,nb", [
+    ((256, 128, 128), 22, 296), ((256, 128, 128), -1, 296), ((256, 128, 128), -1, 148),
+    ((37, 23, 19), -1, 296), ((37, 23, 19), 5, 296), ((64, 48, 40), -1, 296),
+    ((120, 60, 50), -1, 296), ((200, 13, 3), -1, 296), ((5, 3, 1), -1, 296), ((31, 7, 0), -1, 4),
+])
+def test_every_output_plane_written_once(dims, zchunk, nb):
+    lx, ly, lz = dims
+    seen = _outputs(lx, ly, lz, zchunk, nb)
+    ntx, nty = (lx + TX - 1) // (TX - 1), (ly + TY - 1) // (TY - 1)
+    expect = set(itertools.product(range(ntx * nty), range(lz + 1)))
+    assert set(seen) == expect
+    assert all(v == 1 for v in seen.values())
