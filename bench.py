@@ -320,7 +320,8 @@ def run_b200(args):
         return MGSolver(nx, ny, nz, p["fixed_dofs"], nu=nu_scalar, max_levels=w["levels"], options=opts,
                         n_smooth=args.n_smooth)
 
-    fkw = dict(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk, mixed_mode=args.mixed_mode)
+    fkw = dict(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk, mixed_mode=args.mixed_mode,
+               smoother=args.smoother)
     if args.inner_tol is not None:
         fkw["inner_tol"] = args.inner_tol
     fast = solver(SolverOptions.fast(**fkw))
@@ -413,7 +414,7 @@ def run_b200(args):
     # plain FP64 GMG-PCG (same hierarchy, FP64 everywhere) on the same GPU
     plain = None
     if not args.no_plain:
-        ps = solver(SolverOptions.robust(device=local, check_every=args.check_every))
+        ps = solver(SolverOptions.robust(device=local, check_every=args.check_every, smoother=args.smoother))
         L.vf_get_stream(ps._h, ctypes.byref(stream_ptr))
         ext_plain = torch.cuda.ExternalStream(stream_ptr.value)
         ext_save = ext
@@ -556,6 +557,8 @@ def main():
     ap.add_argument("--modal-zchunk", type=int, default=0, help="z-planes per CTA of the modal kernel (0 = auto)")
     ap.add_argument("--kernel-iters", type=int, default=3, help="launches timed by --kernel-profile")
     ap.add_argument("--mixed-mode", choices=("outer64", "reliable", "restart"), default="outer64")
+    ap.add_argument("--smoother", choices=("jacobi", "chebyshev"), default="jacobi",
+                    help="V-cycle smoothing of every arm (plain FP64, mixed, learned)")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed: residual reduction between FP64 corrections (solver default if unset)")
     args = ap.parse_args()

@@ -116,7 +116,13 @@ typedef struct vf_options {
   int32_t autotune;        /* 1 (default): at the first vf_set_material, time candidate
                               z-chunk sizes of the marching kernels on every level and keep
                               the fastest (cached per grid shape for the process) */
-  int32_t reserved[5];
+  int32_t smoother;        /* VF_SMOOTH_JACOBI (default): damped Jacobi sweeps;
+                              VF_SMOOTH_CHEBYSHEV: Chebyshev polynomial smoothing of the same
+                              degree (n_smooth <= 2 sweeps) on [lambda / cheb_ratio, lambda],
+                              lambda the VF_OMEGA_AUTO estimate of lambda_max(D^-1 A_l); needs
+                              VF_OMEGA_AUTO, a modal fine kernel and symmetric coarse storage */
+  int32_t cheb_ratio;      /* VF_SMOOTH_CHEBYSHEV: lambda_max / lower end of the interval (30) */
+  int32_t reserved[3];
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
@@ -125,6 +131,7 @@ enum { VF_FINE_MODAL = 0,     /* modal z-marching kernel, TMA-staged (vf_modal_t
        VF_FINE_MODAL_CPASYNC = 2 };  /* modal z-marching kernel, cp.async-staged (vf_modal.cu) */
 enum { VF_STENCIL_SYM_HALF = 0, VF_STENCIL_SYM = 1, VF_STENCIL_FULL = 2 };
 enum { VF_MIXED_RELIABLE = 0, VF_MIXED_RESTART = 1, VF_MIXED_OUTER64 = 2 };
+enum { VF_SMOOTH_JACOBI = 0, VF_SMOOTH_CHEBYSHEV = 1 };
 
 typedef struct vf_solve_info {
   int32_t iters;           /* PCG iterations (all inner iterations for MIXED);

@@ -35,6 +35,7 @@ def test_abi_and_options(lib):
     assert (o.n_smooth, o.min_elems, o.max_levels, o.coarse_sweeps) == (2, 4, 6, 30)
     assert abs(o.omega - 0.6) < 1e-15
     assert o.mixed_mode == _lib.MIXED_MODES["outer64"] and o.modal_zchunk == 0 and o.autotune == 1
+    assert o.smoother == _lib.SMOOTHERS["jacobi"] and o.cheb_ratio == 30
     assert lib.vf_status_string(_lib.VF_ERR_STALLED) == b"MG-PCG stalled/diverged"
 
 
@@ -71,6 +72,14 @@ def test_create_rejects_bad_args(lib):
         o = _lib.default_options()
         setattr(o, field, bad)
         assert lib.vf_create(4, 4, 4, 0.3, ctypes.byref(o), ctypes.byref(h)) == _lib.VF_ERR_ARG, field
+    # Chebyshev smoothing needs the lambda estimates, at most 2 sweeps and kernels that take its step
+    for fields in ({}, {"omega_mode": 1, "n_smooth": 3}, {"omega_mode": 1, "fine_kernel": 1},
+                   {"omega_mode": 1, "coarse_storage": 2}, {"omega_mode": 1, "cheb_ratio": 1}):
+        o = _lib.default_options()
+        o.smoother = _lib.SMOOTHERS["chebyshev"]
+        for k, v in fields.items():
+            setattr(o, k, v)
+        assert lib.vf_create(4, 4, 4, 0.3, ctypes.byref(o), ctypes.byref(h)) == _lib.VF_ERR_ARG, fields
     assert not h.value
 
 

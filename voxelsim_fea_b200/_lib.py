@@ -33,6 +33,7 @@ VF_OMEGA_FIXED, VF_OMEGA_AUTO = 0, 1
 VF_FINE_MODAL, VF_FINE_GATHER, VF_FINE_MODAL_CPASYNC = 0, 1, 2
 STENCIL_STORAGE = {"sym_half": 0, "sym": 1, "full": 2}
 MIXED_MODES = {"reliable": 0, "restart": 1, "outer64": 2}
+SMOOTHERS = {"jacobi": 0, "chebyshev": 1}
 
 PRECISIONS = {"fp64": VF_PREC_FP64, "mixed": VF_PREC_MIXED, "fp32": VF_PREC_FP32}
 COARSE_OPS = {"rediscretize": VF_COARSE_REDISCRETIZE, "galerkin": VF_COARSE_GALERKIN}
@@ -69,7 +70,7 @@ class VfOptions(ctypes.Structure):
         ("fine_kernel", ctypes.c_int32), ("modal_zchunk", ctypes.c_int32),
         ("coarse_storage", ctypes.c_int32), ("mixed_mode", ctypes.c_int32),
         ("flexible", ctypes.c_int32), ("autotune", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 5),
+        ("smoother", ctypes.c_int32), ("cheb_ratio", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3),
     ]
 
 

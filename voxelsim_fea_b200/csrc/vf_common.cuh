@@ -137,6 +137,11 @@ struct OpArgs {
   const double* ke_tab;   // HOST pointer: [KE(nu) | K_lam | K_mu], 3 x 576 doubles
   const double* omega_dev;  // device: damping of this level (overrides omega when set)
   int* err;                 // device error flag (bounded waits that expired), or nullptr
+  // SMOOTH as a Chebyshev step: out = u + w Minv (b - A u) + c1 dprev, and
+  // dout = out - u (the step's update, the next step's dprev); unused if null
+  const void* dprev;
+  void* dout;
+  const double* c1_dev;
 };
 template <typename T> void launch_fine_op(const Grid& g, int epi, const OpArgs& a, cudaStream_t st);
 
@@ -219,6 +224,7 @@ template <typename T>
 void launch_power_scale(const Grid& g, T* y, const T* minv3, double* partials, KrylovState* ks, cudaStream_t st);
 template <typename T>
 void launch_power_normalize(const Grid& g, const T* y, T* x, const KrylovState* ks, cudaStream_t st);
+void launch_cheb_coefs(const double* lambda, int nl, int ratio, double* coef, cudaStream_t st);
 void launch_power_omega(const KrylovState* ks, double omega_rel, double safety, double* omega_out, double* lambda_out, cudaStream_t st);
 
 // vf_post.cu -- post-processing and the island pre-step

@@ -321,7 +321,35 @@ __global__ void k_power_omega(const KrylovState* ks, double omega_rel, double sa
   *omega_out = lam > 0.0 ? omega_rel * 2.0 / lam : omega_rel;
 }
 
+// Chebyshev smoothing steps per level (three-term recurrence on the interval
+// [beta / ratio, beta] of D^-1 A_l, beta = the padded lambda_max estimate):
+// step 0: x += (1/theta) Minv r; step k: d_k = c1 d_(k-1) + c2 Minv r,
+// x += d_k with rho_k = 1 / (2 sigma - rho_(k-1)), c1 = rho_k rho_(k-1),
+// c2 = 2 rho_k / delta.  coef[(l * 2 + k) * 2 + {0, 1}] = {c1, c2}.
+__global__ void k_cheb_coefs(const double* lambda, int nl, int ratio, double* coef) {
+  const int l = threadIdx.x;
+  if (l >= nl) return;
+  const double beta = lambda[l];
+  double* c = coef + 4 * l;
+  if (!(beta > 0.0)) {   // no free DOF on the level: leave it unchanged
+    c[0] = c[1] = c[2] = c[3] = 0.0;
+    return;
+  }
+  const double alpha = beta / ratio;
+  const double theta = 0.5 * (beta + alpha), delta = 0.5 * (beta - alpha), sigma = theta / delta;
+  const double rho0 = 1.0 / sigma;
+  const double rho1 = 1.0 / (2.0 * sigma - rho0);
+  c[0] = 0.0;
+  c[1] = 1.0 / theta;
+  c[2] = rho1 * rho0;
+  c[3] = 2.0 * rho1 / delta;
+}
+
 }  // namespace
+
+void launch_cheb_coefs(const double* lambda, int nl, int ratio, double* coef, cudaStream_t st) {
+  launch_k(k_cheb_coefs, 1, 32, 0, st, lambda, nl, ratio, coef);
+}
 
 template <typename T>
 void launch_power_init(const Grid& g, T* x, const uint8_t* mask, cudaStream_t st) {

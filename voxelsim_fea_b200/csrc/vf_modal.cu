@@ -91,6 +91,9 @@ __global__ void __launch_bounds__(TX * TY, 2) k_modal_op(Grid g, OpArgs a, Modal
   const T* __restrict__ MUv = (const T*)a.mu;
   const uint8_t* __restrict__ mask = a.mask;
   const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
+  const T* dprev = (const T*)a.dprev;
+  T* dout = (T*)a.dout;
+  const T c1 = a.c1_dev ? (T)(*a.c1_dev) : (T)0;
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TY - 1);
@@ -267,10 +270,12 @@ __global__ void __launch_bounds__(TX * TY, 2) k_modal_op(Grid g, OpArgs a, Modal
                 const T u2 = O::lane(Sp.u[2][ty][tx], l);
                 const T d0 = O::lane(Sp.d[0][dy][tx], l), d1 = O::lane(Sp.d[1][dy][tx], l);
                 const T d2 = O::lane(Sp.d[2][dy][tx], l);
-                const T o0 = u0 + ((m8 & 1) ? w * (d0 * (b0 - k0)) : (T)0);
-                const T o1 = u1 + ((m8 & 2) ? w * (d1 * (b1 - k1)) : (T)0);
-                const T o2 = u2 + ((m8 & 4) ? w * (d2 * (b2 - k2)) : (T)0);
+                T o0 = u0 + ((m8 & 1) ? w * (d0 * (b0 - k0)) : (T)0);
+                T o1 = u1 + ((m8 & 2) ? w * (d1 * (b1 - k1)) : (T)0);
+                T o2 = u2 + ((m8 & 4) ? w * (d2 * (b2 - k2)) : (T)0);
+                if (dprev) { o0 += c1 * dprev[p3]; o1 += c1 * dprev[p3 + 1]; o2 += c1 * dprev[p3 + 2]; }
                 out[p3] = o0; out[p3 + 1] = o1; out[p3 + 2] = o2;
+                if (dout) { dout[p3] = o0 - u0; dout[p3 + 1] = o1 - u1; dout[p3 + 2] = o2 - u2; }
                 if (a.dot_partials) dot += (double)b0 * (double)o0 + (double)b1 * (double)o1 + (double)b2 * (double)o2;
               } else {
                 out[p3] = b0 - k0; out[p3 + 1] = b1 - k1; out[p3 + 2] = b2 - k2;

@@ -121,6 +121,9 @@ __global__ void __launch_bounds__(TX * TY, 2)
   T* __restrict__ out = (T*)a.out;
   const uint8_t* __restrict__ mask = a.mask;
   const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
+  const T* dprev = (const T*)a.dprev;
+  T* dout = (T*)a.dout;
+  const T c1 = a.c1_dev ? (T)(*a.c1_dev) : (T)0;
 
   const int tx = threadIdx.x, ty = threadIdx.y;
   const bool leader = (tx == 0 && ty == 0);
@@ -279,10 +282,12 @@ __global__ void __launch_bounds__(TX * TY, 2)
                 const T u0 = uval(sp, l, 0, ty, tx), u1 = uval(sp, l, 1, ty, tx), u2 = uval(sp, l, 2, ty, tx);
                 const T d0 = bval(sp, l, Lay::offD, 0), d1 = bval(sp, l, Lay::offD, 1);
                 const T d2 = bval(sp, l, Lay::offD, 2);
-                const T o0 = u0 + ((m8 & 1) ? w * (d0 * (b0 - k0)) : (T)0);
-                const T o1 = u1 + ((m8 & 2) ? w * (d1 * (b1 - k1)) : (T)0);
-                const T o2 = u2 + ((m8 & 4) ? w * (d2 * (b2 - k2)) : (T)0);
+                T o0 = u0 + ((m8 & 1) ? w * (d0 * (b0 - k0)) : (T)0);
+                T o1 = u1 + ((m8 & 2) ? w * (d1 * (b1 - k1)) : (T)0);
+                T o2 = u2 + ((m8 & 4) ? w * (d2 * (b2 - k2)) : (T)0);
+                if (dprev) { o0 += c1 * dprev[p3]; o1 += c1 * dprev[p3 + 1]; o2 += c1 * dprev[p3 + 2]; }
                 out[p3] = o0; out[p3 + 1] = o1; out[p3 + 2] = o2;
+                if (dout) { dout[p3] = o0 - u0; dout[p3 + 1] = o1 - u1; dout[p3 + 2] = o2 - u2; }
                 if (a.dot_partials) dot += (double)b0 * (double)o0 + (double)b1 * (double)o1 + (double)b2 * (double)o2;
               } else {
                 out[p3] = b0 - k0; out[p3 + 1] = b1 - k1; out[p3 + 2] = b2 - k2;

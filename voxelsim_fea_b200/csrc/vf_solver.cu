@@ -163,6 +163,7 @@ struct vf_solver {
   int* d_err = nullptr;         // kernels' error flag (expired bounded waits)
   double* d_omega = nullptr;    // damping per level (read by the smoothers)
   double* d_lambda = nullptr;   // lambda_max(D^-1 A_l) estimates (VF_OMEGA_AUTO)
+  double* d_cheb = nullptr;     // Chebyshev steps per level: [level][step][c1, c2]
   std::vector<double> h_omega, h_lambda;
   // block right-hand sides: solvers that share this one's operator data and
   // own their vectors, Krylov state, stream and graphs (vf_solve_block)
@@ -243,9 +244,18 @@ template <> void level_sym_op<float>(vf_solver* s, Level& l, int epi, const OpAr
 
 int auto_zchunk(const Grid& g, int requested);
 
+// A sweep as a Chebyshev step (omega_dev: the step's Minv weight; c1_dev and
+// dprev: the previous step's update; dout: this step's update).
+struct SweepStep {
+  const double* omega_dev = nullptr;
+  const double* c1_dev = nullptr;
+  const void* dprev = nullptr;
+  void* dout = nullptr;
+};
+
 template <typename T>
 void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, KrylovState* ks, double* partials,
-              int slot) {
+              int slot, const SweepStep* step = nullptr) {
   Level& l = s->L[li];
   OpArgs a{};
   a.u = u; a.out = out; a.b = b;
@@ -254,7 +264,12 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
   a.mu = s->lame ? Sel<T>::mu(l) : nullptr;
   a.mask = l.mask;
   a.omega = s->o.omega;
-  a.omega_dev = s->d_omega + li;
+  a.omega_dev = (step && step->omega_dev) ? step->omega_dev : s->d_omega + li;
+  if (step) {
+    a.c1_dev = step->c1_dev;
+    a.dprev = step->dprev;
+    a.dout = step->dout;
+  }
   a.dot_partials = partials;
   a.ks = ks;
   a.dot_slot = slot;
@@ -270,6 +285,43 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
     if (s->o.fine_kernel == VF_FINE_MODAL_CPASYNC || !launch_modal_tma<T>(l.g, epi, a, mc, l.zchunk, s->st))
       launch_modal_op<T>(l.g, epi, a, mc, 8, l.zchunk > 0 ? l.zchunk : auto_zchunk(l.g, 0), s->st);
   }
+}
+
+// Chebyshev smoothing of degree `sweeps` (<= 2) on x (through tmp; dbuf
+// holds the first step's update when the second step needs it): step 0 is a
+// Jacobi sweep weighted 1/theta (from zero: x = Minv b / theta, whose update
+// is x itself), step 1 adds c1 times that update (k_cheb_coefs).
+template <typename T>
+void smooth_cheb(vf_solver* s, int li, T* x, T* tmp, T* dbuf, const T* b, int sweeps, bool from_zero,
+                 KrylovState* ks, int dot_slot) {
+  Level& l = s->L[li];
+  const double* c = s->d_cheb + 4 * li;
+  T* cur = x;
+  SweepStep s0, s1;
+  s0.omega_dev = c + 1;
+  s1.omega_dev = c + 3;
+  s1.c1_dev = c + 2;
+  if (from_zero) {
+    T* first = (sweeps % 2 == 1) ? x : tmp;
+    launch_jacobi_from_zero<T>(l.g, b, Sel<T>::minv(l), l.mask, 0.0, c + 1, first, ks, s->st);
+    cur = first;
+    s1.dprev = first;
+  } else {
+    T* nxt = tmp;
+    const bool last = sweeps == 1;
+    if (sweeps > 1) s0.dout = dbuf;
+    level_op<T>(s, li, EPI_SMOOTH, cur, nxt, b, ks, (last && dot_slot >= 0) ? s->d_partials : nullptr,
+                (last && dot_slot >= 0) ? dot_slot : 0, &s0);
+    cur = nxt;
+    s1.dprev = dbuf;
+  }
+  if (sweeps > 1) {
+    T* nxt = (cur == x) ? tmp : x;
+    level_op<T>(s, li, EPI_SMOOTH, cur, nxt, b, ks, dot_slot >= 0 ? s->d_partials : nullptr,
+                dot_slot >= 0 ? dot_slot : 0, &s1);
+    cur = nxt;
+  }
+  if (cur != x) launch_copy_vec<T>(l.g, cur, x, ks, s->st);
 }
 
 // `sweeps` damped-Jacobi sweeps on x (in place, through tmp); from_zero uses
@@ -325,12 +377,16 @@ void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks, int dot_slo
   Level& c = s->L[li + 1];
   T* tmp = Sel<T>::w(l, 1);
   T* res = Sel<T>::w(l, 2);
-  smooth<T>(s, li, x, tmp, b, s->o.n_smooth, true, ks);
+  const bool cheb = s->o.smoother == VF_SMOOTH_CHEBYSHEV && s->o.n_smooth > 0;
+  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, s->o.n_smooth, true, ks, -1);
+  else smooth<T>(s, li, x, tmp, b, s->o.n_smooth, true, ks);
   level_op<T>(s, li, EPI_RESID, x, res, b, ks, nullptr, 0);
   launch_restrict<T>(l.g, res, c.g, c.mask, Sel<T>::w(c, 3), ks, s->st);
   vcycle<T>(s, li + 1, Sel<T>::w(c, 3), Sel<T>::w(c, 0), ks);
   launch_prolong_add<T>(c.g, Sel<T>::w(c, 0), l.g, l.mask, x, ks, s->st);
-  smooth<T>(s, li, x, tmp, b, s->o.n_smooth, false, ks, dot_slot);
+  // (res is free again: the post-smoothing's first update goes there)
+  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, s->o.n_smooth, false, ks, dot_slot);
+  else smooth<T>(s, li, x, tmp, b, s->o.n_smooth, false, ks, dot_slot);
 }
 
 template <typename T> T** kvec(vf_solver* s);
@@ -624,6 +680,7 @@ int build_levels(vf_solver* s) {
   }
   VF_ALLOC(s->d_err, 1);
   VF_ALLOC(s->d_lambda, 16);
+  VF_ALLOC(s->d_cheb, 16 * 2 * 2);
   VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
   memset(s->h_ks, 0, sizeof(KrylovState));
   return ensure_hist(s, 4096);
@@ -802,6 +859,7 @@ int set_level_omegas(vf_solver* s) {
     }
     launch_power_omega(s->ks, s->o.omega_rel, 1.1, s->d_omega + li, s->d_lambda + li, s->st);
   }
+  if (s->o.smoother == VF_SMOOTH_CHEBYSHEV) launch_cheb_coefs(s->d_lambda, nl, s->o.cheb_ratio, s->d_cheb, s->st);
   VF_CHECK_LAUNCH();
   return VF_OK;   // h_omega / h_lambda are read back by fetch_level_omegas (a blocking copy)
 }
@@ -938,6 +996,8 @@ void vf_options_default(vf_options* o) {
   o->modal_zchunk = 0;
   o->coarse_storage = VF_STENCIL_SYM_HALF;
   o->mixed_mode = VF_MIXED_OUTER64;
+  o->smoother = VF_SMOOTH_JACOBI;
+  o->cheb_ratio = 30;
   o->autotune = 1;
 }
 
@@ -978,8 +1038,15 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
       o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0 ||
       o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0 ||
       o.fine_kernel < 0 || o.fine_kernel > 2 || o.modal_zchunk < -1 || o.coarse_storage < 0 ||
-      o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 2) {
+      o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 2 || o.smoother < 0 || o.smoother > 1) {
     g_last_error = "invalid vf_options field";
+    return VF_ERR_ARG;
+  }
+  if (o.smoother == VF_SMOOTH_CHEBYSHEV &&
+      (o.omega_mode != VF_OMEGA_AUTO || o.n_smooth > 2 || o.cheb_ratio < 2 || o.fine_kernel == VF_FINE_GATHER ||
+       o.coarse_storage == VF_STENCIL_FULL)) {
+    g_last_error = "Chebyshev smoothing needs omega_mode AUTO, n_smooth <= 2, cheb_ratio >= 2, a modal fine kernel "
+                   "and symmetric coarse storage";
     return VF_ERR_ARG;
   }
   int ndev = 0;
@@ -1901,6 +1968,7 @@ void share_operator(vf_solver* c, const vf_solver* m) {
   c->dense_n = m->dense_n;
   c->d_omega = m->d_omega;
   c->d_lambda = m->d_lambda;
+  c->d_cheb = m->d_cheb;
   c->h_omega = m->h_omega;
   c->h_lambda = m->h_lambda;
   c->h_mask_ref = m->h_mask_ref;

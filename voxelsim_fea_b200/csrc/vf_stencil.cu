@@ -580,6 +580,9 @@ __global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, cons
   const T* __restrict__ minv = (const T*)a.minv;
   const uint8_t* __restrict__ mask = a.mask;
   const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
+  const T* dprev = (const T*)a.dprev;
+  T* dout = (T*)a.dout;
+  const T c1 = a.c1_dev ? (T)(*a.c1_dev) : (T)0;
 
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SX + tx;
   const int X0 = blockIdx.x * SX, Y0 = blockIdx.y * SY;
@@ -690,9 +693,13 @@ __global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, cons
         dot += (double)u[p3] * (double)k0 + (double)u[p3 + 1] * (double)k1 + (double)u[p3 + 2] * (double)k2;
     } else if (EPI == EPI_SMOOTH) {
       const T r0 = b[p3] - k0, r1 = b[p3 + 1] - k1, r2 = b[p3 + 2] - k2;
-      out[p3] = u[p3] + ((m & 1) ? w * (minv[p3] * r0) : (T)0);
-      out[p3 + 1] = u[p3 + 1] + ((m & 2) ? w * (minv[p3 + 1] * r1) : (T)0);
-      out[p3 + 2] = u[p3 + 2] + ((m & 4) ? w * (minv[p3 + 2] * r2) : (T)0);
+      const T u0 = u[p3], u1 = u[p3 + 1], u2 = u[p3 + 2];
+      T o0 = u0 + ((m & 1) ? w * (minv[p3] * r0) : (T)0);
+      T o1 = u1 + ((m & 2) ? w * (minv[p3 + 1] * r1) : (T)0);
+      T o2 = u2 + ((m & 4) ? w * (minv[p3 + 2] * r2) : (T)0);
+      if (dprev) { o0 += c1 * dprev[p3]; o1 += c1 * dprev[p3 + 1]; o2 += c1 * dprev[p3 + 2]; }
+      out[p3] = o0; out[p3 + 1] = o1; out[p3 + 2] = o2;
+      if (dout) { dout[p3] = o0 - u0; dout[p3 + 1] = o1 - u1; dout[p3 + 2] = o2 - u2; }
     } else {
       out[p3] = b[p3] - k0; out[p3 + 1] = b[p3 + 1] - k1; out[p3 + 2] = b[p3 + 2] - k2;
     }

@@ -48,6 +48,10 @@ class SolverOptions:
     # replacement) | "restart" (refinement)
     mixed_mode: str = "outer64"
     flexible: bool = False           # flexible CG (automatic with a learned stage)
+    # "jacobi" | "chebyshev" (same sweep count, polynomial on [lambda/cheb_ratio, lambda];
+    # needs omega_mode="auto", n_smooth <= 2)
+    smoother: str = "jacobi"
+    cheb_ratio: int = 30
     autotune: bool = True            # time z-chunk candidates of the marching kernels at set-up
     omega_mode: str = "fixed"        # "fixed" (reference) | "auto" (omega_l = rel * 2 / lambda_l)
     omega_rel: float = 0.8
@@ -155,6 +159,8 @@ class MGSolver:
         o.mixed_mode = _lib.MIXED_MODES[self.options.mixed_mode]
         o.flexible = int(bool(self.options.flexible))
         o.autotune = int(bool(self.options.autotune))
+        o.smoother = _lib.SMOOTHERS[self.options.smoother]
+        o.cheb_ratio = int(self.options.cheb_ratio)
         h = ctypes.c_void_p()
         _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
                    None, "vf_create")
