@@ -557,7 +557,7 @@ def main():
     ap.add_argument("--modal-zchunk", type=int, default=0, help="z-planes per CTA of the modal kernel (0 = auto)")
     ap.add_argument("--kernel-iters", type=int, default=3, help="launches timed by --kernel-profile")
     ap.add_argument("--mixed-mode", choices=("outer64", "reliable", "restart"), default="outer64")
-    ap.add_argument("--smoother", choices=("jacobi", "chebyshev"), default="jacobi",
+    ap.add_argument("--smoother", choices=("jacobi", "chebyshev"), default="chebyshev",
                     help="V-cycle smoothing of every arm (plain FP64, mixed, learned)")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed: residual reduction between FP64 corrections (solver default if unset)")

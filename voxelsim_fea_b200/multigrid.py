@@ -31,6 +31,15 @@ import numpy as np
 from . import _lib, compute_plan
 
 
+def _preset_smoother(kw):
+    """The presets smooth with Chebyshev polynomials wherever the chosen kernels
+    take its step (modal fine kernel, symmetric coarse storage, auto damping)."""
+    if kw.get("fine_kernel") == "gather" or kw.get("coarse_storage") == "full" or \
+            kw.get("omega_mode", "auto") != "auto":
+        return "jacobi"
+    return "chebyshev"
+
+
 @dataclasses.dataclass
 class SolverOptions:
     """B200 solver options beyond the reference's keyword arguments."""
@@ -73,7 +82,8 @@ class SolverOptions:
         iterations) is off: it was tuned for the rediscretized hierarchy, and
         the CG residual norm of a converging solve on high-contrast geometry is
         not monotone."""
-        base = dict(coarse="galerkin", coarsest="cholesky", omega_mode="auto", stall_guard=False)
+        base = dict(coarse="galerkin", coarsest="cholesky", omega_mode="auto", stall_guard=False,
+                    smoother=_preset_smoother(kw))
         base.update(kw)
         return cls(**base)
 
@@ -82,7 +92,7 @@ class SolverOptions:
         """Galerkin hierarchy, mixed precision: by default FP64 PCG preconditioned by
         the FP32 V-cycle (``mixed_mode="outer64"``)."""
         base = dict(coarse="galerkin", coarsest="cholesky", precision="mixed", omega_mode="auto",
-                    stall_guard=False)
+                    stall_guard=False, smoother=_preset_smoother(kw))
         base.update(kw)
         return cls(**base)
 
