@@ -101,3 +101,17 @@ def test_grid_assembly_matches_reference_semantics():
     np.testing.assert_array_equal(active, [True, False])
     np.testing.assert_array_equal(fixed, [0, 2, 9, 11])
     assert f[3 * 2] == 1.0 and f[3 * 5 + 2] == -2.0 and f[3 * 11] == 1.0 and abs(f.sum() - (-3.0)) < 1e-15
+
+
+def test_presets_pick_a_supported_smoother():
+    """robust() / fast() smooth with Chebyshev polynomials unless the chosen
+    kernels or damping cannot take its step; the reference preset keeps Jacobi."""
+    from voxelsim_fea_b200.multigrid import SolverOptions
+    assert SolverOptions().smoother == "jacobi"
+    assert SolverOptions.reference().smoother == "jacobi"
+    assert SolverOptions.robust().smoother == "chebyshev"
+    assert SolverOptions.fast().smoother == "chebyshev"
+    assert SolverOptions.robust(fine_kernel="gather").smoother == "jacobi"
+    assert SolverOptions.fast(coarse_storage="full").smoother == "jacobi"
+    assert SolverOptions.robust(omega_mode="fixed").smoother == "jacobi"
+    assert SolverOptions.robust(smoother="jacobi").smoother == "jacobi"
