@@ -68,3 +68,45 @@ def galerkin_hierarchy(nx, ny, nz, E, fixed_dofs, nu=0.3, min_elems=4, max_level
         Dc = sp.diags(fc.astype(float))
         out.append(((Dc @ Ac @ Dc).tocsr(), fc))
     return out
+
+
+def _lambda_max(A, dinv, free, iters=30, seed=0):
+    """Power-iteration estimate of lambda_max(D^-1 A) on the free DOFs."""
+    x = np.random.default_rng(seed).standard_normal(A.shape[0]) * free
+    lam = 0.0
+    for _ in range(iters):
+        y = dinv * (A @ x)
+        lam = np.linalg.norm(y) / np.linalg.norm(x)
+        x = y / np.linalg.norm(y)
+    return lam
+
+
+def smoothed_hierarchy(nx, ny, nz, E, fixed_dofs, nu=0.3, min_elems=4, max_levels=6, lam=None, mu=None,
+                       omega=4.0 / 3.0, pad=1.1):
+    """[(A_l, free_l)], [P_l]: Galerkin levels with smoothed prolongations.
+
+    P_l = D_l (P - (omega / lambda_l) D_l^-1 A_l P) (one damped-Jacobi step
+    applied to the trilinear P, lambda_l the padded lambda_max(D^-1 A_l)),
+    A_{l+1} = D_{l+1} P_l^T A_l P_l D_{l+1}; the coarse stencils reach two
+    nodes out (125 blocks) instead of one.  Not a reference algorithm: the
+    candidate coarse space the device hierarchy is measured against."""
+    dims = level_dims(nx, ny, nz, min_elems, max_levels)
+    K = fine_matrix(nx, ny, nz, E, nu, lam, mu)
+    free = np.ones(K.shape[0], dtype=bool)
+    free[np.asarray(fixed_dofs, dtype=np.int64)] = False
+    D = sp.diags(free.astype(float))
+    out = [((D @ K @ D).tocsr(), free)]
+    Ps = []
+    for li in range(1, len(dims)):
+        A, fr = out[-1]
+        d = A.diagonal()
+        dinv = np.where(fr & (d > 0), 1.0 / np.where(d > 0, d, 1.0), 0.0)
+        lmax = pad * _lambda_max(A, dinv, fr)
+        P = prolong_matrix(dims[li - 1], dims[li])
+        Psm = (sp.diags(fr.astype(float)) @ (P - (omega / lmax) * (sp.diags(dinv) @ (A @ P)))).tocsr()
+        Ac = (Psm.T @ A @ Psm).tocsr()
+        fc = Ac.diagonal() > 0
+        Dc = sp.diags(fc.astype(float))
+        Ps.append((Psm @ Dc).tocsr())
+        out.append(((Dc @ Ac @ Dc).tocsr(), fc))
+    return out, Ps
