@@ -25,6 +25,7 @@ solve does not shard in this build.
 
 import argparse
 import ctypes
+import hashlib
 import json
 import os
 import subprocess
@@ -40,6 +41,7 @@ sys.path.insert(0, REPO)
 METRIC = "MDOF/s to 1e-8 relative residual (time-to-solution), matrix-free hex8 GMG-PCG"
 UNIT = "MDOF/s"
 TOL = 1e-8
+REF_TOL = 1e-12      # the FP64 solve the errors are stated against
 E_MIN = 1e-9
 
 WORKLOADS = {
@@ -59,6 +61,11 @@ WORKLOADS = {
     "bracket_192": dict(shape=(192, 192, 192), seed=0, sigma=4.0, load=5000.0, patch=16, levels=5),
 }
 CPU_SAMPLE = dict(shape=(64, 32, 32), seed=0, sigma=4.0, load=5000.0, patch=16)
+PORT_NOTE = ("the reference is pure Python/numpy and is not present on the GPU host; its algorithm runs as the "
+             "oracle/ restatement, which is pinned to golden vectors generated by importing the reference "
+             "(tests/golden/make_golden.py, tests/test_oracle_golden.py)")
+DTYPE_MIXED = ("f32 V-cycle with FP16-valued scaled Galerkin stencils on the coarse levels, f64 Krylov "
+               "(FP64 fine operator for A p, dots, coarsest Cholesky solve)")
 
 
 def make_problem(w):
@@ -75,6 +82,67 @@ def make_problem(w):
 def mg_modulus(p):
     """VoxelFEA's MG convention: inactive voxels carry e_min * E (fea.py:467-469)."""
     return np.where(p["active"], p["E_stiff"], p["E_stiff"] * E_MIN)
+
+
+def active_nodes(p):
+    """Nodes of the active voxels (reference node order, x fastest)."""
+    nx, ny, nz = p["dims"]
+    a = np.asarray(p["active"], dtype=bool).reshape(nx, ny, nz)
+    n = np.zeros((nx + 1, ny + 1, nz + 1), dtype=bool)
+    for ox in (0, 1):
+        for oy in (0, 1):
+            for oz in (0, 1):
+                n[ox:ox + nx, oy:oy + ny, oz:oz + nz] |= a
+    return n.transpose(2, 1, 0).ravel()
+
+
+def field_errors(u, vm, u_ref, vm_ref, node_act, elem_act):
+    """Max-abs error over the active nodes (all three components) / max |u_ref|
+    there, and the same for the element von Mises stress over active voxels."""
+    du = np.abs(u - u_ref).reshape(-1, 3)[node_act]
+    su = np.abs(u_ref).reshape(-1, 3)[node_act].max()
+    dv = np.abs(vm - vm_ref)[elem_act]
+    sv = np.abs(vm_ref)[elem_act].max()
+    return {"u_rel_err": float(du.max() / su), "vm_rel_err": float(dv.max() / sv)}
+
+
+# DRAM traffic of the roofline kernel comes from an ncu capture summary under
+# profiles/, which records the bytes per launch and a hash of the kernel's
+# sources; the figure is reported only while the sources still hash the same.
+ROOFLINE_SOURCES = ("vf_modal_tma.cu", "vf_modal.cuh", "vf_common.cuh", "vf_wait.cuh", "vf_reduce.cuh")
+ROOFLINE_SUMMARY = "k_modal_tma_smooth_fp32_bracket256.md"
+
+
+def kernel_source_sha(files=ROOFLINE_SOURCES):
+    h = hashlib.sha256()
+    for f in files:
+        with open(os.path.join(REPO, "voxelsim_fea_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def profiled_traffic(summary=ROOFLINE_SUMMARY):
+    """(bytes per launch, note): dram read + write bytes of one launch from the
+    summary's `dram_bytes_per_launch:` line, if its `source_sha16:` line matches
+    the current sources; (None, why) otherwise."""
+    path = os.path.join(REPO, "profiles", summary)
+    try:
+        text = open(path).read()
+    except OSError:
+        return None, "no ncu summary"
+    rec = {}
+    for ln in text.splitlines():
+        ln = ln.strip().strip("`")
+        for key in ("source_sha16:", "dram_bytes_per_launch:"):
+            if ln.startswith(key):
+                rec[key[:-1]] = ln[len(key):].strip()
+    want = kernel_source_sha()
+    if rec.get("source_sha16") != want:
+        return None, f"ncu summary {summary} predates the current kernel sources (sha {want})"
+    try:
+        return float(rec["dram_bytes_per_launch"]), f"ncu capture ({summary}, source sha {want})"
+    except (KeyError, ValueError):
+        return None, f"ncu summary {summary} has no dram_bytes_per_launch line"
 
 
 # --------------------------------------------------------------------------- clocks
@@ -203,11 +271,39 @@ def cpu_baseline_record(full=None):
               "what": "one full-size FP64 element-by-element K u (gather, 24x24 GEMM, bincount scatter) of "
                       "the bench workload, numpy restatement of the reference's apply, host cores"}
     return {"value": dof / dt / 1e6, "unit": UNIT, "cores": cpu_cores(), "kind": "port", "matvec_full_size": mv,
+            "port": PORT_NOTE,
             "sample": (f"numpy restatement of the reference's Jacobi-PCG (core/fea.py:497-593) to {TOL:g} "
                        f"on the seeded bracket generator at {CPU_SAMPLE['shape'][0]}x{CPU_SAMPLE['shape'][1]}x"
                        f"{CPU_SAMPLE['shape'][2]} ({dof} DOF, {it} iterations, {dt:.1f} s); the reference's "
                        f"MG path does not converge on this geometry"),
             "seconds": dt, "iterations": it}
+
+
+def gpu_same_sample(device, check_every, steps=5):
+    """The mixed-precision device solver on the CPU arm's sample (the same
+    seeded 64x32x32 bracket to the same tolerance), timed with CUDA events:
+    the like-for-like partner of the CPU figure."""
+    import torch
+    from voxelsim_fea_b200 import generators
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    p = generators.bracket(shape=CPU_SAMPLE["shape"], seed=CPU_SAMPLE["seed"], sigma=CPU_SAMPLE["sigma"],
+                           load_n=CPU_SAMPLE["load"], patch=CPU_SAMPLE["patch"])
+    nx, ny, nz = p["dims"]
+    m = MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=4,
+                 options=SolverOptions.fast(device=device, check_every=check_every))
+    E = mg_modulus(p)
+    for _ in range(2):
+        m.solve(E, p["f"], tol=TOL)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u = m.solve(E, p["f"], tol=TOL)
+    dt = (time.perf_counter() - t0) / steps
+    res = {"mdof_per_s": m.ndof / dt / 1e6, "ms_per_solve": dt * 1e3, "iterations": int(m.last_iters),
+           "true_resid": float(m.last_info.true_resid), "dof": int(m.ndof),
+           "timing": "host clock around MGSolver.solve (host arrays in, displacement out)"}
+    m.close()
+    return res
 
 
 def run_reference(args):
@@ -231,7 +327,8 @@ def run_reference(args):
                    "method": "Jacobi-PCG (reference fallback path)", "parallelism": "host cores"},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu_cores(), "kind": "port",
-                         "sample": f"bracket generator 64x32x32 ({dof} DOF, {it} iterations) per step"},
+                         "sample": f"bracket generator 64x32x32 ({dof} DOF, {it} iterations) per step",
+                         "port": PORT_NOTE},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -276,8 +373,8 @@ def run_batch(args):
     line = {"metric": METRIC, "value": ndof / (ms / 1e3) / 1e6, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": ("f32 V-cycle, f64 Krylov (FP64 fine operator for A p, dots, coarsest solve)"
-                      if args.mixed_mode == "outer64" else "f32 (FP64 dots, refinement residual, coarsest solve)"),
+            "dtype": (DTYPE_MIXED if args.mixed_mode == "outer64"
+                      else "f32 (FP64 dots, refinement residual, coarsest solve)"),
             "data": "synthetic (seeded generator)",
             "config": {"workload": f"batch{args.batch}_parts_32-128", "dof": ndof, "parts": args.batch,
                        "iterations_max": max(s.last_iters for s in solvers), "timing": "host clock, synchronous call"}}
@@ -410,20 +507,57 @@ def run_b200(args):
         raise SystemExit(f"bench: solve did not reach tol={TOL:g} (true residual {true_resid:.3e}, "
                          f"{iters} iterations): no valid measurement")
     value = world * K * ndof / (ms / 1e3) / 1e6
+    u_mixed = u_d.cpu().numpy() if K == 1 else None
+
+    # Displacement and von Mises error of every arm against an FP64 solve
+    # converged far below the bench tolerance (same geometry, load and
+    # hierarchy, FP64 throughout, relative residual < REF_TOL).
+    E_stress = np.ascontiguousarray(p["E_stress"], dtype=np.float64)
+    nu_host = np.ascontiguousarray(p["nu"], dtype=np.float64) if per_voxel_nu else None
+    act_u8 = np.ascontiguousarray(p["active"], dtype=np.uint8)
+    node_act = active_nodes(p)
+    elem_act = np.asarray(p["active"], dtype=bool)
+
+    def von_mises(u):
+        vm = np.empty(nelem)
+        _lib.check(L.vf_von_mises(fast._h, _lib.ptr(np.ascontiguousarray(u)), _lib.ptr(E_stress),
+                                  _lib.ptr(nu_host), _lib.ptr(act_u8), _lib.ptr(vm)), fast._h)
+        return vm
 
     # plain FP64 GMG-PCG (same hierarchy, FP64 everywhere) on the same GPU
     plain = None
-    if not args.no_plain:
+    ref_fields = None
+    u_plain = None
+    if not args.no_plain or (K == 1 and not args.no_errors):
         ps = solver(SolverOptions.robust(device=local, check_every=args.check_every, smoother=args.smoother))
         L.vf_get_stream(ps._h, ctypes.byref(stream_ptr))
         ext_plain = torch.cuda.ExternalStream(stream_ptr.value)
         ext_save = ext
         ext = ext_plain
-        pms, (pit, pres, _), _, _ = timed(ps, max(1, args.steps // 2), 1)
+        if not args.no_plain:
+            pms, (pit, pres, _), _, _ = timed(ps, max(1, args.steps // 2), 1)
+            plain = {"ms_per_solve": pms, "iterations": pit, "true_resid": pres,
+                     "mdof_per_s": ndof / (pms / 1e3) / 1e6, "speedup_of_mixed": pms / ms}
+            u_plain = u_d.cpu().numpy() if K == 1 else None
         ext = ext_save
-        plain = {"ms_per_solve": pms, "iterations": pit, "true_resid": pres,
-                 "mdof_per_s": ndof / (pms / 1e3) / 1e6, "speedup_of_mixed": pms / ms}
+        if K == 1 and not args.no_errors:
+            _lib.check(L.vf_set_material(ps._h, ctypes.c_void_p(E_d.data_ptr()), nu_ptr, DEV), ps._h)
+            rinfo = _lib.VfSolveInfo()
+            rc = L.vf_solve(ps._h, ctypes.c_void_p(f_d.data_ptr()), None, REF_TOL, 20000, DEV,
+                            ctypes.c_void_p(u_d.data_ptr()), ctypes.byref(rinfo))
+            if rc == _lib.VF_OK and rinfo.true_resid < 1e3 * REF_TOL:
+                u_ref = u_d.cpu().numpy()
+                ref_fields = (u_ref, von_mises(u_ref), {"tol": REF_TOL, "iterations": int(rinfo.iters),
+                                                        "true_resid": float(rinfo.true_resid)})
+            else:
+                print(f"bench: FP64 reference solve did not converge (status {rc}, true residual "
+                      f"{rinfo.true_resid:.3e}); no error figures", file=sys.stderr)
         ps.close()
+
+    def errors_of(u):
+        if ref_fields is None or u is None:
+            return None
+        return field_errors(u, von_mises(u), ref_fields[0], ref_fields[1], node_act, elem_act)
 
     # learned stage + mixed precision (flexible CG with the U-Net stage after
     # each V-cycle), packaged weights; reported beside the mixed solver
@@ -441,7 +575,11 @@ def run_b200(args):
                    "mdof_per_s": ndof / (lms / 1e3) / 1e6,
                    "speedup_vs_plain_fp64": (plain["ms_per_solve"] / lms) if plain else None,
                    "converged": bool(lres < TOL)}
+        if K == 1:
+            learned["errors_vs_fp64_ref"] = errors_of(u_d.cpu().numpy())
         ls.close()
+    if plain is not None:
+        plain["errors_vs_fp64_ref"] = errors_of(u_plain)
 
     # roofline of the dominant kernel: fused FP32 Jacobi sweep on the fine level
     nodes = (nx + 1) * (ny + 1) * (nz + 1)
@@ -457,16 +595,20 @@ def run_b200(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = sweep_bytes / (kms.value / 1e3) / 1e9
-    # DRAM traffic of one launch from the ncu capture summarised in
-    # profiles/k_modal_tma_smooth_fp32_bracket256.md (read + write, same workload)
-    traffic = 184.44e6 + 34.92e6
+    traffic, traffic_src = profiled_traffic()
+    a64 = ctypes.c_double()
+    _lib.check(L.vf_time_kernel(fast._h, 0, _lib.VF_PREC_FP64, 50, ctypes.byref(a64)), fast._h)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "traffic_unit": "B per launch (ncu)",
+                "frac": achieved / peak, "traffic": traffic, "traffic_unit": "B per launch (dram read + write)",
+                "traffic_source": traffic_src,
                 "kernel": "k_modal_tma<float, SMOOTH> (fused damped-Jacobi sweep, level 0, TMA-staged)",
                 "ms_per_launch": kms.value, "algorithmic_bytes_per_launch": sweep_bytes,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst)" if peaks else "fallback 6650 GB/s",
                 "matvec_ms_per_launch": amv.value,
-                "matvec_gbs": 29 * nodes / (amv.value / 1e3) / 1e9}
+                "matvec_gbs": 29 * nodes / (amv.value / 1e3) / 1e9,
+                "matvec_frac": 29 * nodes / (amv.value / 1e3) / 1e9 / peak,
+                "matvec_fp64_ms_per_launch": a64.value,
+                "matvec_fp64_gbs": 57 * nodes / (a64.value / 1e3) / 1e9}
 
     # e2e through the public API: modulus and load in, displacement out, host
     # numpy arrays in page-locked memory, every step
@@ -500,14 +642,21 @@ def run_b200(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_record(full=((nx, ny, nz), E_mg, nu_scalar))
+        same = gpu_same_sample(local, args.check_every)
+        same["speedup_vs_cpu"] = same["mdof_per_s"] / cpu["value"]
+        cpu["gpu_same_sample"] = same
+        if cpu.get("matvec_full_size"):
+            mv = cpu["matvec_full_size"]
+            mv["device_fp64_ms_per_apply"] = a64.value
+            mv["device_fp64_speedup"] = mv["seconds_per_apply"] * 1e3 / a64.value
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": ("f32 V-cycle, f64 Krylov (FP64 fine operator for A p, dots, coarsest solve)"
-                      if args.mixed_mode == "outer64" else "f32 (FP64 dots, refinement residual, coarsest solve)"),
+            "dtype": (DTYPE_MIXED if args.mixed_mode == "outer64"
+                      else "f32 (FP64 dots, refinement residual, coarsest solve)"),
             "data": "synthetic (seeded generator)",
             "config": {"workload": args.workload + (f"_block{K}" if K > 1 else ""), "dof": ndof,
                        "rhs_per_step": K, "active_voxels": int(p["active"].sum()),
@@ -516,6 +665,8 @@ def run_b200(args):
                        "tol": TOL, "l2": "working set > 126 MB L2 (vectors 54-107 MB each)",
                        "parallelism": f"replicas x{world}"},
             "iterations": iters, "outer_iterations": outer, "true_resid": true_resid,
+            "errors_vs_fp64_ref": errors_of(u_mixed),
+            "fp64_ref": ref_fields[2] if ref_fields else None,
             "setup_ms_per_step": setup_ms,
             "time_to_solution_s": ms / 1e3,
             "plain_fp64": plain,
@@ -549,6 +700,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0,
                     help="N independent parts (edges 32..128) per step in one vf_solve_batch call")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-errors", action="store_true", help="skip the FP64 reference solve and the error figures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nvtx", action="store_true", help="wrap the timed steps in NVTX range vf_timed")
     ap.add_argument("--kernel-profile", choices=("apply", "smooth", "resid", "restrict", "prolong", "vcycle"),

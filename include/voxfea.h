@@ -276,18 +276,19 @@ int vf_time_kernel(vf_solver* s, int32_t kernel, int32_t precision, int32_t iter
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory -- programs that own all device memory through their own allocator or
  * a fixed arena, and code that must avoid the implicit device synchronisation of
- * cudaMalloc/cudaFree.  Computes y = mask(K u) (the fine hex8 operator with
- * Ke(nu), the reference's MGSolver._apply at level 0, multigrid.py:318-341) and
- * *u_dot_y = u . y on `stream` (cudaStream_t, NULL = default stream), without a
- * solver handle and without allocating: its only scratch is a fixed static
- * device array of 256 KiB + 256 B, shared by every call on a device.
+ * cudaMalloc/cudaFree.  Computes y = mask(K u) -- the level-0 operator of
+ * vf_apply, the fine hex8 operator with Ke(nu) -- and *u_dot_y = u . y on
+ * `stream` (cudaStream_t, NULL = default stream), without a solver handle and
+ * without allocating: its only scratch is a fixed static device array of
+ * 256 KiB + 256 B, shared by every call on a device.
  * All pointers are device pointers in the reference layout: E (nelem, iz-fastest),
  * free_mask (one byte per node, bit c set <=> DOF c free), u and y (3 per node),
- * u_dot_y (one double).  Limits: (nx+1)(ny+1)(nz+1) <= 8,388,608 nodes, else
- * VF_ERR_ARG.  The first call on each device sets up the scratch address; make
- * it before any stream capture.  Calls that overlap on the GPU race on the
- * shared scratch: order them on one stream.  Asynchronous: returns after
- * enqueueing. */
+ * u_dot_y (one double).  u, y and u_dot_y must not overlap (an overlapping y or
+ * u_dot_y returns VF_ERR_ARG).  Limits: (nx+1)(ny+1)(nz+1) <= 8,388,608 nodes,
+ * else VF_ERR_ARG.  The first call on each device looks up the scratch address
+ * and keeps it; make it before any stream capture, and make no call on a device
+ * after cudaDeviceReset there.  Calls that overlap on the GPU race on the shared
+ * scratch: order them on one stream.  Asynchronous: returns after enqueueing. */
 int vf_apply_noalloc(int32_t nx, int32_t ny, int32_t nz, double nu, const double* E,
                      const uint8_t* free_mask, const double* u, double* y, double* u_dot_y,
                      void* stream);

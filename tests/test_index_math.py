@@ -6,8 +6,11 @@ written by exactly one (CTA, lane, step), for grids with partial tiles,
 ranges that cross tile boundaries, and more CTAs than units."""
 
 import itertools
+import os
 
 import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 TX, TY, L = 32, 8, 2   # CTA tile (threads) and z-lanes of the FP32 kernel
 
@@ -63,3 +66,21 @@ def test_every_output_plane_written_once(dims, zchunk, nb):
     expect = set(itertools.product(range(ntx * nty), range(lz + 1)))
     assert set(seen) == expect
     assert all(v == 1 for v in seen.values())
+
+
+def test_tma_wait_is_bounded_by_one_second():
+    """The TMA pipeline's mbarrier wait (vf_wait.cuh): the suspend-time hint is
+    in nanoseconds, and polls x hint stays within the 1 s wall-time limit, so a
+    stuck stage cannot hold a CTA longer than about a second."""
+    import re
+    src = open(os.path.join(REPO, "voxelsim_fea_b200", "csrc", "vf_wait.cuh")).read()
+
+    def const(name):
+        m = re.search(name + r"\s*=\s*([0-9]+)u", src)
+        assert m, name
+        return int(m.group(1))
+
+    hint, polls, limit = const("kPollHintNs"), const("kMaxPolls"), const("kWaitLimitNs")
+    assert limit <= 1_000_000_000
+    assert hint * polls <= limit
+    assert hint <= 10_000          # a poll sleeps at most 10 us

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <type_traits>
 #include <utility>
@@ -32,6 +33,26 @@ inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
                      Args&&... args) {
   count_launch(st);
   kern<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+}
+
+// One-time set-up of a kernel that takes more than 48 KiB of dynamic shared
+// memory.  The runtime applies cudaFuncSetAttribute per device, and a process
+// may drive solvers on several devices, so the attribute is set -- and the
+// resident CTAs per SM measured -- the first time each device launches the
+// kernel; `cache` holds one slot per device ordinal.  Returns CTAs per SM (>= 1).
+constexpr int kMaxDevices = 64;
+template <typename Kern>
+inline int kernel_prepare(std::atomic<int> (&cache)[kMaxDevices], Kern kern, size_t smem, int threads) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  std::atomic<int>* slot = (dev >= 0 && dev < kMaxDevices) ? &cache[dev] : nullptr;
+  const int have = slot ? slot->load() : 0;
+  if (have > 0) return have;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int o = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, threads, smem) != cudaSuccess || o < 1) o = 1;
+  if (slot) slot->store(o);
+  return o;
 }
 
 struct Grid {

@@ -347,11 +347,8 @@ void launch_modal_op(const Grid& g, int epi, const OpArgs& a, const ModalConst& 
   do {                                                                                        \
     auto kern = k_modal_op<T, LM, EP, TYV>;                                                   \
     constexpr size_t smem = modal_smem_bytes<T, TYV, LM, EP>();                               \
-    static std::atomic<bool> attr{false};                                                     \
-    if (!attr.load()) {                                                                       \
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
-      attr.store(true);                                                                       \
-    }                                                                                         \
+    static std::atomic<int> per_dev[kMaxDevices];                                             \
+    kernel_prepare(per_dev, kern, smem, TX * TYV);                                            \
     launch_k(kern, grid, block, smem, st, g, a, mc, zchunk);                                  \
   } while (0)
   if (lame) {

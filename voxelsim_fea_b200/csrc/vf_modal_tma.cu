@@ -14,8 +14,10 @@
 // 16-byte boundary (the rule for tiled bulk copies) and the box is widened by
 // up to 3 elements; threads index from the remainder.  Out-of-range planes
 // and columns read zeros (the tensor maps' fill), like the ghost shell.
-// Every wait on an mbarrier is bounded: on expiry the kernel raises an error
-// flag that the host turns into a status.
+// Every wait on an mbarrier is bounded (vf_wait.cuh: about 1 s): on expiry
+// the CTA stops marching, raises the error flag (the host turns it into a
+// status), waits -- again bounded -- for the copies it still has in flight
+// and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -28,6 +30,7 @@
 #include "vf_common.cuh"
 #include "vf_modal.cuh"
 #include "vf_reduce.cuh"
+#include "vf_wait.cuh"
 
 namespace vf {
 
@@ -75,29 +78,12 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(su32(bar)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(su32(bar)), "r"(parity), "r"(1000000u)
-      : "memory");
-  return ok != 0;
-}
 __device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
       "[%5];\n" ::"r"(su32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(su32(bar))
       : "memory");
-}
-
-// Bounded wait: ~1e6 polls of at most ~1 us each; on expiry raise the flag
-// (the solver reports VF_ERR_CUDA) and continue.
-__device__ __forceinline__ void wait_stage(uint64_t* bar, unsigned parity, int* err) {
-  for (int i = 0; i < (1 << 20); ++i)
-    if (mbar_try_wait(bar, parity)) return;
-  if (err) atomicExch(err, 1);
 }
 
 template <typename T, bool LAME, int EPI>
@@ -148,6 +134,7 @@ __global__ void __launch_bounds__(TX * TY, 2)
   const int sz = g.px * g.py;
   // per-segment geometry (set at the top of each segment)
   int X0 = 0, Y0 = 0, Xc = 0, Yc = 0, colbase = 0, xu = 0, ou = 0, xe = 0, oe = 0, nsteps = 0, gbase = 0;
+  int issued_hi = -1;   // leader: running index of the last step whose copies were issued
   bool out_col = false;
   int z0[L], oend[L];
 
@@ -162,6 +149,7 @@ __global__ void __launch_bounds__(TX * TY, 2)
   auto issue = [&](int s) {   // leader only
     const int st = (gbase + s) % NSTAGE;
     unsigned char* base = smem + st * Lay::STAGE;
+    issued_hi = gbase + s;
     mbar_expect_tx(&bar[st], Lay::TXB);
 #pragma unroll
     for (int l = 0; l < L; ++l) {
@@ -195,11 +183,13 @@ __global__ void __launch_bounds__(TX * TY, 2)
   P hiPrev[3][4];
   double dot = 0.0;
 
-  auto step = [&](const int s, P (&Fc)[3][4], const P (&Fp)[3][4]) {
+  // false: this step's copies did not arrive in time (every thread agrees)
+  auto step = [&](const int s, P (&Fc)[3][4], const P (&Fp)[3][4]) -> bool {
     const int gs = gbase + s;
     const int st = gs % NSTAGE, sp = (gs + NSTAGE - 1) % NSTAGE;
-    wait_stage(&bar[st], (unsigned)((gs / NSTAGE) & 1), a.err);
-    __syncthreads();                         // step s-1 done everywhere: stage (s+2) is free
+    const bool arrived = mbar_wait_bounded(&bar[st], (unsigned)((gs / NSTAGE) & 1));
+    // the barrier also marks step s-1 done everywhere: stage (s+2) is free
+    if (__syncthreads_or(!arrived)) return false;
     if (leader && s + 2 < nsteps) issue(s + 2);
     uint8_t mk[L];
 #pragma unroll
@@ -299,9 +289,11 @@ __global__ void __launch_bounds__(TX * TY, 2)
     } else {
       __syncthreads();
     }
+    return true;
   };
 
   P Fa[3][4], Fb[3][4];
+  int failed_at = -1;   // running index of the step whose copies did not arrive
   // Segments: a new segment's first two loads go to the stages of steps
   // gbase-4 and gbase-3, whose last readers (steps gbase-3 and gbase-2) every
   // thread has left once the leader is past step gbase-1's first barrier.
@@ -340,13 +332,27 @@ __global__ void __launch_bounds__(TX * TY, 2)
     }
 #pragma unroll 1
     for (int s = 0; s < nsteps; ++s) {
-      step(s, Fa, Fb);
+      if (!step(s, Fa, Fb)) {
+        failed_at = gbase + s;
+        break;
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int m = 0; m < 4; ++m) Fb[c][m] = Fa[c][m];
     }
+    if (failed_at >= 0) break;
     gbase += nsteps;
+  }
+  if (failed_at >= 0) {
+    // expired wait: flag it, then let the copies still in flight (steps
+    // failed_at .. issued_hi, at most three) land before the CTA exits --
+    // each wait bounded like the first
+    if (leader) {
+      if (a.err) atomicExch(a.err, 1);
+      for (int k = failed_at; k <= issued_hi; ++k) mbar_wait_bounded(&bar[k % NSTAGE], (unsigned)((k / NSTAGE) & 1));
+    }
+    __syncthreads();
   }
   // APPLY: u.y (p.Ap); SMOOTH: b.u' (the V-cycle's last sweep: r.z)
   if ((EPI == EPI_APPLY || EPI == EPI_SMOOTH) && a.dot_partials && ks)
@@ -424,13 +430,8 @@ bool launch_modal_tma(const Grid& g, int epi, const OpArgs& a, const ModalConst&
   do {                                                                                        \
     auto kern = k_modal_tma<T, LM, EP>;                                                       \
     constexpr size_t smem = Layout<T, LM, EP>::total();                                       \
-    static std::atomic<int> per_sm{0};                                                        \
-    if (per_sm.load() == 0) {                                                                 \
-      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);     \
-      int o = 0;                                                                              \
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, TX * TY, smem) != cudaSuccess || o < 1) o = 1; \
-      per_sm.store(o);                                                                        \
-    }                                                                                         \
+    static std::atomic<int> per_dev[kMaxDevices];                                             \
+    const int per_sm = kernel_prepare(per_dev, kern, smem, TX * TY);                          \
     long long nb;                                                                             \
     if (zchunk > 0) {                                                                         \
       nb = tiles * ((g.lz + 1 + zchunk - 1) / zchunk);                                        \
@@ -438,7 +439,7 @@ bool launch_modal_tma(const Grid& g, int epi, const OpArgs& a, const ModalConst&
       int dev = 0, sms = 148;                                                                 \
       cudaGetDevice(&dev);                                                                    \
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);                      \
-      nb = std::min<long long>((long long)sms * per_sm.load(), units);                        \
+      nb = std::min<long long>((long long)sms * per_sm, units);                               \
     }                                                                                         \
     launch_k(kern, dim3((unsigned)nb), block, smem, st, g, a, mc, zchunk, mu, me, mm, mb, md); \
   } while (0)

@@ -301,13 +301,8 @@ __global__ void k_reduce_partials(const float* __restrict__ partial, int nparts,
 template <int CIN, int COUT>
 int conv_forward_t(const NnConvArgs& a, cudaStream_t st) {
   constexpr size_t smem = conv_smem_bytes<CIN, COUT>();
-  static std::atomic<int> attr_dev{-1};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev.load() != dev) {
-    cudaFuncSetAttribute(k_conv3<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_dev.store(dev);
-  }
+  static std::atomic<int> per_dev[kMaxDevices];
+  kernel_prepare(per_dev, k_conv3<CIN, COUT>, smem, NTHREADS);
   const long long tiles = (long long)((a.X + OTX - 1) / OTX) * ((a.Y + OTY - 1) / OTY) * ((a.Z + OTZ - 1) / OTZ);
   if (tiles <= 0) return 0;
   launch_k(k_conv3<CIN, COUT>, dim3((unsigned)tiles), dim3(NTHREADS), smem, st, a);
@@ -324,13 +319,8 @@ int conv_wgrad_t(const void* x, const void* dy, float* dw, float* work, size_t w
   nb = std::min<long long>(nb, (long long)(work_bytes / per));
   if (nb < 1) return -1;
   constexpr size_t smem = Cfg::smem();
-  static std::atomic<int> attr_dev{-1};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (attr_dev.load() != dev) {
-    cudaFuncSetAttribute(k_conv3_wgrad<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_dev.store(dev);
-  }
+  static std::atomic<int> per_dev[kMaxDevices];
+  kernel_prepare(per_dev, k_conv3_wgrad<CIN, COUT>, smem, NTHREADS);
   launch_k(k_conv3_wgrad<CIN, COUT>, dim3((unsigned)nb, 27 / Cfg::TAPS), dim3(NTHREADS), smem, st,
            (const bf16*)x, (const bf16*)dy, work, X, Y, Z);
   const long long n = 27LL * COUT * CIN;

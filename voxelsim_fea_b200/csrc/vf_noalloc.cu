@@ -19,8 +19,12 @@
 //     Calls whose kernels overlap on the GPU (different streams, no ordering)
 //     race on the array and give wrong results: order them on one stream;
 //   * the first call on each device looks up the array's device address
-//     (cudaGetSymbolAddress with that device current); make that first call
-//     before any stream capture.
+//     (cudaGetSymbolAddress with that device current) and keeps it for the
+//     process; make that first call before any stream capture.  A
+//     cudaDeviceReset tears the module down with the context, so the kept
+//     address is stale afterwards: make no call on that device after a reset;
+//   * u, y and u_dot_y must not overlap: threads read u at neighbouring nodes
+//     while others write y, so an in-place call is rejected.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -165,6 +169,17 @@ extern "C" int vf_apply_noalloc(int32_t nx, int32_t ny, int32_t nz, double nu, c
     vf::g_last_error = "vf_apply_noalloc: grid has " + std::to_string(nn) + " nodes; the fixed scratch array "
                        "supports at most " + std::to_string(kMaxNodes) + " ((nx+1)(ny+1)(nz+1) <= 8388608)";
     return VF_ERR_ARG;
+  }
+  {
+    // [u, u + 3nn), [y, y + 3nn) and the one double at u_dot_y must be disjoint
+    const uintptr_t bu = (uintptr_t)u, by = (uintptr_t)y, bd = (uintptr_t)u_dot_y;
+    const uintptr_t len = (uintptr_t)(3 * nn) * sizeof(double);
+    auto overlap = [](uintptr_t a0, uintptr_t a1, uintptr_t b0, uintptr_t b1) { return a0 < b1 && b0 < a1; };
+    if (overlap(bu, bu + len, by, by + len) || overlap(bd, bd + sizeof(double), bu, bu + len) ||
+        overlap(bd, bd + sizeof(double), by, by + len)) {
+      vf::g_last_error = "vf_apply_noalloc: u, y and u_dot_y must not overlap";
+      return VF_ERR_ARG;
+    }
   }
   unsigned char* base = nullptr;
   int rc = scratch_for_device(&base);

@@ -32,102 +32,147 @@ import numpy as np
 _STRESS_PERCENTILE = 99.0   # solve_worker.py:37
 
 
-class SolverClient:
-    """Launch the worker and poll it without blocking (solve_worker.py:46-167).
-
-    Events from :meth:`poll`: ('voxel', frac), ('solve', info|None),
-    ('done', final dict), ('error', message), ('running', frac)."""
+class _JobFiles:
+    """The files one job exchanges with its worker, in a private temp folder:
+    job.pkl (in), status.json (progress, rewritten atomically by the worker),
+    final.pkl (result) and worker.log (the worker's stdout and stderr)."""
 
     def __init__(self):
-        self._proc = None
-        self._dir = None
-        self._logf = None
-        self._finished = False
+        self.root = tempfile.mkdtemp(prefix="voxfea_b200_solve_")
+        self.job = os.path.join(self.root, "job.pkl")
+        self.status = os.path.join(self.root, "status.json")
+        self.final = os.path.join(self.root, "final.pkl")
+        self.log = os.path.join(self.root, "worker.log")
 
-    def start(self, job):
-        self._dir = tempfile.mkdtemp(prefix="voxfea_b200_solve_")
-        job_path = os.path.join(self._dir, "job.pkl")
-        with open(job_path, "wb") as fh:
+    def spawn_worker(self, job):
+        """Write the job and start the worker process on it; returns
+        (process, open log handle)."""
+        with open(self.job, "wb") as fh:
             pickle.dump(job, fh)
-        cmd = [sys.executable, "-m", "voxelsim_fea_b200.solve_worker", job_path, self._dir]
-        env = dict(os.environ)
-        pkg_parent = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-        env["PYTHONPATH"] = os.pathsep.join(p for p in (pkg_parent, env.get("PYTHONPATH", "")) if p)
-        self._logf = open(os.path.join(self._dir, "worker.log"), "wb")
-        self._proc = subprocess.Popen(cmd, stdout=self._logf, stderr=self._logf, env=env)
+        # the worker imports this package by name: put its parent folder on the
+        # child's path (the parent process's own sys.path is left alone)
+        env = os.environ.copy()
+        here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        env["PYTHONPATH"] = os.pathsep.join(filter(None, [here, env.get("PYTHONPATH")]))
+        log = open(self.log, "wb")
+        proc = subprocess.Popen([sys.executable, "-m", "voxelsim_fea_b200.solve_worker", self.job, self.root],
+                                stdout=log, stderr=subprocess.STDOUT, env=env)
+        return proc, log
 
-    def _status(self):
+    def read_status(self):
+        """The worker's last status record, or None while there is none (or
+        it cannot be parsed yet)."""
         try:
-            with open(os.path.join(self._dir, "status.json")) as fh:
+            with open(self.status) as fh:
                 return json.load(fh)
-        except Exception:
+        except (OSError, ValueError):
             return None
 
-    def _log_tail(self):
+    def read_final(self):
+        with open(self.final, "rb") as fh:
+            return pickle.load(fh)
+
+    def log_text(self):
         try:
-            with open(os.path.join(self._dir, "worker.log"), "rb") as fh:
+            with open(self.log, "rb") as fh:
                 return fh.read().decode("utf-8", "replace").strip()
-        except Exception:
+        except OSError:
             return ""
 
+    def remove(self):
+        shutil.rmtree(self.root, ignore_errors=True)
+
+
+class SolverClient:
+    """Runs one solve job in a worker process and reports its progress without
+    blocking -- the parent side of core/solve_worker.py (its SolverClient,
+    solve_worker.py:44-153), whose event protocol this keeps.
+
+    :meth:`poll` returns one of
+      ('voxel', frac)    the worker is building the grid (0..1);
+      ('solve', info)    the CG solve runs; info is None until the worker's
+                         first progress record, then {'iter', 'resid', 'tol'};
+      ('done', final)    the result dict of final.pkl (returned once; later
+                         polls give ('running', 1.0));
+      ('error', message)
+      ('running', frac)  nothing new to report."""
+
+    def __init__(self):
+        self._files = None
+        self._proc = None
+        self._log = None
+        self._delivered = False
+
+    def start(self, job):
+        self._files = _JobFiles()
+        self._proc, self._log = self._files.spawn_worker(job)
+
+    # -- progress ------------------------------------------------------------
     def poll(self):
-        if self._finished:
+        if self._delivered:
             return ("running", 1.0)
-        st = self._status()
-        if st is None:
-            if self._proc is not None and self._proc.poll() is not None:
-                return ("error", self._log_tail() or "worker exited early")
-            return ("running", 0.0)
-        phase = st.get("phase")
-        if phase == "error":
-            return ("error", st.get("error") or self._log_tail() or "worker error")
-        if phase == "voxel":
-            return ("voxel", float(st.get("frac", 0.0)))
-        if phase == "solve":
-            info = None
-            if "cg_iter" in st:
-                info = {"iter": int(st.get("cg_iter", 0)), "resid": float(st.get("cg_resid", float("nan"))),
-                        "tol": float(st.get("cg_tol", 1e-6))}
-            return ("solve", info)
-        if phase == "done":
-            try:
-                with open(os.path.join(self._dir, "final.pkl"), "rb") as fh:
-                    final = pickle.load(fh)
-            except Exception as exc:
-                return ("error", f"could not read solver result: {exc}")
-            self._finished = True
-            return ("done", final)
+        status = self._files.read_status() if self._files is not None else None
+        if status is None:
+            return self._before_first_status()
+        react = self._BY_PHASE.get(status.get("phase"))
+        return react(self, status) if react is not None else ("running", 0.0)
+
+    def _before_first_status(self):
+        exited = self._proc is not None and self._proc.poll() is not None
+        if exited:
+            log = self._files.log_text() if self._files is not None else ""
+            return ("error", log or "worker exited early")
         return ("running", 0.0)
 
+    def _phase_voxel(self, status):
+        return ("voxel", float(status.get("frac", 0.0)))
+
+    def _phase_solve(self, status):
+        if "cg_iter" not in status:
+            return ("solve", None)
+        return ("solve", {"iter": int(status["cg_iter"]),
+                          "resid": float(status.get("cg_resid", float("nan"))),
+                          "tol": float(status.get("cg_tol", 1e-6))})
+
+    def _phase_done(self, status):
+        try:
+            final = self._files.read_final()
+        except Exception as exc:   # a truncated or missing result file
+            return ("error", f"could not read solver result: {exc}")
+        self._delivered = True
+        return ("done", final)
+
+    def _phase_error(self, status):
+        return ("error", status.get("error") or self._files.log_text() or "worker error")
+
+    _BY_PHASE = {"voxel": _phase_voxel, "solve": _phase_solve, "done": _phase_done, "error": _phase_error}
+
     def wait(self, timeout=None, interval=0.05):
-        """Block until done/error (convenience for scripts and tests)."""
-        t0 = time.time()
+        """Poll until the job is done or failed (for scripts and tests)."""
+        deadline = None if timeout is None else time.monotonic() + timeout
         while True:
-            ev = self.poll()
-            if ev[0] in ("done", "error"):
-                return ev
-            if timeout is not None and time.time() - t0 > timeout:
+            event = self.poll()
+            if event[0] in ("done", "error"):
+                return event
+            if deadline is not None and time.monotonic() > deadline:
                 return ("error", "timeout")
             time.sleep(interval)
 
+    # -- teardown --------------------------------------------------------------
     def cancel(self):
+        """Stop a running worker and remove the job's files."""
         if self._proc is not None and self._proc.poll() is None:
-            try:
-                self._proc.terminate()
-            except Exception:
-                pass
+            self._proc.terminate()
         self.cleanup()
 
     def cleanup(self):
-        if self._logf is not None:
-            try:
-                self._logf.close()
-            except Exception:
-                pass
-            self._logf = None
-        if self._dir and os.path.isdir(self._dir):
-            shutil.rmtree(self._dir, ignore_errors=True)
-        self._dir = None
+        """Close the log handle and remove the job's files (idempotent)."""
+        log, self._log = self._log, None
+        if log is not None and not log.closed:
+            log.close()
+        files, self._files = self._files, None
+        if files is not None:
+            files.remove()
 
 
 def solver_available():
