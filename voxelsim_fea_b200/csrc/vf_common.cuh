@@ -201,6 +201,41 @@ template <typename T, typename S> void launch_stencil_sym_op(const Grid& g, int 
 int sym_zchunk(const Grid& g);
 void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu, const uint8_t* fmask,
                                const Grid& c, double* stencil_c, const double* Gtab, int lame, cudaStream_t st);
+
+// vf_wide.cu -- reach-R Galerkin levels (coarse space with a smoothed prolongation).
+// Scaled symmetric storage of a reach-R stencil: the diagonal block (6
+// values) and the upper blocks s > center (9 values each), padded to whole
+// 16-byte chunks; warp-chunked like SymLayout.
+template <typename S, int R> struct WideLayout {
+  static constexpr int W = 2 * R + 1, NB = W * W * W, NU = NB / 2;
+  static constexpr int NV = 6 + 9 * NU;
+  static constexpr int VPC = 16 / (int)sizeof(S);
+  static constexpr int NVP = (NV + 7) / 8 * 8;
+  static constexpr int NCH = NVP / VPC;
+  using Q = typename std::conditional<sizeof(S) == 8, double, float>::type;
+  __host__ __device__ static constexpr long long off(long long p, int k) {
+    return ((p >> 5) * NCH + k / VPC) * (32LL * VPC) + (p & 31) * VPC + (k % VPC);
+  }
+  static size_t count(long long n) { return (size_t)((n + 31) / 32) * 32 * NVP; }
+};
+size_t wide_prolong_count(const Grid& f, int Pr);
+size_t wide_rapb_count(const Grid& f, int Pr, int Rf);
+// A_c (reach Rc = (2 Pr + Rf) / 2, full FP64 stencil) = P_s^T A_f P_s with
+// P_s = D_f (I - c D_f^-1 A_f) P (c = *cdev; cdev null or *cdev == 0: the
+// trilinear P, Pr = 1); psb / bsb: scratch of wide_prolong_count /
+// wide_rapb_count doubles.
+void launch_wide_galerkin(const Grid& f, const double* stf, int Rf, const uint8_t* fmask, const double* minvf,
+                          const double* cdev, int Pr, const Grid& c, double* stc, int Rc, double* psb, double* bsb,
+                          cudaStream_t st);
+void launch_wide_mask(const Grid& c, int R, double* stc, uint8_t* cmask, double* minv3, cudaStream_t st);
+template <typename S, int R>
+void launch_wide_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc,
+                          typename WideLayout<S, R>::Q* sqrtd, cudaStream_t st_);
+template <typename T, typename S, int R>
+void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st);
+int wide_op_grid_blocks(const Grid& g);
+int wide_dense_assemble(const Grid& c, int R, const double* stencil, const uint8_t* cmask, double* A, int n,
+                        cudaStream_t st);
 void launch_galerkin_from_stencil(const Grid& f, const double* stencil_f, const Grid& c, double* stencil_c, cudaStream_t st);
 void launch_stencil_mask_and_diag(const Grid& c, double* stencil, uint8_t* cmask, double* minv3, cudaStream_t st);
 

@@ -1,0 +1,583 @@
+// Wide Galerkin levels: the coarse space with a smoothed prolongation.
+//
+// The robust hierarchy's coarse operators A_{l+1} = D P^T A_l P D use the
+// reference's trilinear P (core/multigrid.py:42-73).  On the transfer from a
+// Galerkin level l to l+1 this library can instead use the smoothed
+// prolongation of smoothed aggregation,
+//
+//     P_s = D_l (I - c_l D_l^-1 A_l) P,     c_l = (4/3) / lambda_l,
+//
+// lambda_l the padded power-iteration estimate of lambda_max(D_l^-1 A_l),
+// and A_{l+1} = D_{l+1} P_s^T A_l P_s D_{l+1}.  The smoothed basis functions
+// reach one fine node further, so the coarse operator couples each node with
+// the nodes up to two (in general: R) coarse spacings away: 125 blocks of
+// 3x3 per node instead of 27.  The transfers themselves need no new kernel
+// (vf_solver.cu): restriction P_s^T r = P^T (r - c A (Minv r)) and
+// prolongation x += P_s e = t - c Minv A t (t = P e) are the level's own
+// residual and sweep kernels.
+//
+// Set-up (FP64, once per set_material), for the transfer l -> l+1:
+//   k_prolong_blocks  the 3x3 blocks P_s[i][J] of every fine node i (AoS,
+//                     (Pr+1)^3 coarse slots per node; Pr = 1 + R_l when
+//                     smoothed, 1 for the trilinear P);
+//   k_rap_b           B = A_l P_s, (Pr+R_l+1)^3 coarse slots per fine node;
+//   k_rap_c           the diagonal and upper blocks of A_{l+1} = P_s^T B, one
+//                     CTA per coarse node, P_s[.][I] staged in shared memory;
+//   k_wide_mirror     the lower blocks as the neighbours' transposed upper
+//                     ones (the coarse operator is exactly symmetric);
+//   k_wide_mask_diag  D_{l+1} = DOFs with a positive diagonal, rows / columns
+//                     of the others zeroed, inverse diagonal.
+// Full stencils: st[(s*9 + 3r + c) * n + p], s = ((dz+R)*W + (dy+R))*W + (dx+R),
+// W = 2R+1: coupling of DOF r of node p with DOF c of node p + (dx,dy,dz).
+//
+// Apply (V-cycle): symmetric, diagonally scaled storage as on the 27-block
+// levels (vf_stencil.cu) -- the diagonal block (6 values) and the upper
+// blocks s > center (9 values each) of A~ = D^-1/2 A D^-1/2, FP16 for the
+// FP32 V-cycle, warp-chunked so a warp loads one 16-byte chunk of 32
+// consecutive nodes at once; the lower blocks are read transposed from the
+// neighbour that stores them.  One thread per padded node; the vector is read
+// through the L1 (the coarse levels are small).
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
+#include "vf_common.cuh"
+#include "vf_reduce.cuh"
+
+namespace vf {
+
+namespace {
+
+__host__ __device__ constexpr int wide_w(int R) { return 2 * R + 1; }
+__host__ __device__ constexpr int wide_nb(int R) { return (2 * R + 1) * (2 * R + 1) * (2 * R + 1); }
+
+// 1-D trilinear weight of a coarse node at fine offset d
+__device__ __forceinline__ double tw(int d) { return d == 0 ? 1.0 : ((d == 1 || d == -1) ? 0.5 : 0.0); }
+// ceil(v / 2) for any sign
+__device__ __forceinline__ int ceil_half(int v) { return v >= 0 ? (v + 1) / 2 : -((-v) / 2); }
+
+__device__ __forceinline__ bool inside(const Grid& g, int x, int y, int z) {
+  return x >= 0 && x <= g.lx && y >= 0 && y <= g.ly && z >= 0 && z <= g.lz;
+}
+
+__device__ __forceinline__ void interior_xyz(const Grid& g, long long t, int& x, int& y, int& z) {
+  const int nx1 = g.lx + 1, ny1 = g.ly + 1;
+  x = (int)(t % nx1);
+  const long long r = t / nx1;
+  y = (int)(r % ny1);
+  z = (int)(r / ny1);
+}
+
+__device__ __forceinline__ void decode(const Grid& g, int p, int& x, int& y, int& z) {
+  x = p % g.px - 1;
+  const int t = p / g.px;
+  y = t % g.py - 1;
+  z = t / g.py - 1;
+}
+
+inline int blocks_for(long long n, int threads, long long cap = 148LL * 64) {
+  long long b = (n + threads - 1) / threads;
+  if (b > cap) b = cap;
+  return (int)(b < 1 ? 1 : b);
+}
+
+// ---- set-up ----------------------------------------------------------------
+
+// P_s[i][J] per fine interior node i and coarse slot (ax, ay, az), J = jlo(i) + a,
+// jlo = ceil((i - Pr) / 2) per axis; psb[(p * NS + slot) * 9 + 3r + c].
+__global__ void k_prolong_blocks(Grid f, const double* __restrict__ stf, int Rf, const uint8_t* __restrict__ fm,
+                                 const double* __restrict__ minvf, const double* __restrict__ cdev, int Pr, Grid c,
+                                 double* __restrict__ psb) {
+  const int NA = Pr + 1, NS = NA * NA * NA;
+  const int W = wide_w(Rf), NB = wide_nb(Rf);
+  const long long nint = (long long)(f.lx + 1) * (f.ly + 1) * (f.lz + 1);
+  const double cc = cdev ? *cdev : 0.0;
+  const long long nf = f.n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nint * NS;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int slot = (int)(t % NS);
+    int x, y, z;
+    interior_xyz(f, t / NS, x, y, z);
+    const int p = f.idx(x, y, z);
+    const int ax = slot % NA, ay = (slot / NA) % NA, az = slot / (NA * NA);
+    const int Jx = ceil_half(x - Pr) + ax, Jy = ceil_half(y - Pr) + ay, Jz = ceil_half(z - Pr) + az;
+    double blk[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) blk[k] = 0.0;
+    if (inside(c, Jx, Jy, Jz)) {
+      const uint8_t m = fm[p];
+      const double w = tw(x - 2 * Jx) * tw(y - 2 * Jy) * tw(z - 2 * Jz);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        if ((m >> r) & 1) blk[4 * r] = w;
+      if (cc != 0.0 && m) {
+        // - c Minv_i sum_d A[i][d] w(i + d, J)
+        double acc[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+        for (int s = 0; s < NB; ++s) {
+          const int dx = s % W - Rf, dy = (s / W) % W - Rf, dz = s / (W * W) - Rf;
+          const double wk = tw(x + dx - 2 * Jx) * tw(y + dy - 2 * Jy) * tw(z + dz - 2 * Jz);
+          if (wk == 0.0 || !inside(f, x + dx, y + dy, z + dz)) continue;
+#pragma unroll
+          for (int k = 0; k < 9; ++k) acc[k] += wk * stf[((long long)s * 9 + k) * nf + p];
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const double mr = minvf[3LL * p + r];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) blk[3 * r + k] -= cc * mr * acc[3 * r + k];
+        }
+      }
+    }
+    double* out = psb + ((long long)p * NS + slot) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[k] = blk[k];
+  }
+}
+
+// B[k][J] = sum_d A[k][d] P_s[k + d][J] per fine interior node k and coarse
+// slot b, J = ceil((k - Pr - Rf) / 2) + b per axis; bsb[(p * NSB + b) * 9 + 3r + c].
+__global__ void k_rap_b(Grid f, const double* __restrict__ stf, int Rf, const double* __restrict__ psb, int Pr,
+                        Grid c, double* __restrict__ bsb) {
+  const int NA = Pr + 1, NS = NA * NA * NA;
+  const int NBA = Pr + Rf + 1, NSB = NBA * NBA * NBA;
+  const int W = wide_w(Rf), NB = wide_nb(Rf);
+  const long long nint = (long long)(f.lx + 1) * (f.ly + 1) * (f.lz + 1);
+  const long long nf = f.n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nint * NSB;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(t % NSB);
+    int x, y, z;
+    interior_xyz(f, t / NSB, x, y, z);
+    const int p = f.idx(x, y, z);
+    const int Jx = ceil_half(x - Pr - Rf) + b % NBA, Jy = ceil_half(y - Pr - Rf) + (b / NBA) % NBA;
+    const int Jz = ceil_half(z - Pr - Rf) + b / (NBA * NBA);
+    double acc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+    if (inside(c, Jx, Jy, Jz)) {
+      for (int s = 0; s < NB; ++s) {
+        const int ix = x + s % W - Rf, iy = y + (s / W) % W - Rf, iz = z + s / (W * W) - Rf;
+        if (!inside(f, ix, iy, iz)) continue;
+        const int ax = Jx - ceil_half(ix - Pr), ay = Jy - ceil_half(iy - Pr), az = Jz - ceil_half(iz - Pr);
+        if (ax < 0 || ax > Pr || ay < 0 || ay > Pr || az < 0 || az > Pr) continue;
+        const double* P = psb + ((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9;
+        double A[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) A[k] = stf[((long long)s * 9 + k) * nf + p];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc)
+            acc[3 * r + cc] += A[3 * r] * P[cc] + A[3 * r + 1] * P[3 + cc] + A[3 * r + 2] * P[6 + cc];
+      }
+    }
+    double* out = bsb + ((long long)p * NSB + b) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[k] = acc[k];
+  }
+}
+
+// A_{l+1}[I][I + D] = sum_i P_s[i][I]^T B[i][I + D] for the diagonal and the
+// upper offsets D of reach Rc: one CTA per coarse interior node I, P_s[.][I]
+// of the (2Pr+1)^3 fine nodes around 2I in shared memory, one thread per D.
+constexpr int kRapThreads = 64;
+__global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const double* __restrict__ psb, int Pr,
+                                                       const double* __restrict__ bsb, Grid c, int Rc,
+                                                       double* __restrict__ stc) {
+  extern __shared__ double sps[];   // [(2Pr+1)^3][9]
+  const int NA = Pr + 1, NS = NA * NA * NA;
+  const int NBA = Pr + Rf + 1, NSB = NBA * NBA * NBA;
+  const int WI = 2 * Pr + 1, NI = WI * WI * WI;
+  const int Wc = wide_w(Rc), NBc = wide_nb(Rc), SC = NBc / 2;
+  const long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
+  const long long nc = c.n;
+  for (long long node = blockIdx.x; node < nint; node += gridDim.x) {
+    int X, Y, Z;
+    interior_xyz(c, node, X, Y, Z);
+    const int pI = c.idx(X, Y, Z);
+    __syncthreads();   // the previous node's readers are done with sps
+    for (int e = threadIdx.x; e < NI * 9; e += blockDim.x) {
+      const int i = e / 9, k = e % 9;
+      const int ix = 2 * X + i % WI - Pr, iy = 2 * Y + (i / WI) % WI - Pr, iz = 2 * Z + i / (WI * WI) - Pr;
+      double v = 0.0;
+      if (inside(f, ix, iy, iz)) {
+        const int ax = X - ceil_half(ix - Pr), ay = Y - ceil_half(iy - Pr), az = Z - ceil_half(iz - Pr);
+        v = psb[((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9 + k];
+      }
+      sps[e] = v;
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u <= SC; u += blockDim.x) {
+      const int s = SC + u;   // center and upper offsets
+      const int Dx = s % Wc - Rc, Dy = (s / Wc) % Wc - Rc, Dz = s / (Wc * Wc) - Rc;
+      const int Jx = X + Dx, Jy = Y + Dy, Jz = Z + Dz;
+      double acc[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+      if (inside(c, Jx, Jy, Jz)) {
+        for (int i = 0; i < NI; ++i) {
+          const int ix = 2 * X + i % WI - Pr, iy = 2 * Y + (i / WI) % WI - Pr, iz = 2 * Z + i / (WI * WI) - Pr;
+          if (!inside(f, ix, iy, iz)) continue;
+          const int bx = Jx - ceil_half(ix - Pr - Rf), by = Jy - ceil_half(iy - Pr - Rf);
+          const int bz = Jz - ceil_half(iz - Pr - Rf);
+          if (bx < 0 || bx >= NBA || by < 0 || by >= NBA || bz < 0 || bz >= NBA) continue;
+          const double* P = sps + i * 9;
+          const double* B = bsb + ((long long)f.idx(ix, iy, iz) * NSB + (bz * NBA + by) * NBA + bx) * 9;
+          double Bv[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) Bv[k] = B[k];
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+              acc[3 * r + cc] += P[r] * Bv[cc] + P[3 + r] * Bv[3 + cc] + P[6 + r] * Bv[6 + cc];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * nc + pI] = acc[k];
+    }
+  }
+}
+
+// Lower offsets from the upper ones: block (s, p)[r][c] = block (NB-1-s, p + off(s))[c][r].
+__global__ void k_wide_mirror(Grid c, int R, double* __restrict__ stc) {
+  const int W = wide_w(R), NB = wide_nb(R), SC = NB / 2;
+  const long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
+  const long long nc = c.n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)SC * nint;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(t / nint);
+    int X, Y, Z;
+    interior_xyz(c, t % nint, X, Y, Z);
+    const int p = c.idx(X, Y, Z);
+    const int MX = X + s % W - R, MY = Y + (s / W) % W - R, MZ = Z + s / (W * W) - R;
+    const bool in = inside(c, MX, MY, MZ);
+    const long long q = in ? c.idx(MX, MY, MZ) : 0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+        stc[((long long)s * 9 + 3 * r + cc) * nc + p] =
+            in ? stc[((long long)(NB - 1 - s) * 9 + 3 * cc + r) * nc + q] : 0.0;
+  }
+}
+
+// D_{l+1} from the diagonal, rows / columns of the other DOFs zeroed, Minv.
+__global__ void k_wide_mask_from_diag(Grid c, int R, const double* __restrict__ st, uint8_t* __restrict__ cmask) {
+  const int SC = wide_nb(R) / 2;
+  const long long n = c.n;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < c.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(c, p, x, y, z);
+    uint8_t m = 0;
+    if (inside(c, x, y, z))
+      for (int r = 0; r < 3; ++r)
+        if (st[((long long)SC * 9 + 4 * r) * n + p] > 0.0) m |= (uint8_t)(1 << r);
+    cmask[p] = m;
+  }
+}
+
+__global__ void k_wide_apply_mask(Grid c, int R, double* __restrict__ st, const uint8_t* __restrict__ cmask,
+                                  double* __restrict__ minv3) {
+  const int W = wide_w(R), NB = wide_nb(R), SC = NB / 2;
+  const long long n = c.n;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < c.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(c, p, x, y, z);
+    const bool in = inside(c, x, y, z);
+    const uint8_t mp = cmask[p];
+    for (int s = 0; s < NB; ++s) {
+      const int qx = x + s % W - R, qy = y + (s / W) % W - R, qz = z + s / (W * W) - R;
+      const uint8_t mq = (in && inside(c, qx, qy, qz)) ? cmask[c.idx(qx, qy, qz)] : (uint8_t)0;
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc)
+          if (!(in && ((mp >> r) & 1) && ((mq >> cc) & 1))) st[((long long)s * 9 + 3 * r + cc) * n + p] = 0.0;
+    }
+    for (int r = 0; r < 3; ++r) {
+      const double d = st[((long long)SC * 9 + 4 * r) * n + p];
+      minv3[3LL * p + r] = ((mp >> r) & 1) && d != 0.0 ? 1.0 / d : 0.0;
+    }
+  }
+}
+
+// ---- scaled symmetric storage ----------------------------------------------
+template <typename S> __device__ __forceinline__ S to_s(double v);
+template <> __device__ __forceinline__ float to_s<float>(double v) { return (float)v; }
+template <> __device__ __forceinline__ double to_s<double>(double v) { return v; }
+template <> __device__ __forceinline__ __half to_s<__half>(double v) { return __double2half(v); }
+__host__ __device__ constexpr int dr(int k) { return k < 3 ? 0 : (k < 5 ? 1 : 2); }
+__host__ __device__ constexpr int dc(int k) { return k < 3 ? k : (k < 5 ? k - 2 : 2); }
+
+template <typename S, int R>
+__global__ void k_wide_compress(Grid g, const double* __restrict__ st, const uint8_t* __restrict__ mask,
+                                S* __restrict__ stc, typename WideLayout<S, R>::Q* __restrict__ sqrtd) {
+  using L = WideLayout<S, R>;
+  using Q = typename L::Q;
+  constexpr int W = 2 * R + 1, NB = W * W * W, SC = NB / 2;
+  const long long n = g.n;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(g, p, x, y, z);
+    const bool in = inside(g, x, y, z);
+    double sp[3];
+    for (int r = 0; r < 3; ++r) {
+      const double d = in ? st[((long long)SC * 9 + 4 * r) * n + p] : 0.0;
+      sp[r] = (in && ((mask[p] >> r) & 1) && d > 0.0) ? 1.0 / sqrt(d) : 0.0;
+      sqrtd[3LL * p + r] = (Q)(sp[r] > 0.0 ? 1.0 / sp[r] : 0.0);
+    }
+    for (int k = 0; k < 6; ++k)
+      stc[L::off(p, k)] = to_s<S>(in ? st[((long long)SC * 9 + 3 * dr(k) + dc(k)) * n + p] * sp[dr(k)] * sp[dc(k)]
+                                     : 0.0);
+    for (int u = 1; u <= SC; ++u) {
+      const int s = SC + u;
+      const int qx = x + s % W - R, qy = y + (s / W) % W - R, qz = z + s / (W * W) - R;
+      double sq[3] = {0.0, 0.0, 0.0};
+      if (in && inside(g, qx, qy, qz)) {
+        const int q = g.idx(qx, qy, qz);
+        for (int cc = 0; cc < 3; ++cc) {
+          const double d = st[((long long)SC * 9 + 4 * cc) * n + q];
+          sq[cc] = (((mask[q] >> cc) & 1) && d > 0.0) ? 1.0 / sqrt(d) : 0.0;
+        }
+      }
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc) {
+          const double v = (sp[r] != 0.0 && sq[cc] != 0.0) ? st[((long long)s * 9 + 3 * r + cc) * n + p] * sp[r] * sq[cc]
+                                                           : 0.0;
+          stc[L::off(p, 6 + 9 * (u - 1) + 3 * r + cc)] = to_s<S>(v);
+        }
+    }
+    for (int k = L::NV; k < L::NVP; ++k) stc[L::off(p, k)] = to_s<S>(0.0);
+  }
+}
+
+// One 16-byte chunk, unpacked to the accumulation type.
+template <typename S, typename A> struct WChunk;
+template <> struct WChunk<__half, float> {
+  float v[8];
+  __device__ __forceinline__ void load(const __half* base) {
+    const uint4 w = __ldg(reinterpret_cast<const uint4*>(base));
+    const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      __half2 h;
+      memcpy(&h, &ws[i], 4);
+      const float2 f = __half22float2(h);
+      v[2 * i] = f.x;
+      v[2 * i + 1] = f.y;
+    }
+  }
+};
+template <> struct WChunk<float, float> {
+  float v[4];
+  __device__ __forceinline__ void load(const float* base) {
+    const float4 w = __ldg(reinterpret_cast<const float4*>(base));
+    v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
+  }
+};
+template <> struct WChunk<double, double> {
+  double v[2];
+  __device__ __forceinline__ void load(const double* base) {
+    const double2 w = __ldg(reinterpret_cast<const double2*>(base));
+    v[0] = w.x; v[1] = w.y;
+  }
+};
+
+// y = mask(D^1/2 A~ D^1/2 u) with the epilogues of the other level kernels
+// (APPLY, SMOOTH with the Chebyshev step fields, RESID; a null rhs reads as
+// zero).  One thread per padded node (ghost and pad nodes idle).
+template <typename T, typename S, int R, int EPI>
+__global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __restrict__ stc,
+                                                 const T* __restrict__ sqd) {
+  using L = WideLayout<S, R>;
+  using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
+  constexpr int VPC = L::VPC, W = 2 * R + 1, NB = W * W * W, SC = NB / 2;
+  KrylovState* ks = a.ks;
+  if (ks && ks->done) return;
+  const T* __restrict__ u = (const T*)a.u;
+  T* out = (T*)a.out;
+  const T* b = (const T*)a.b;
+  const T* __restrict__ minv = (const T*)a.minv;
+  const uint8_t* __restrict__ mask = a.mask;
+  const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
+  const T* dprev = (const T*)a.dprev;
+  T* dout = (T*)a.dout;
+  const T c1 = a.c1_dev ? (T)(*a.c1_dev) : (T)0;
+  double dot = 0.0;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
+    int x, y, z;
+    decode(g, p, x, y, z);
+    if (!inside(g, x, y, z)) continue;
+    const uint8_t m = mask[p];
+    auto V = [&](int q, int c) -> A { return (A)__ldg(sqd + 3LL * q + c) * (A)__ldg(u + 3LL * q + c); };
+    A acc[3] = {(A)0, (A)0, (A)0};
+    if (m) {
+      const A v0 = V(p, 0), v1 = V(p, 1), v2 = V(p, 2);
+      // own chunks: diagonal block and the upper blocks (every index below is
+      // a compile-time constant once the loops are unrolled)
+      const S* own = stc + L::off(p, 0);
+      A vq[3] = {(A)0, (A)0, (A)0};
+#pragma unroll
+      for (int j = 0; j < L::NCH; ++j) {
+        WChunk<S, A> ch;
+        ch.load(own + (long long)j * 32 * VPC);
+#pragma unroll
+        for (int i = 0; i < VPC; ++i) {
+          const int k = j * VPC + i;
+          if (k < 6) {
+            const int r = dr(k), c = dc(k);
+            const A vc = c == 0 ? v0 : (c == 1 ? v1 : v2);
+            const A vr = r == 0 ? v0 : (r == 1 ? v1 : v2);
+            acc[r] += ch.v[i] * vc;
+            if (r != c) acc[c] += ch.v[i] * vr;
+          } else if (k < L::NV) {
+            const int s = SC + 1 + (k - 6) / 9, rc = (k - 6) % 9;
+            if (rc == 0) {
+              const int qx = x + s % W - R, qy = y + (s / W) % W - R, qz = z + s / (W * W) - R;
+              const bool qin = inside(g, qx, qy, qz);
+              const int qn = qin ? g.idx(qx, qy, qz) : 0;
+              vq[0] = qin ? V(qn, 0) : (A)0;
+              vq[1] = qin ? V(qn, 1) : (A)0;
+              vq[2] = qin ? V(qn, 2) : (A)0;
+            }
+            acc[rc / 3] += ch.v[i] * vq[rc % 3];
+          }
+        }
+      }
+      // lower blocks: upper block s of q = p - off(s), transposed
+#pragma unroll
+      for (int s = SC + 1; s < NB; ++s) {
+        const int qx = x - (s % W - R), qy = y - ((s / W) % W - R), qz = z - (s / (W * W) - R);
+        if (!inside(g, qx, qy, qz)) continue;
+        const int q = g.idx(qx, qy, qz);
+        const A w0 = V(q, 0), w1 = V(q, 1), w2 = V(q, 2);
+        const int k0 = 6 + 9 * (s - SC - 1);
+        const S* base = stc + L::off(q, 0);
+#pragma unroll
+        for (int j = k0 / VPC; j <= (k0 + 8) / VPC; ++j) {
+          WChunk<S, A> ch;
+          ch.load(base + (long long)j * 32 * VPC);
+#pragma unroll
+          for (int i = 0; i < VPC; ++i) {
+            const int k = j * VPC + i;
+            if (k >= k0 && k < k0 + 9) {
+              const int r = (k - k0) / 3, c = (k - k0) % 3;
+              acc[c] += ch.v[i] * (r == 0 ? w0 : (r == 1 ? w1 : w2));
+            }
+          }
+        }
+      }
+    }
+    const long long p3 = 3LL * p;
+    const T k0 = (m & 1) ? (T)(acc[0] * (A)sqd[p3]) : (T)0;
+    const T k1 = (m & 2) ? (T)(acc[1] * (A)sqd[p3 + 1]) : (T)0;
+    const T k2 = (m & 4) ? (T)(acc[2] * (A)sqd[p3 + 2]) : (T)0;
+    const T b0 = b ? b[p3] : (T)0, b1 = b ? b[p3 + 1] : (T)0, b2 = b ? b[p3 + 2] : (T)0;
+    if (EPI == EPI_APPLY) {
+      out[p3] = k0; out[p3 + 1] = k1; out[p3 + 2] = k2;
+      if (a.dot_partials)
+        dot += (double)u[p3] * (double)k0 + (double)u[p3 + 1] * (double)k1 + (double)u[p3 + 2] * (double)k2;
+    } else if (EPI == EPI_SMOOTH) {
+      const T u0 = u[p3], u1 = u[p3 + 1], u2 = u[p3 + 2];
+      T o0 = u0 + ((m & 1) ? w * (minv[p3] * (b0 - k0)) : (T)0);
+      T o1 = u1 + ((m & 2) ? w * (minv[p3 + 1] * (b1 - k1)) : (T)0);
+      T o2 = u2 + ((m & 4) ? w * (minv[p3 + 2] * (b2 - k2)) : (T)0);
+      if (dprev) { o0 += c1 * dprev[p3]; o1 += c1 * dprev[p3 + 1]; o2 += c1 * dprev[p3 + 2]; }
+      out[p3] = o0; out[p3 + 1] = o1; out[p3 + 2] = o2;
+      if (dout) { dout[p3] = o0 - u0; dout[p3 + 1] = o1 - u1; dout[p3 + 2] = o2 - u2; }
+    } else {
+      out[p3] = b0 - k0; out[p3 + 1] = b1 - k1; out[p3 + 2] = b2 - k2;
+    }
+  }
+  if (EPI == EPI_APPLY && a.dot_partials && ks) reduce_and_finalize(dot, a.dot_partials, ks, a.dot_slot, nullptr);
+}
+
+// Dense row-major A of a reach-R level (reference node order, DOF 3*node + c),
+// identity rows on non-free DOFs.
+__global__ void k_wide_dense_assemble(Grid c, int R, const double* __restrict__ st, const uint8_t* __restrict__ cm,
+                                      double* __restrict__ A, int n) {
+  const int W = wide_w(R), NB = wide_nb(R), SC = NB / 2;
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1;
+  const long long nint = (long long)nx1 * ny1 * (c.lz + 1);
+  const long long ns = c.n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nint * NB;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / NB), s = (int)(t % NB);
+    int x, y, z;
+    interior_xyz(c, r, x, y, z);
+    const int X = x + s % W - R, Y = y + (s / W) % W - R, Z = z + s / (W * W) - R;
+    if (!inside(c, X, Y, Z)) continue;
+    const int q = X + nx1 * (Y + ny1 * Z);
+    const int p = c.idx(x, y, z);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        A[(long long)(3 * r + i) * n + 3 * q + j] = st[((long long)s * 9 + 3 * i + j) * ns + p];
+    if (s == SC) {
+      const uint8_t m = cm[p];
+      for (int i = 0; i < 3; ++i)
+        if (!((m >> i) & 1)) A[(long long)(3 * r + i) * n + 3 * r + i] = 1.0;
+    }
+  }
+}
+
+}  // namespace
+
+// ---- launchers ---------------------------------------------------------------
+size_t wide_prolong_count(const Grid& f, int Pr) { return (size_t)f.n * (Pr + 1) * (Pr + 1) * (Pr + 1) * 9; }
+size_t wide_rapb_count(const Grid& f, int Pr, int Rf) {
+  const size_t a = (size_t)(Pr + Rf + 1);
+  return (size_t)f.n * a * a * a * 9;
+}
+
+void launch_wide_galerkin(const Grid& f, const double* stf, int Rf, const uint8_t* fmask, const double* minvf,
+                          const double* cdev, int Pr, const Grid& c, double* stc, int Rc, double* psb, double* bsb,
+                          cudaStream_t st) {
+  const long long nintf = (long long)(f.lx + 1) * (f.ly + 1) * (f.lz + 1);
+  const long long nintc = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
+  const int NS = (Pr + 1) * (Pr + 1) * (Pr + 1), NBA = Pr + Rf + 1;
+  launch_k(k_prolong_blocks, blocks_for(nintf * NS, 128), 128, 0, st, f, stf, Rf, fmask, minvf, cdev, Pr, c, psb);
+  launch_k(k_rap_b, blocks_for(nintf * NBA * NBA * NBA, 128), 128, 0, st, f, stf, Rf, psb, Pr, c, bsb);
+  const int WI = 2 * Pr + 1;
+  const size_t smem = sizeof(double) * WI * WI * WI * 9;
+  launch_k(k_rap_c, (int)std::min<long long>(nintc, 148LL * 256), kRapThreads, smem, st, f, Rf, psb, Pr, bsb, c, Rc,
+           stc);
+  launch_k(k_wide_mirror, blocks_for((long long)(wide_nb(Rc) / 2) * nintc, 128), 128, 0, st, c, Rc, stc);
+}
+
+void launch_wide_mask(const Grid& c, int R, double* stc, uint8_t* cmask, double* minv3, cudaStream_t st) {
+  launch_k(k_wide_mask_from_diag, blocks_for(c.n, 256), 256, 0, st, c, R, stc, cmask);
+  launch_k(k_wide_apply_mask, blocks_for(c.n, 128), 128, 0, st, c, R, stc, cmask, minv3);
+}
+
+template <typename S, int R>
+void launch_wide_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc,
+                          typename WideLayout<S, R>::Q* sqrtd, cudaStream_t st_) {
+  launch_k(k_wide_compress<S, R>, blocks_for(g.n, 128), 128, 0, st_, g, st, mask, stc, sqrtd);
+}
+template void launch_wide_compress<__half, 2>(const Grid&, const double*, const uint8_t*, __half*, float*, cudaStream_t);
+template void launch_wide_compress<float, 2>(const Grid&, const double*, const uint8_t*, float*, float*, cudaStream_t);
+template void launch_wide_compress<double, 2>(const Grid&, const double*, const uint8_t*, double*, double*, cudaStream_t);
+
+template <typename T, typename S, int R>
+void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
+  const int blocks = blocks_for(g.n, 128, 148LL * 16);
+  if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else launch_k(k_wide_op<T, S, R, EPI_RESID>, blocks, 128, 0, st, g, a, stc, sqrtd);
+}
+template void launch_wide_op<float, __half, 2>(const Grid&, int, const OpArgs&, const __half*, const float*, cudaStream_t);
+template void launch_wide_op<float, float, 2>(const Grid&, int, const OpArgs&, const float*, const float*, cudaStream_t);
+template void launch_wide_op<double, double, 2>(const Grid&, int, const OpArgs&, const double*, const double*,
+                                                cudaStream_t);
+int wide_op_grid_blocks(const Grid& g) { return blocks_for(g.n, 128, 148LL * 16); }
+
+int wide_dense_assemble(const Grid& c, int R, const double* stencil, const uint8_t* cmask, double* A, int n,
+                        cudaStream_t st) {
+  cudaMemsetAsync(A, 0, sizeof(double) * (size_t)n * n, st);
+  const long long work = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1) * wide_nb(R);
+  launch_k(k_wide_dense_assemble, blocks_for(work, 256, 148LL * 256), 256, 0, st, c, R, stencil, cmask, A, n);
+  return 0;
+}
+
+}  // namespace vf
