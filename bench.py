@@ -427,7 +427,7 @@ def run_b200(args):
                         n_smooth=args.n_smooth)
 
     fkw = dict(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk, mixed_mode=args.mixed_mode,
-               smoother=args.smoother)
+               smoother=args.smoother, smoothed_transfers=args.smoothed_transfers)
     if args.inner_tol is not None:
         fkw["inner_tol"] = args.inner_tol
     fast = solver(SolverOptions.fast(**fkw))
@@ -538,7 +538,8 @@ def run_b200(args):
     ref_fields = None
     u_plain = None
     if not args.no_plain or (K == 1 and not args.no_errors):
-        ps = solver(SolverOptions.robust(device=local, check_every=args.check_every, smoother=args.smoother))
+        ps = solver(SolverOptions.robust(device=local, check_every=args.check_every, smoother=args.smoother,
+                                         smoothed_transfers=args.smoothed_transfers))
         L.vf_get_stream(ps._h, ctypes.byref(stream_ptr))
         ext_plain = torch.cuda.ExternalStream(stream_ptr.value)
         ext_save = ext
@@ -721,6 +722,8 @@ def main():
     ap.add_argument("--mixed-mode", choices=("outer64", "reliable", "restart"), default="outer64")
     ap.add_argument("--smoother", choices=("jacobi", "chebyshev"), default="chebyshev",
                     help="V-cycle smoothing of every arm (plain FP64, mixed, learned)")
+    ap.add_argument("--smoothed-transfers", type=int, default=0,
+                    help="bitmask of transfers l -> l+1 with the smoothed prolongation (2: level 1 -> 2)")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed: residual reduction between FP64 corrections (solver default if unset)")
     args = ap.parse_args()

@@ -122,7 +122,14 @@ typedef struct vf_options {
                               lambda the VF_OMEGA_AUTO estimate of lambda_max(D^-1 A_l); needs
                               VF_OMEGA_AUTO, a modal fine kernel and symmetric coarse storage */
   int32_t cheb_ratio;      /* VF_SMOOTH_CHEBYSHEV: lambda_max / lower end of the interval (30) */
-  int32_t reserved[3];
+  int32_t smoothed_transfers; /* bit l set: the transfer from Galerkin level l to l+1 uses the
+                              smoothed prolongation P_s = D (I - (4/3) D^-1 A_l / lambda_l) P
+                              (P the reference's trilinear P, multigrid.py:42-73; lambda_l the
+                              VF_OMEGA_AUTO estimate), and A_{l+1} = P_s^T A_l P_s couples nodes
+                              two coarse spacings apart (125 blocks).  Bit 1 only (level 1 -> 2):
+                              needs VF_COARSE_GALERKIN, VF_OMEGA_AUTO and symmetric storage; 0 =
+                              trilinear everywhere (default) */
+  int32_t reserved[2];
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };

@@ -82,14 +82,19 @@ def _lambda_max(A, dinv, free, iters=30, seed=0):
 
 
 def smoothed_hierarchy(nx, ny, nz, E, fixed_dofs, nu=0.3, min_elems=4, max_levels=6, lam=None, mu=None,
-                       omega=4.0 / 3.0, pad=1.1):
+                       omega=4.0 / 3.0, pad=1.1, smoothed=None, lams=None):
     """[(A_l, free_l)], [P_l]: Galerkin levels with smoothed prolongations.
 
     P_l = D_l (P - (omega / lambda_l) D_l^-1 A_l P) (one damped-Jacobi step
     applied to the trilinear P, lambda_l the padded lambda_max(D^-1 A_l)),
     A_{l+1} = D_{l+1} P_l^T A_l P_l D_{l+1}; the coarse stencils reach two
     nodes out (125 blocks) instead of one.  Not a reference algorithm: the
-    candidate coarse space the device hierarchy is measured against."""
+    coarse space of the device hierarchy's smoothed transfers
+    (vf_options.smoothed_transfers), checked against this.
+
+    smoothed: the transfers l -> l+1 to smooth (None: all; the others use the
+    trilinear P = D_l P); lams: {l: padded lambda_l} to use instead of this
+    module's own power-iteration estimate (the device's, for entrywise checks)."""
     dims = level_dims(nx, ny, nz, min_elems, max_levels)
     K = fine_matrix(nx, ny, nz, E, nu, lam, mu)
     free = np.ones(K.shape[0], dtype=bool)
@@ -99,11 +104,14 @@ def smoothed_hierarchy(nx, ny, nz, E, fixed_dofs, nu=0.3, min_elems=4, max_level
     Ps = []
     for li in range(1, len(dims)):
         A, fr = out[-1]
-        d = A.diagonal()
-        dinv = np.where(fr & (d > 0), 1.0 / np.where(d > 0, d, 1.0), 0.0)
-        lmax = pad * _lambda_max(A, dinv, fr)
         P = prolong_matrix(dims[li - 1], dims[li])
-        Psm = (sp.diags(fr.astype(float)) @ (P - (omega / lmax) * (sp.diags(dinv) @ (A @ P)))).tocsr()
+        if smoothed is None or (li - 1) in smoothed:
+            d = A.diagonal()
+            dinv = np.where(fr & (d > 0), 1.0 / np.where(d > 0, d, 1.0), 0.0)
+            lmax = lams[li - 1] if lams and (li - 1) in lams else pad * _lambda_max(A, dinv, fr)
+            Psm = (sp.diags(fr.astype(float)) @ (P - (omega / lmax) * (sp.diags(dinv) @ (A @ P)))).tocsr()
+        else:
+            Psm = (sp.diags(fr.astype(float)) @ P).tocsr()
         Ac = (Psm.T @ A @ Psm).tocsr()
         fc = Ac.diagonal() > 0
         Dc = sp.diags(fc.astype(float))

@@ -228,6 +228,8 @@ void launch_wide_galerkin(const Grid& f, const double* stf, int Rf, const uint8_
                           const double* cdev, int Pr, const Grid& c, double* stc, int Rc, double* psb, double* bsb,
                           cudaStream_t st);
 void launch_wide_mask(const Grid& c, int R, double* stc, uint8_t* cmask, double* minv3, cudaStream_t st);
+// coef = (4/3) / lambda (0 when lambda <= 0), on the device
+void launch_smoothing_coef(const double* lambda, double* coef, cudaStream_t st);
 template <typename S, int R>
 void launch_wide_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc,
                           typename WideLayout<S, R>::Q* sqrtd, cudaStream_t st_);

@@ -80,10 +80,14 @@ struct Level {
   double* E64 = nullptr; double* mu64 = nullptr; double* minv64 = nullptr; double* st64 = nullptr;
   float* E32 = nullptr; float* mu32 = nullptr; float* minv32 = nullptr; float* st32 = nullptr;
   // symmetric scaled stencils (Galerkin levels): 123 values per node + sqrt(diag)
+  // (reach 2: WideLayout, 568 values per node)
   double* sym64 = nullptr; double* sq64 = nullptr;
   float* sym32 = nullptr; __half* sym16 = nullptr; float* sq32 = nullptr;
-  double* w64[4] = {nullptr, nullptr, nullptr, nullptr};   // x, tmp, resid, rhs
-  float* w32[4] = {nullptr, nullptr, nullptr, nullptr};
+  int reach = 1;             // Galerkin stencil reach: 1 (27 blocks) or 2 (125 blocks, vf_wide.cu)
+  bool smooth_down = false;  // the transfer to the next level uses the smoothed prolongation
+  // x, tmp, resid, rhs, and a second temporary for the smoothed restriction
+  double* w64[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float* w32[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 template <typename T> struct Sel;
@@ -164,6 +168,11 @@ struct vf_solver {
   double* d_omega = nullptr;    // damping per level (read by the smoothers)
   double* d_lambda = nullptr;   // lambda_max(D^-1 A_l) estimates (VF_OMEGA_AUTO)
   double* d_cheb = nullptr;     // Chebyshev steps per level: [level][step][c1, c2]
+  double* d_spc = nullptr;      // smoothed transfers: c_l = (4/3) / lambda_l per level
+  double* d_one = nullptr;      // the constant 1 (step field of the smoothed prolongation)
+  double* d_psb = nullptr;      // set-up scratch of the wide Galerkin products (vf_wide.cu)
+  double* d_bsb = nullptr;
+  std::vector<char> lam_done;   // lambda_l already estimated during this set-up
   std::vector<double> h_omega, h_lambda;
   // block right-hand sides: solvers that share this one's operator data and
   // own their vectors, Krylov state, stream and graphs (vf_solve_block)
@@ -234,12 +243,18 @@ int nlev(const vf_solver* s) { return use_mg(s) ? (int)s->L.size() : 1; }
 // ---------------------------------------------------------------------------
 template <typename T> void level_sym_op(vf_solver* s, Level& l, int epi, const OpArgs& a);
 template <> void level_sym_op<double>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
-  launch_stencil_sym_op<double, double>(l.g, epi, a, l.sym64, l.sq64, l.szchunk, s->st);
+  if (l.reach == 2) launch_wide_op<double, double, 2>(l.g, epi, a, l.sym64, l.sq64, s->st);
+  else launch_stencil_sym_op<double, double>(l.g, epi, a, l.sym64, l.sq64, l.szchunk, s->st);
 }
 template <> void level_sym_op<float>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
-  if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
+  if (l.reach == 2) {
+    if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) launch_wide_op<float, __half, 2>(l.g, epi, a, l.sym16, l.sq32, s->st);
+    else launch_wide_op<float, float, 2>(l.g, epi, a, l.sym32, l.sq32, s->st);
+  } else if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) {
     launch_stencil_sym_op<float, __half>(l.g, epi, a, l.sym16, l.sq32, l.szchunk, s->st);
-  else launch_stencil_sym_op<float, float>(l.g, epi, a, l.sym32, l.sq32, l.szchunk, s->st);
+  } else {
+    launch_stencil_sym_op<float, float>(l.g, epi, a, l.sym32, l.sq32, l.szchunk, s->st);
+  }
 }
 
 int auto_zchunk(const Grid& g, int requested);
@@ -355,6 +370,47 @@ void smooth(vf_solver* s, int li, T* x, T* tmp, const T* b, int sweeps, bool fro
   if (cur != x) launch_copy_vec<T>(l.g, cur, x, ks, s->st);
 }
 
+// Transfers between level li and li + 1.  Trilinear: r_c = P^T r, x += P e.
+// Smoothed (l.smooth_down): with P_s = D (I - c Minv A) P,
+//   r_c = P_s^T r = P^T (r - c A (Minv r))   (r masked),
+//   x  += P_s e   = t - c Minv A t + x,  t = P e,
+// i.e. a from-zero sweep, a residual and the trilinear restriction; and the
+// trilinear prolongation into a temporary followed by one sweep of the level
+// operator with a zero rhs, weight c and the step field (dprev = x, c1 = 1).
+// Temporaries: w[1] and w[4] of level li (free outside the smoothing).
+template <typename T>
+void restrict_level(vf_solver* s, int li, const T* r, T* rc, KrylovState* ks) {
+  Level& l = s->L[li];
+  Level& c = s->L[li + 1];
+  if (!l.smooth_down) {
+    launch_restrict<T>(l.g, r, c.g, c.mask, rc, ks, s->st);
+    return;
+  }
+  T* z = Sel<T>::w(l, 1);
+  T* rs = Sel<T>::w(l, 4);
+  launch_jacobi_from_zero<T>(l.g, r, Sel<T>::minv(l), l.mask, 0.0, s->d_spc + li, z, ks, s->st);
+  level_op<T>(s, li, EPI_RESID, z, rs, r, ks, nullptr, 0);
+  launch_restrict<T>(l.g, rs, c.g, c.mask, rc, ks, s->st);
+}
+
+template <typename T>
+void prolong_level(vf_solver* s, int li, const T* ec, T* x, KrylovState* ks) {
+  Level& l = s->L[li];
+  Level& c = s->L[li + 1];
+  if (!l.smooth_down) {
+    launch_prolong_add<T>(c.g, ec, l.g, l.mask, x, ks, s->st);
+    return;
+  }
+  T* t = Sel<T>::w(l, 1);
+  cudaMemsetAsync(t, 0, sizeof(T) * 3 * (size_t)l.g.n, s->st);
+  launch_prolong_add<T>(c.g, ec, l.g, l.mask, t, ks, s->st);
+  SweepStep st;
+  st.omega_dev = s->d_spc + li;
+  st.c1_dev = s->d_one;
+  st.dprev = x;
+  level_op<T>(s, li, EPI_SMOOTH, t, x, nullptr, ks, nullptr, 0, &st);
+}
+
 template <typename T>
 void coarse_solve(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
   Level& l = s->L[li];
@@ -381,9 +437,9 @@ void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks, int dot_slo
   if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, s->o.n_smooth, true, ks, -1);
   else smooth<T>(s, li, x, tmp, b, s->o.n_smooth, true, ks);
   level_op<T>(s, li, EPI_RESID, x, res, b, ks, nullptr, 0);
-  launch_restrict<T>(l.g, res, c.g, c.mask, Sel<T>::w(c, 3), ks, s->st);
+  restrict_level<T>(s, li, res, Sel<T>::w(c, 3), ks);
   vcycle<T>(s, li + 1, Sel<T>::w(c, 3), Sel<T>::w(c, 0), ks);
-  launch_prolong_add<T>(c.g, Sel<T>::w(c, 0), l.g, l.mask, x, ks, s->st);
+  prolong_level<T>(s, li, Sel<T>::w(c, 0), x, ks);
   // (res is free again: the post-smoothing's first update goes there)
   if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, s->o.n_smooth, false, ks, dot_slot);
   else smooth<T>(s, li, x, tmp, b, s->o.n_smooth, false, ks, dot_slot);
@@ -622,7 +678,22 @@ int build_levels(vf_solver* s) {
       return VF_ERR_ARG;
     }
     l.galerkin = (i > 0 && s->o.coarse_op == VF_COARSE_GALERKIN);
+    // stencil reach: level 1 is built from the hex8 level (27 blocks); a
+    // level below a smoothed transfer reaches (2 Pr + R_fine) / 2 coarse
+    // spacings with Pr = 1 + R_fine (smoothed) or 1 (trilinear)
+    if (i >= 2 && l.galerkin) {
+      const Level& f = s->L[i - 1];
+      const int pr = f.smooth_down ? 1 + f.reach : 1;
+      l.reach = (2 * pr + f.reach) / 2;
+    }
+    l.smooth_down = l.galerkin && i + 1 < dims.size() && ((s->o.smoothed_transfers >> i) & 1);
+    if (l.reach > 2) {
+      s->err = "smoothed transfers give level " + std::to_string(i) + " a stencil reach of " +
+               std::to_string(l.reach) + " (at most 2 supported)";
+      return VF_ERR_UNSUPPORTED;
+    }
     const size_t n = l.g.n;
+    const size_t nblk = (size_t)(2 * l.reach + 1) * (2 * l.reach + 1) * (2 * l.reach + 1);
     VF_ALLOC(l.mask, n);
     VF_ALLOC(l.minv64, 3 * n);
     VF_ALLOC(l.minv32, 3 * n);
@@ -630,19 +701,45 @@ int build_levels(vf_solver* s) {
       VF_ALLOC(l.E64, n);
       VF_ALLOC(l.E32, n);
     } else {
-      VF_ALLOC(l.st64, 243 * n);
+      VF_ALLOC(l.st64, 9 * nblk * n);
       if (s->o.coarse_storage == VF_STENCIL_FULL) VF_ALLOC(l.st32, 243 * n);
       else {
-        VF_ALLOC(l.sym64, SymLayout<double>::count(n));
+        using W64 = WideLayout<double, 2>;
+        using W32 = WideLayout<float, 2>;
+        using W16 = WideLayout<__half, 2>;
+        const bool wide = l.reach == 2;
+        const size_t c64 = wide ? W64::count(n) : SymLayout<double>::count(n);
+        const size_t c32 = wide ? W32::count(n) : SymLayout<float>::count(n);
+        const size_t c16 = wide ? W16::count(n) : SymLayout<__half>::count(n);
+        VF_ALLOC(l.sym64, c64);
         VF_ALLOC(l.sq64, 3 * n);
         VF_ALLOC(l.sq32, 3 * n);
-        if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) VF_ALLOC(l.sym16, SymLayout<__half>::count(n));
-        else VF_ALLOC(l.sym32, SymLayout<float>::count(n));
+        if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) VF_ALLOC(l.sym16, c16);
+        else VF_ALLOC(l.sym32, c32);
       }
     }
     for (int k = 0; k < 4; ++k) {
       VF_ALLOC(l.w64[k], 3 * n);
       VF_ALLOC(l.w32[k], 3 * n);
+    }
+    if (l.smooth_down) {
+      VF_ALLOC(l.w64[4], 3 * n);
+      VF_ALLOC(l.w32[4], 3 * n);
+    }
+  }
+  // set-up scratch of the wide Galerkin products
+  {
+    size_t np = 0, nb = 0;
+    for (size_t i = 2; i < s->L.size(); ++i) {
+      const Level& f = s->L[i - 1];
+      if (s->L[i].reach < 2) continue;
+      const int pr = f.smooth_down ? 1 + f.reach : 1;
+      np = std::max(np, wide_prolong_count(f.g, pr));
+      nb = std::max(nb, wide_rapb_count(f.g, pr, f.reach));
+    }
+    if (np) {
+      VF_ALLOC(s->d_psb, np);
+      VF_ALLOC(s->d_bsb, nb);
     }
   }
   const Grid& g0 = s->L[0].g;
@@ -681,6 +778,13 @@ int build_levels(vf_solver* s) {
   VF_ALLOC(s->d_err, 1);
   VF_ALLOC(s->d_lambda, 16);
   VF_ALLOC(s->d_cheb, 16 * 2 * 2);
+  VF_ALLOC(s->d_spc, 16);
+  VF_ALLOC(s->d_one, 1);
+  {
+    const double one = 1.0;
+    VF_TRY(cudaMemcpyAsync(s->d_one, &one, sizeof(double), cudaMemcpyHostToDevice, s->st));
+    VF_TRY(cudaStreamSynchronize(s->st));
+  }
   VF_TRY(cudaMallocHost(&s->h_ks, sizeof(KrylovState)));
   memset(s->h_ks, 0, sizeof(KrylovState));
   return ensure_hist(s, 4096);
@@ -716,7 +820,7 @@ int autotune_levels(vf_solver* s) {
   } ev{t0, t1};
   for (size_t li = 0; li < s->L.size(); ++li) {
     Level& l = s->L[li];
-    const bool stencil = l.galerkin && s->o.coarse_storage != VF_STENCIL_FULL;
+    const bool stencil = l.galerkin && s->o.coarse_storage != VF_STENCIL_FULL && l.reach == 1;
     const bool modal = !l.galerkin && s->o.fine_kernel == VF_FINE_MODAL;
     if (!stencil && !modal) continue;
     if (modal && s->o.modal_zchunk != 0) continue;   // fixed by the caller
@@ -836,6 +940,26 @@ int build_masks(vf_solver* s) {
 // stays contractive on every level whatever the contrast (plain omega = 0.6
 // is divergent on high modes when lambda_max(D^-1 A) > 3.3, as on noise
 // geometry with void elements).
+// lambda_max(D^-1 A_li) by power iteration (x <- D^-1 A x / ||.||) into
+// d_lambda[li] (padded by 1.1), omega_li into d_omega[li]; in FP32 on the
+// V-cycle's FP32 operators (half-precision scaled stencils on Galerkin
+// levels): lambda is needed to a few percent, and the FP32 sweeps cost half
+// the FP64 ones.
+int power_level(vf_solver* s, int li) {
+  init_ks(*s->h_ks, 1.0, 1, 0, 0, 1.0);
+  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+  Level& l = s->L[li];
+  launch_power_init<float>(l.g, l.w32[0], l.mask, s->st);
+  for (int k = 0; k < std::max(2, s->o.power_iters); ++k) {
+    level_op<float>(s, li, EPI_APPLY, l.w32[0], l.w32[1], nullptr, nullptr, nullptr, 0);
+    launch_power_scale<float>(l.g, l.w32[1], l.minv32, s->d_partials, s->ks, s->st);
+    launch_power_normalize<float>(l.g, l.w32[1], l.w32[0], s->ks, s->st);
+  }
+  launch_power_omega(s->ks, s->o.omega_rel, 1.1, s->d_omega + li, s->d_lambda + li, s->st);
+  VF_CHECK_LAUNCH();
+  return VF_OK;
+}
+
 int set_level_omegas(vf_solver* s) {
   const int nl = nlev(s);
   s->h_omega.assign(nl, s->o.omega);
@@ -844,20 +968,10 @@ int set_level_omegas(vf_solver* s) {
     VF_TRY(cudaMemcpyAsync(s->d_omega, s->h_omega.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, s->st));
     return VF_OK;
   }
-  init_ks(*s->h_ks, 1.0, 1, 0, 0, 1.0);
-  VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
-  // in FP32 on the V-cycle's FP32 operators (half-precision scaled stencils
-  // on Galerkin levels): lambda is needed to a few percent (it is padded by
-  // the 1.1 safety factor), and the FP32 sweeps cost half the FP64 ones
   for (int li = 0; li < nl; ++li) {
-    Level& l = s->L[li];
-    launch_power_init<float>(l.g, l.w32[0], l.mask, s->st);
-    for (int k = 0; k < std::max(2, s->o.power_iters); ++k) {
-      level_op<float>(s, li, EPI_APPLY, l.w32[0], l.w32[1], nullptr, nullptr, nullptr, 0);
-      launch_power_scale<float>(l.g, l.w32[1], l.minv32, s->d_partials, s->ks, s->st);
-      launch_power_normalize<float>(l.g, l.w32[1], l.w32[0], s->ks, s->st);
-    }
-    launch_power_omega(s->ks, s->o.omega_rel, 1.1, s->d_omega + li, s->d_lambda + li, s->st);
+    if (li < (int)s->lam_done.size() && s->lam_done[li]) continue;   // estimated while the hierarchy was built
+    int rc = power_level(s, li);
+    if (rc) return rc;
   }
   if (s->o.smoother == VF_SMOOTH_CHEBYSHEV) launch_cheb_coefs(s->d_lambda, nl, s->o.cheb_ratio, s->d_cheb, s->st);
   VF_CHECK_LAUNCH();
@@ -897,7 +1011,8 @@ int build_dense_coarsest(vf_solver* s) {
     launch_stencil_from_elements(lc.g, lc.E64, s->lame ? lc.mu64 : nullptr, lc.mask, st,
                                  s->lame ? s->d_Ktab_lame : s->d_Ktab, s->lame ? 1 : 0, sd);
   }
-  dense_assemble(lc.g, st, lc.mask, s->d_Ainv, n, sd);
+  if (lc.reach > 1) wide_dense_assemble(lc.g, lc.reach, st, lc.mask, s->d_Ainv, n, sd);
+  else dense_assemble(lc.g, st, lc.mask, s->d_Ainv, n, sd);
   dense_cholesky_inverse(s->d_Ainv, s->d_dense_work, n, s->d_info, sd);
   VF_CHECK_LAUNCH();
   int info = 0;
@@ -1049,6 +1164,13 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
                    "and symmetric coarse storage";
     return VF_ERR_ARG;
   }
+  if (o.smoothed_transfers != 0 &&
+      ((o.smoothed_transfers & ~2) != 0 || o.method != VF_METHOD_MG || o.coarse_op != VF_COARSE_GALERKIN ||
+       o.omega_mode != VF_OMEGA_AUTO || o.coarse_storage == VF_STENCIL_FULL)) {
+    g_last_error = "smoothed transfers: bit 1 (level 1 -> 2) only, with the MG method, Galerkin coarse "
+                   "operators, omega_mode AUTO and symmetric coarse storage";
+    return VF_ERR_ARG;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) { g_last_error = "no CUDA device"; return VF_ERR_NO_DEVICE; }
   if (o.device < 0 || o.device >= ndev) { g_last_error = "device ordinal out of range"; return VF_ERR_ARG; }
@@ -1167,11 +1289,53 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
   const double dL = lame ? s->tab[576] : s->tab[0];
   const double dM = lame ? s->tab[1152] : 0.0;
   launch_inv_diag_fine<double>(g0, l0.E64, lame ? l0.mu64 : nullptr, dL, dM, l0.minv64, s->st);
+  // A level's FP32 copies / compressed stencils: built as soon as the level is
+  // complete when a smoothed transfer needs its lambda, else after the loop.
+  std::vector<char> finalized(s->L.size(), 0);
+  s->lam_done.assign(s->L.size(), 0);
+  auto finalize = [&](size_t i) {
+    Level& l = s->L[i];
+    const long long n = l.g.n;
+    if (!l.galerkin) {
+      launch_convert<double, float>(l.E64, l.E32, n, s->st);
+      if (lame) launch_convert<double, float>(l.mu64, l.mu32, n, s->st);
+    } else if (s->o.coarse_storage == VF_STENCIL_FULL) {
+      launch_convert<double, float>(l.st64, l.st32, 243 * n, s->st);
+    } else if (l.reach == 2) {
+      launch_wide_compress<double, 2>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+      if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
+        launch_wide_compress<__half, 2>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
+      else
+        launch_wide_compress<float, 2>(l.g, l.st64, l.mask, l.sym32, l.sq32, s->st);
+    } else {
+      launch_stencil_compress<double>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+      if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
+        launch_stencil_compress<__half>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
+      else
+        launch_stencil_compress<float>(l.g, l.st64, l.mask, l.sym32, l.sq32, s->st);
+    }
+    launch_convert<double, float>(l.minv64, l.minv32, 3 * n, s->st);
+    finalized[i] = 1;
+  };
   if (use_mg(s)) {
     for (size_t i = 1; i < s->L.size(); ++i) {
       Level& f = s->L[i - 1];
       Level& c = s->L[i];
-      if (!c.galerkin) {
+      if (c.galerkin && c.reach == 2) {
+        // reach-2 level: from the smoothed (or, below a reach-2 level, the
+        // trilinear) prolongation of level i-1
+        const int pr = f.smooth_down ? 1 + f.reach : 1;
+        if (f.smooth_down) {
+          finalize(i - 1);
+          int rc = power_level(s, (int)i - 1);
+          if (rc) return rc;
+          s->lam_done[i - 1] = 1;
+          launch_smoothing_coef(s->d_lambda + i - 1, s->d_spc + i - 1, s->st);
+        }
+        launch_wide_galerkin(f.g, f.st64, f.reach, f.mask, f.minv64, f.smooth_down ? s->d_spc + i - 1 : nullptr, pr,
+                             c.g, c.st64, c.reach, s->d_psb, s->d_bsb, s->st);
+        launch_wide_mask(c.g, c.reach, c.st64, c.mask, c.minv64, s->st);
+      } else if (!c.galerkin) {
         launch_coarsen_E<double>(f.g, f.E64, c.g, c.E64, s->st);
         if (lame) launch_coarsen_E<double>(f.g, f.mu64, c.g, c.mu64, s->st);
         launch_inv_diag_fine<double>(c.g, c.E64, lame ? c.mu64 : nullptr, dL, dM, c.minv64, s->st);
@@ -1187,24 +1351,9 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
       }
     }
   }
-  // FP32 copies
-  for (size_t i = 0; i < (size_t)nlev(s); ++i) {
-    Level& l = s->L[i];
-    const long long n = l.g.n;
-    if (!l.galerkin) {
-      launch_convert<double, float>(l.E64, l.E32, n, s->st);
-      if (lame) launch_convert<double, float>(l.mu64, l.mu32, n, s->st);
-    } else if (s->o.coarse_storage == VF_STENCIL_FULL) {
-      launch_convert<double, float>(l.st64, l.st32, 243 * n, s->st);
-    } else {
-      launch_stencil_compress<double>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
-      if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
-        launch_stencil_compress<__half>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
-      else
-        launch_stencil_compress<float>(l.g, l.st64, l.mask, l.sym32, l.sq32, s->st);
-    }
-    launch_convert<double, float>(l.minv64, l.minv32, 3 * n, s->st);
-  }
+  // FP32 copies and the compressed stencils of the remaining levels
+  for (size_t i = 0; i < (size_t)nlev(s); ++i)
+    if (!finalized[i]) finalize(i);
   VF_CHECK_LAUNCH();
   // the coarsest factorization (second stream) overlaps the damping estimates
   const bool dense = use_mg(s) && s->o.coarsest == VF_COARSEST_CHOLESKY;
@@ -1775,9 +1924,10 @@ static int restrict_t(vf_solver* s, int level, const double* rf, double* rc_out)
   Level& l = s->L[level];
   Level& c = s->L[level + 1];
   T* a = Sel<T>::w(l, 2);
-  int rc = op_in<T>(s, level, rf, a, nullptr);
+  // the smoothed restriction is P_s^T r with P_s = D (...): masked input
+  int rc = op_in<T>(s, level, rf, a, l.smooth_down ? l.mask : nullptr);
   if (rc) return rc;
-  launch_restrict<T>(l.g, a, c.g, c.mask, Sel<T>::w(c, 3), nullptr, s->st);
+  restrict_level<T>(s, level, a, Sel<T>::w(c, 3), nullptr);
   return op_out<T>(s, level + 1, Sel<T>::w(c, 3), rc_out);
 }
 
@@ -1788,7 +1938,7 @@ static int prolong_t(vf_solver* s, int level, const double* ec, double* ef) {
   int rc = op_in<T>(s, level + 1, ec, Sel<T>::w(c, 0), nullptr);
   if (rc) return rc;
   cudaMemsetAsync(Sel<T>::w(l, 0), 0, sizeof(T) * 3 * (size_t)l.g.n, s->st);
-  launch_prolong_add<T>(c.g, Sel<T>::w(c, 0), l.g, l.mask, Sel<T>::w(l, 0), nullptr, s->st);
+  prolong_level<T>(s, level, Sel<T>::w(c, 0), Sel<T>::w(l, 0), nullptr);
   return op_out<T>(s, level, Sel<T>::w(l, 0), ef);
 }
 
@@ -1963,7 +2113,10 @@ void share_operator(vf_solver* c, const vf_solver* m) {
     d.E64 = sl.E64; d.mu64 = sl.mu64; d.minv64 = sl.minv64; d.st64 = sl.st64;
     d.E32 = sl.E32; d.mu32 = sl.mu32; d.minv32 = sl.minv32; d.st32 = sl.st32;
     d.sym64 = sl.sym64; d.sq64 = sl.sq64; d.sym32 = sl.sym32; d.sym16 = sl.sym16; d.sq32 = sl.sq32;
+    d.reach = sl.reach; d.smooth_down = sl.smooth_down;
   }
+  c->d_spc = m->d_spc;
+  c->d_one = m->d_one;
   c->d_Ainv = m->d_Ainv;
   c->dense_n = m->dense_n;
   c->d_omega = m->d_omega;
@@ -2001,7 +2154,7 @@ int make_child(vf_solver* m, vf_solver** out) {
   auto body = [&]() -> int {
     for (auto& l : s->L) {
       const size_t n = l.g.n;
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < (l.smooth_down ? 5 : 4); ++k) {
         VF_ALLOC(l.w64[k], 3 * n);
         VF_ALLOC(l.w32[k], 3 * n);
       }

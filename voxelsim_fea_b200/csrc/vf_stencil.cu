@@ -575,8 +575,11 @@ __global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, cons
   KrylovState* ks = a.ks;
   if (ks && ks->done) return;
   const T* __restrict__ u = (const T*)a.u;
-  T* __restrict__ out = (T*)a.out;
-  const T* __restrict__ b = (const T*)a.b;
+  // out may be the step field dprev (the smoothed prolongation updates x in
+  // place: each element is read and written by the same thread); a null rhs
+  // reads as zero
+  T* out = (T*)a.out;
+  const T* b = (const T*)a.b;
   const T* __restrict__ minv = (const T*)a.minv;
   const uint8_t* __restrict__ mask = a.mask;
   const T w = a.omega_dev ? (T)(*a.omega_dev) : (T)a.omega;
@@ -687,12 +690,13 @@ __global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, cons
     const T k0 = (m & 1) ? (T)(acc[0] * (A)sqd[p3]) : (T)0;
     const T k1 = (m & 2) ? (T)(acc[1] * (A)sqd[p3 + 1]) : (T)0;
     const T k2 = (m & 4) ? (T)(acc[2] * (A)sqd[p3 + 2]) : (T)0;
+    const T b0 = b ? b[p3] : (T)0, b1 = b ? b[p3 + 1] : (T)0, b2 = b ? b[p3 + 2] : (T)0;
     if (EPI == EPI_APPLY) {
       out[p3] = k0; out[p3 + 1] = k1; out[p3 + 2] = k2;
       if (a.dot_partials)
         dot += (double)u[p3] * (double)k0 + (double)u[p3 + 1] * (double)k1 + (double)u[p3 + 2] * (double)k2;
     } else if (EPI == EPI_SMOOTH) {
-      const T r0 = b[p3] - k0, r1 = b[p3 + 1] - k1, r2 = b[p3 + 2] - k2;
+      const T r0 = b0 - k0, r1 = b1 - k1, r2 = b2 - k2;
       const T u0 = u[p3], u1 = u[p3 + 1], u2 = u[p3 + 2];
       T o0 = u0 + ((m & 1) ? w * (minv[p3] * r0) : (T)0);
       T o1 = u1 + ((m & 2) ? w * (minv[p3 + 1] * r1) : (T)0);
@@ -701,7 +705,7 @@ __global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, cons
       out[p3] = o0; out[p3 + 1] = o1; out[p3 + 2] = o2;
       if (dout) { dout[p3] = o0 - u0; dout[p3 + 1] = o1 - u1; dout[p3 + 2] = o2 - u2; }
     } else {
-      out[p3] = b[p3] - k0; out[p3 + 1] = b[p3 + 1] - k1; out[p3 + 2] = b[p3 + 2] - k2;
+      out[p3] = b0 - k0; out[p3 + 1] = b1 - k1; out[p3 + 2] = b2 - k2;
     }
   }
   if (EPI == EPI_APPLY && a.dot_partials && ks) reduce_and_finalize(dot, a.dot_partials, ks, a.dot_slot, nullptr);

@@ -521,9 +521,18 @@ __global__ void k_wide_dense_assemble(Grid c, int R, const double* __restrict__ 
   }
 }
 
+__global__ void k_smoothing_coef(const double* __restrict__ lambda, double* __restrict__ coef) {
+  const double l = *lambda;
+  *coef = l > 0.0 ? (4.0 / 3.0) / l : 0.0;
+}
+
 }  // namespace
 
 // ---- launchers ---------------------------------------------------------------
+void launch_smoothing_coef(const double* lambda, double* coef, cudaStream_t st) {
+  launch_k(k_smoothing_coef, 1, 1, 0, st, lambda, coef);
+}
+
 size_t wide_prolong_count(const Grid& f, int Pr) { return (size_t)f.n * (Pr + 1) * (Pr + 1) * (Pr + 1) * 9; }
 size_t wide_rapb_count(const Grid& f, int Pr, int Rf) {
   const size_t a = (size_t)(Pr + Rf + 1);

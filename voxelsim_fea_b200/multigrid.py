@@ -68,6 +68,9 @@ class SolverOptions:
     fine_kernel: str = "modal"       # "modal" (z-marching, TMA) | "modal_cpasync" | "gather" (27-neighbour)
     modal_zchunk: int = 0            # z-planes per CTA of the modal kernel (0 = automatic, -1 = one even wave)
     coarse_storage: str = "sym_half"  # Galerkin stencils: "sym_half" | "sym" | "full"
+    # bit l: the transfer from Galerkin level l to l+1 uses the smoothed
+    # prolongation (I - (4/3) D^-1 A_l / lambda_l) P; bit 1 (level 1 -> 2) only
+    smoothed_transfers: int = 0
 
     @classmethod
     def reference(cls, **kw):
@@ -171,6 +174,7 @@ class MGSolver:
         o.autotune = int(bool(self.options.autotune))
         o.smoother = _lib.SMOOTHERS[self.options.smoother]
         o.cheb_ratio = int(self.options.cheb_ratio)
+        o.smoothed_transfers = int(self.options.smoothed_transfers)
         h = ctypes.c_void_p()
         _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
                    None, "vf_create")
