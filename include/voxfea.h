@@ -322,6 +322,31 @@ int vf_solve_batch(vf_solver* const* solvers, int32_t n, const double* const* E,
                    const double* const* nu_elem, const double* const* F, double tol,
                    int32_t max_it, uint32_t flags, double* const* U, vf_solve_info* infos);
 
+/* ---- grid assembly of a solve job (core/solve_worker.py:242-287) --------------
+ * Role masks -> active voxels (uint8 per element, iz-fastest), fixed-DOF bits
+ * (uint8 per node: bit c set <=> DOF c fixed) and the nodal force vector
+ * (3 per node, N), on the device.  roles[i] / masks[i] / meta[3i..3i+2]:
+ *   VF_ROLE_BUILD    per-element mask; the last one is the active set
+ *   VF_ROLE_EXCLUDE  per-element mask removed from it
+ *   VF_ROLE_BEARING  per-node mask; meta = axes (0/1) whose DOFs are fixed
+ *   VF_ROLE_LOAD     per-node mask; meta = force spread evenly over its nodes,
+ *                    added role by role in order (the reference's sums)
+ * flags VF_SOLVE_DEVICE_PTRS: masks and outputs are device pointers.
+ * *n_active_out / *n_fixed_out (optional): active voxels, fixed DOFs. */
+enum { VF_ROLE_BUILD = 0, VF_ROLE_EXCLUDE = 1, VF_ROLE_BEARING = 2, VF_ROLE_LOAD = 3 };
+int vf_assemble_grid(int32_t nx, int32_t ny, int32_t nz, int32_t n_roles, const int32_t* roles,
+                     const uint8_t* const* masks, const double* meta, uint32_t flags, uint8_t* active_out,
+                     uint8_t* fixed_bits_out, double* force_out, int64_t* n_active_out, int64_t* n_fixed_out);
+/* fea.drop_unsupported_islands (fea.py:207-227) with the supports given as the
+ * per-node fixed-DOF bits of vf_assemble_grid (flags as there). */
+int vf_drop_unsupported_islands_mask(int32_t nx, int32_t ny, int32_t nz, const uint8_t* active,
+                                     const uint8_t* fixed_bits, uint32_t flags, uint8_t* kept_out,
+                                     int64_t* n_removed);
+/* VoxelFEA.set_fixed (fea.py:357-369) from per-node fixed-DOF bits (bit c set
+ * <=> DOF c fixed; host, or device with VF_SOLVE_DEVICE_PTRS) instead of a DOF
+ * list. */
+int vf_set_fixed_mask(vf_solver* s, const uint8_t* fixed_bits, uint32_t flags);
+
 /* Per-element displacement field of the result views (core/solve_worker.py:374-388):
  * disp_out[e] = mean over the 8 corners of |u_node| (FP32, element order
  * iz-fastest); u: 3 values per node, reference node order (host arrays). */

@@ -84,10 +84,11 @@ def test_create_rejects_bad_args(lib):
 
 
 def test_grid_assembly_matches_reference_semantics():
-    """solve_worker.assemble (host bookkeeping) on role masks: active = build &
+    """The oracle's restatement of the grid assembly (the checker of the
+    device assembly, vf_assemble_grid) on role masks: active = build &
     ~exclude, fixed DOFs per bearing axis flags, load split evenly over the
     load nodes (solve_worker.py:242-270)."""
-    from voxelsim_fea_b200.solve_worker import assemble
+    from oracle.assemble import assemble
     dims = (2, 1, 1)
     nn = 3 * 2 * 2
     build = np.array([True, True])

@@ -34,6 +34,7 @@ VF_FINE_MODAL, VF_FINE_GATHER, VF_FINE_MODAL_CPASYNC = 0, 1, 2
 STENCIL_STORAGE = {"sym_half": 0, "sym": 1, "full": 2}
 MIXED_MODES = {"reliable": 0, "restart": 1, "outer64": 2}
 SMOOTHERS = {"jacobi": 0, "chebyshev": 1}
+ROLES = {"build": 0, "exclude": 1, "bearing": 2, "load": 3}   # VF_ROLE_* of vf_assemble_grid
 
 PRECISIONS = {"fp64": VF_PREC_FP64, "mixed": VF_PREC_MIXED, "fp32": VF_PREC_FP32}
 COARSE_OPS = {"rediscretize": VF_COARSE_REDISCRETIZE, "galerkin": VF_COARSE_GALERKIN}
@@ -52,6 +53,7 @@ EXPORTS = (
     "vf_nn_wgrad_workspace", "vf_learned_param_count", "vf_learned_configure", "vf_learned_info",
     "vf_learned_input", "vf_learned_apply", "vf_level_mask", "vf_mg_propagate", "vf_solve_block",
     "vf_solve_batch", "vf_inside_points", "vf_inside_grid", "vf_element_displacement",
+    "vf_assemble_grid", "vf_drop_unsupported_islands_mask", "vf_set_fixed_mask",
 )
 
 
@@ -156,6 +158,11 @@ def _declare(L):
                                           ctypes.POINTER(VfSolveInfo)]),
         "vf_inside_points": (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_int64, _P, ctypes.c_int64, _P, _P]),
         "vf_element_displacement": (ctypes.c_int, [_I32, _I32, _I32, _P, _P]),
+        "vf_assemble_grid": (ctypes.c_int, [_I32, _I32, _I32, _I32, _P, _P, _P, ctypes.c_uint32, _P, _P, _P,
+                                            ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+        "vf_drop_unsupported_islands_mask": (ctypes.c_int, [_I32, _I32, _I32, _P, _P, ctypes.c_uint32, _P,
+                                                            ctypes.POINTER(ctypes.c_int64)]),
+        "vf_set_fixed_mask": (ctypes.c_int, [_P, _P, ctypes.c_uint32]),
         "vf_inside_grid": (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_int64, _P, _P, ctypes.c_double, _I32,
                                           _P, _P]),
     }

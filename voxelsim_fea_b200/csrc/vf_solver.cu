@@ -1242,6 +1242,23 @@ int vf_set_fixed(vf_solver* s, const int64_t* fixed, int64_t n) {
   return build_masks(s);
 }
 
+int vf_set_fixed_mask(vf_solver* s, const uint8_t* bits, uint32_t flags) {
+  if (!s || !bits) return VF_ERR_ARG;
+  cudaSetDevice(s->device);
+  const size_t nn = s->h_mask_ref.size();
+  std::vector<uint8_t> staged;
+  const uint8_t* b = bits;
+  if (flags & VF_SOLVE_DEVICE_PTRS) {
+    staged.resize(nn);
+    VF_TRY(cudaMemcpy(staged.data(), bits, nn, cudaMemcpyDeviceToHost));
+    b = staged.data();
+  }
+  for (size_t i = 0; i < nn; ++i) s->h_mask_ref[i] = (uint8_t)(kFreeAll & ~(b[i] & 7));
+  s->have_fixed = true;
+  s->have_material = false;   // masks feed the coarse operators
+  return build_masks(s);
+}
+
 int vf_set_active(vf_solver* s, const uint8_t* active) {
   if (!s) return VF_ERR_ARG;
   cudaSetDevice(s->device);

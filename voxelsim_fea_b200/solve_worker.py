@@ -6,8 +6,9 @@ add-on's parent side runs unchanged.
 
 What runs where: the inside tests of the part / exclusion / bearing / load
 meshes on the device (voxelsim_fea_b200.inside: the reference's parity ray
-cast, points generated on the device); grid assembly on the host (O(voxels)
-bookkeeping, solve_worker.py:242-287); the unsupported-island removal, the
+cast, points generated on the device); grid assembly on the device
+(vf_assemble_grid: active voxels, fixed-DOF bits, nodal forces,
+solve_worker.py:242-287); the unsupported-island removal, the
 solve and the von Mises stress on the device (VoxelFEA); the per-element
 displacement / safety-factor fields and the summary numbers as in
 solve_worker.py:356-431.
@@ -214,38 +215,55 @@ def element_displacement(u, dims):
 
 
 def assemble(descr, masks, dims):
-    """Grid assembly (solve_worker.py:242-270): active voxels, fixed DOFs,
-    nodal force vector from the role masks."""
-    nx, ny, nz = dims
-    inside = None
-    excl = np.zeros(nx * ny * nz, dtype=bool)
-    fixed = []
-    force = np.zeros(3 * (nx + 1) * (ny + 1) * (nz + 1))
-    for (role, meta), mask in zip(descr, masks):
-        if role == "build":
-            inside = mask
-        elif role == "exclude":
-            excl = excl | mask
-        elif role == "bearing":
-            nodes = np.nonzero(mask)[0]
-            for c, on in enumerate(meta):
-                if on:
-                    fixed.append(3 * nodes + c)
-        elif role == "load":
-            nodes = np.nonzero(mask)[0]
-            if len(nodes):
-                fv = np.asarray(meta, dtype=float) / len(nodes)
-                for c in range(3):
-                    force[3 * nodes + c] += fv[c]
-    if inside is None:
-        inside = np.zeros(nx * ny * nz, dtype=bool)
-    active = inside & ~excl
-    fixed_dofs = np.unique(np.concatenate(fixed)).astype(np.int64) if fixed else np.zeros(0, dtype=np.int64)
-    return active, fixed_dofs, force
+    """Grid assembly (solve_worker.py:242-270) on the device (vf_assemble_grid):
+    role masks -> (active bool[nelem], fixed_dofs int64 sorted, force
+    float64[ndof], fixed_bits uint8[nnode] with bit c set <=> DOF c fixed)."""
+    import ctypes
+    from . import _lib
+    nx, ny, nz = (int(v) for v in dims)
+    ne, nn = nx * ny * nz, (nx + 1) * (ny + 1) * (nz + 1)
+    n = len(descr)
+    roles = np.array([_lib.ROLES[r] for r, _ in descr], dtype=np.int32)
+    meta = np.zeros(3 * max(n, 1))
+    arrays = []
+    for i, ((role, m), mask) in enumerate(zip(descr, masks)):
+        size = ne if role in ("build", "exclude") else nn
+        a = np.ascontiguousarray(np.asarray(mask, dtype=bool).ravel().view(np.uint8))
+        if a.size != size:
+            raise ValueError(f"{role} mask has {a.size} entries, expected {size}")
+        arrays.append(a)
+        if role in ("bearing", "load"):
+            meta[3 * i:3 * i + 3] = np.asarray(m, dtype=float)[:3]
+    ptrs = (ctypes.c_void_p * max(n, 1))(*[a.ctypes.data for a in arrays])
+    active = np.empty(ne, dtype=np.uint8)
+    bits = np.empty(nn, dtype=np.uint8)
+    force = np.empty(3 * nn)
+    n_act, n_fix = ctypes.c_int64(), ctypes.c_int64()
+    _lib.check(_lib.load().vf_assemble_grid(nx, ny, nz, n, _lib.ptr(roles), ptrs, _lib.ptr(meta), 0,
+                                            _lib.ptr(active), _lib.ptr(bits), _lib.ptr(force),
+                                            ctypes.byref(n_act), ctypes.byref(n_fix)), None, "assemble")
+    fixed_dofs = np.flatnonzero(((bits[:, None] >> np.arange(3, dtype=np.uint8)) & 1).ravel()).astype(np.int64)
+    return active.astype(bool), fixed_dofs, force, bits
+
+
+def drop_unsupported_islands_bits(active, fixed_bits, dims):
+    """Island removal (core/fea.py:207-227) with the supports as per-node
+    fixed-DOF bits, on the device; returns (kept bool[nelem], n_removed)."""
+    import ctypes
+    from . import _lib
+    nx, ny, nz = (int(v) for v in dims)
+    act = np.ascontiguousarray(np.asarray(active, dtype=bool).ravel().view(np.uint8))
+    kept = np.empty_like(act)
+    nrem = ctypes.c_int64()
+    _lib.check(_lib.load().vf_drop_unsupported_islands_mask(nx, ny, nz, _lib.ptr(act),
+                                                            _lib.ptr(np.ascontiguousarray(fixed_bits)), 0,
+                                                            _lib.ptr(kept), ctypes.byref(nrem)),
+               None, "drop_unsupported_islands")
+    return kept.astype(bool), int(nrem.value)
 
 
 def _worker_main(job_path, work_dir):
-    from . import fea, inside
+    from . import inside
     from .fea import VoxelFEA
     from .multigrid import SolverOptions
 
@@ -275,12 +293,12 @@ def _worker_main(job_path, work_dir):
         set_status(phase="voxel", frac=done / total)
 
     # --- grid assembly, islands ------------------------------------------------
-    active, fixed_dofs, force = assemble(descr, masks, dims)
+    active, fixed_dofs, force, fixed_bits = assemble(descr, masks, dims)
     n_islands_removed = 0
     if fixed_dofs.size and active.any():
-        kept3d, n_islands_removed = fea.drop_unsupported_islands(active.reshape(nx, ny, nz), fixed_dofs)
+        kept, n_islands_removed = drop_unsupported_islands_bits(active, fixed_bits, dims)
         if n_islands_removed:
-            active = kept3d.ravel()
+            active = kept
     if int(active.sum()) == 0:
         set_status(phase="error", error="No material inside the part at this resolution "
                                         "(check the Part object / resolution)")
