@@ -203,20 +203,26 @@ void launch_galerkin_from_fine(const Grid& f, const double* E, const double* mu,
                                const Grid& c, double* stencil_c, const double* Gtab, int lame, cudaStream_t st);
 
 // vf_wide.cu -- reach-R Galerkin levels (coarse space with a smoothed prolongation).
-// Scaled symmetric storage of a reach-R stencil: the diagonal block (6
-// values) and the upper blocks s > center (9 values each), padded to whole
-// 16-byte chunks; warp-chunked like SymLayout.
+// Scaled symmetric storage of a reach-R stencil, split over G = 8 lanes per
+// node: block u of a node -- the upper blocks s = center + 1 + u (u < NU)
+// and the diagonal block (u = NU), 9 values each -- belongs to lane u % G,
+// slot u / G; a lane holds NJ blocks (9 NJ values, zero padded).  Storage is
+// warp-chunked over virtual nodes v = p * G + lane: 16-byte chunk j of 32
+// consecutive virtual nodes is contiguous, so the 32 lanes of a warp (4
+// nodes) load one chunk each in one 512-byte transaction.
 template <typename S, int R> struct WideLayout {
   static constexpr int W = 2 * R + 1, NB = W * W * W, NU = NB / 2;
-  static constexpr int NV = 6 + 9 * NU;
+  static constexpr int G = 8;
+  static constexpr int NBLK = NU + 1;
+  static constexpr int NJ = (NBLK + G - 1) / G;
+  static constexpr int NVL = (NJ * 9 + 7) / 8 * 8;
   static constexpr int VPC = 16 / (int)sizeof(S);
-  static constexpr int NVP = (NV + 7) / 8 * 8;
-  static constexpr int NCH = NVP / VPC;
+  static constexpr int NCH = NVL / VPC;
   using Q = typename std::conditional<sizeof(S) == 8, double, float>::type;
-  __host__ __device__ static constexpr long long off(long long p, int k) {
-    return ((p >> 5) * NCH + k / VPC) * (32LL * VPC) + (p & 31) * VPC + (k % VPC);
+  __host__ __device__ static constexpr long long off(long long v, int k) {
+    return ((v >> 5) * NCH + k / VPC) * (32LL * VPC) + (v & 31) * VPC + (k % VPC);
   }
-  static size_t count(long long n) { return (size_t)((n + 31) / 32) * 32 * NVP; }
+  static size_t count(long long n) { return (size_t)((n * G + 31) / 32) * 32 * NVL; }
 };
 size_t wide_prolong_count(const Grid& f, int Pr);
 size_t wide_rapb_count(const Grid& f, int Pr, int Rf);

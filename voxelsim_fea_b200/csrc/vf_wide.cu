@@ -307,15 +307,13 @@ template <typename S> __device__ __forceinline__ S to_s(double v);
 template <> __device__ __forceinline__ float to_s<float>(double v) { return (float)v; }
 template <> __device__ __forceinline__ double to_s<double>(double v) { return v; }
 template <> __device__ __forceinline__ __half to_s<__half>(double v) { return __double2half(v); }
-__host__ __device__ constexpr int dr(int k) { return k < 3 ? 0 : (k < 5 ? 1 : 2); }
-__host__ __device__ constexpr int dc(int k) { return k < 3 ? k : (k < 5 ? k - 2 : 2); }
 
 template <typename S, int R>
 __global__ void k_wide_compress(Grid g, const double* __restrict__ st, const uint8_t* __restrict__ mask,
                                 S* __restrict__ stc, typename WideLayout<S, R>::Q* __restrict__ sqrtd) {
   using L = WideLayout<S, R>;
   using Q = typename L::Q;
-  constexpr int W = 2 * R + 1, NB = W * W * W, SC = NB / 2;
+  constexpr int W = 2 * R + 1, NB = W * W * W, SC = NB / 2, G = L::G;
   const long long n = g.n;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
     int x, y, z;
@@ -327,11 +325,14 @@ __global__ void k_wide_compress(Grid g, const double* __restrict__ st, const uin
       sp[r] = (in && ((mask[p] >> r) & 1) && d > 0.0) ? 1.0 / sqrt(d) : 0.0;
       sqrtd[3LL * p + r] = (Q)(sp[r] > 0.0 ? 1.0 / sp[r] : 0.0);
     }
-    for (int k = 0; k < 6; ++k)
-      stc[L::off(p, k)] = to_s<S>(in ? st[((long long)SC * 9 + 3 * dr(k) + dc(k)) * n + p] * sp[dr(k)] * sp[dc(k)]
-                                     : 0.0);
-    for (int u = 1; u <= SC; ++u) {
-      const int s = SC + u;
+    for (int u = 0; u < L::G * L::NJ; ++u) {
+      const long long v = (long long)p * G + u % G;
+      const int k0 = 9 * (u / G);
+      if (u >= L::NBLK) {
+        for (int k = 0; k < 9; ++k) stc[L::off(v, k0 + k)] = to_s<S>(0.0);
+        continue;
+      }
+      const int s = (u == L::NU) ? SC : SC + 1 + u;
       const int qx = x + s % W - R, qy = y + (s / W) % W - R, qz = z + s / (W * W) - R;
       double sq[3] = {0.0, 0.0, 0.0};
       if (in && inside(g, qx, qy, qz)) {
@@ -343,12 +344,13 @@ __global__ void k_wide_compress(Grid g, const double* __restrict__ st, const uin
       }
       for (int r = 0; r < 3; ++r)
         for (int cc = 0; cc < 3; ++cc) {
-          const double v = (sp[r] != 0.0 && sq[cc] != 0.0) ? st[((long long)s * 9 + 3 * r + cc) * n + p] * sp[r] * sq[cc]
-                                                           : 0.0;
-          stc[L::off(p, 6 + 9 * (u - 1) + 3 * r + cc)] = to_s<S>(v);
+          const double val = (sp[r] != 0.0 && sq[cc] != 0.0) ? st[((long long)s * 9 + 3 * r + cc) * n + p] * sp[r] * sq[cc]
+                                                             : 0.0;
+          stc[L::off(v, k0 + 3 * r + cc)] = to_s<S>(val);
         }
     }
-    for (int k = L::NV; k < L::NVP; ++k) stc[L::off(p, k)] = to_s<S>(0.0);
+    for (int gl = 0; gl < G; ++gl)
+      for (int k = 9 * L::NJ; k < L::NVL; ++k) stc[L::off((long long)p * G + gl, k)] = to_s<S>(0.0);
   }
 }
 
@@ -384,15 +386,69 @@ template <> struct WChunk<double, double> {
   }
 };
 
+// The 9 values of slot jj of virtual node v (chunks straddled as needed).
+template <typename S, typename A, typename L, int JJ>
+__device__ __forceinline__ void load_block(const S* __restrict__ stc, long long v, A (&blk)[9]) {
+  constexpr int VPC = L::VPC, K0 = 9 * JJ;
+#pragma unroll
+  for (int j = K0 / VPC; j <= (K0 + 8) / VPC; ++j) {
+    WChunk<S, A> ch;
+    ch.load(stc + L::off(v, j * VPC));
+#pragma unroll
+    for (int i = 0; i < VPC; ++i) {
+      const int k = j * VPC + i;
+      if (k >= K0 && k < K0 + 9) blk[k - K0] = ch.v[i];
+    }
+  }
+}
+
+template <typename S, typename A, typename L, int JJ>
+struct WideBlocks {
+  // acc (this node's rows) += own block u = lane + G*JJ applied to the
+  // neighbour p + off(s); for an upper block also the transposed upper block
+  // u of the node p - off(s) (lane and slot are the same there).
+  template <typename VF>
+  __device__ __forceinline__ static void run(const S* __restrict__ stc, const Grid& g, int p, int lane, int x, int y,
+                                             int z, A (&acc)[3], VF V) {
+    constexpr int R = (L::W - 1) / 2, W = L::W, SC = L::NB / 2;
+    const int u = lane + L::G * JJ;
+    if (u < L::NBLK) {
+      const int s = (u == L::NU) ? SC : SC + 1 + u;
+      const int dx = s % W - R, dy = (s / W) % W - R, dz = s / (W * W) - R;
+      const long long v = (long long)p * L::G + lane;
+      if (inside(g, x + dx, y + dy, z + dz)) {
+        const int q = g.idx(x + dx, y + dy, z + dz);
+        A blk[9];
+        load_block<S, A, L, JJ>(stc, v, blk);
+        const A v0 = V(q, 0), v1 = V(q, 1), v2 = V(q, 2);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) acc[r] += blk[3 * r] * v0 + blk[3 * r + 1] * v1 + blk[3 * r + 2] * v2;
+      }
+      if (u < L::NU && inside(g, x - dx, y - dy, z - dz)) {
+        const int q = g.idx(x - dx, y - dy, z - dz);
+        A blk[9];
+        load_block<S, A, L, JJ>(stc, (long long)q * L::G + lane, blk);
+        const A w0 = V(q, 0), w1 = V(q, 1), w2 = V(q, 2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] += blk[c] * w0 + blk[3 + c] * w1 + blk[6 + c] * w2;
+      }
+    }
+    if constexpr (JJ + 1 < L::NJ) WideBlocks<S, A, L, JJ + 1>::run(stc, g, p, lane, x, y, z, acc, V);
+  }
+};
+
 // y = mask(D^1/2 A~ D^1/2 u) with the epilogues of the other level kernels
 // (APPLY, SMOOTH with the Chebyshev step fields, RESID; a null rhs reads as
-// zero).  One thread per padded node (ghost and pad nodes idle).
+// zero).  G = 8 lanes per node: each lane applies its own blocks and the
+// transposed blocks of the same lane and slot of the lower neighbours, the
+// partial sums meet through warp shuffles, and lanes 0..2 write component
+// 0..2 of the node.
 template <typename T, typename S, int R, int EPI>
 __global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __restrict__ stc,
                                                  const T* __restrict__ sqd) {
   using L = WideLayout<S, R>;
   using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
-  constexpr int VPC = L::VPC, W = 2 * R + 1, NB = W * W * W, SC = NB / 2;
+  constexpr int G = L::G;
   KrylovState* ks = a.ks;
   if (ks && ks->done) return;
   const T* __restrict__ u = (const T*)a.u;
@@ -404,90 +460,41 @@ __global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __re
   const T* dprev = (const T*)a.dprev;
   T* dout = (T*)a.dout;
   const T c1 = a.c1_dev ? (T)(*a.c1_dev) : (T)0;
+  auto V = [&](int q, int c) -> A { return (A)__ldg(sqd + 3LL * q + c) * (A)__ldg(u + 3LL * q + c); };
   double dot = 0.0;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < g.n; p += gridDim.x * blockDim.x) {
-    int x, y, z;
-    decode(g, p, x, y, z);
-    if (!inside(g, x, y, z)) continue;
-    const uint8_t m = mask[p];
-    auto V = [&](int q, int c) -> A { return (A)__ldg(sqd + 3LL * q + c) * (A)__ldg(u + 3LL * q + c); };
+  // whole warps iterate together (the shuffles need every lane)
+  const long long nv = ((long long)g.n * G + 31) / 32 * 32;
+  for (long long vv = blockIdx.x * (long long)blockDim.x + threadIdx.x; vv < nv;
+       vv += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(vv / G), lane = (int)(vv % G);
+    int x = -1, y = -1, z = -1;
+    if (p < g.n) decode(g, p, x, y, z);
+    const bool in = p < g.n && inside(g, x, y, z);
+    const uint8_t m = in ? mask[p] : (uint8_t)0;
     A acc[3] = {(A)0, (A)0, (A)0};
-    if (m) {
-      const A v0 = V(p, 0), v1 = V(p, 1), v2 = V(p, 2);
-      // own chunks: diagonal block and the upper blocks (every index below is
-      // a compile-time constant once the loops are unrolled)
-      const S* own = stc + L::off(p, 0);
-      A vq[3] = {(A)0, (A)0, (A)0};
+    if (m) WideBlocks<S, A, L, 0>::run(stc, g, p, lane, x, y, z, acc, V);
 #pragma unroll
-      for (int j = 0; j < L::NCH; ++j) {
-        WChunk<S, A> ch;
-        ch.load(own + (long long)j * 32 * VPC);
+    for (int o = 1; o < G; o <<= 1) {
 #pragma unroll
-        for (int i = 0; i < VPC; ++i) {
-          const int k = j * VPC + i;
-          if (k < 6) {
-            const int r = dr(k), c = dc(k);
-            const A vc = c == 0 ? v0 : (c == 1 ? v1 : v2);
-            const A vr = r == 0 ? v0 : (r == 1 ? v1 : v2);
-            acc[r] += ch.v[i] * vc;
-            if (r != c) acc[c] += ch.v[i] * vr;
-          } else if (k < L::NV) {
-            const int s = SC + 1 + (k - 6) / 9, rc = (k - 6) % 9;
-            if (rc == 0) {
-              const int qx = x + s % W - R, qy = y + (s / W) % W - R, qz = z + s / (W * W) - R;
-              const bool qin = inside(g, qx, qy, qz);
-              const int qn = qin ? g.idx(qx, qy, qz) : 0;
-              vq[0] = qin ? V(qn, 0) : (A)0;
-              vq[1] = qin ? V(qn, 1) : (A)0;
-              vq[2] = qin ? V(qn, 2) : (A)0;
-            }
-            acc[rc / 3] += ch.v[i] * vq[rc % 3];
-          }
-        }
-      }
-      // lower blocks: upper block s of q = p - off(s), transposed
-#pragma unroll
-      for (int s = SC + 1; s < NB; ++s) {
-        const int qx = x - (s % W - R), qy = y - ((s / W) % W - R), qz = z - (s / (W * W) - R);
-        if (!inside(g, qx, qy, qz)) continue;
-        const int q = g.idx(qx, qy, qz);
-        const A w0 = V(q, 0), w1 = V(q, 1), w2 = V(q, 2);
-        const int k0 = 6 + 9 * (s - SC - 1);
-        const S* base = stc + L::off(q, 0);
-#pragma unroll
-        for (int j = k0 / VPC; j <= (k0 + 8) / VPC; ++j) {
-          WChunk<S, A> ch;
-          ch.load(base + (long long)j * 32 * VPC);
-#pragma unroll
-          for (int i = 0; i < VPC; ++i) {
-            const int k = j * VPC + i;
-            if (k >= k0 && k < k0 + 9) {
-              const int r = (k - k0) / 3, c = (k - k0) % 3;
-              acc[c] += ch.v[i] * (r == 0 ? w0 : (r == 1 ? w1 : w2));
-            }
-          }
-        }
-      }
+      for (int c = 0; c < 3; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
     }
-    const long long p3 = 3LL * p;
-    const T k0 = (m & 1) ? (T)(acc[0] * (A)sqd[p3]) : (T)0;
-    const T k1 = (m & 2) ? (T)(acc[1] * (A)sqd[p3 + 1]) : (T)0;
-    const T k2 = (m & 4) ? (T)(acc[2] * (A)sqd[p3 + 2]) : (T)0;
-    const T b0 = b ? b[p3] : (T)0, b1 = b ? b[p3 + 1] : (T)0, b2 = b ? b[p3 + 2] : (T)0;
+    if (!in || lane >= 3) continue;
+    const int c = lane;
+    const long long pc = 3LL * p + c;
+    const A ac = c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]);
+    const T kc = ((m >> c) & 1) ? (T)(ac * (A)sqd[pc]) : (T)0;
+    const T bc = b ? b[pc] : (T)0;
     if (EPI == EPI_APPLY) {
-      out[p3] = k0; out[p3 + 1] = k1; out[p3 + 2] = k2;
-      if (a.dot_partials)
-        dot += (double)u[p3] * (double)k0 + (double)u[p3 + 1] * (double)k1 + (double)u[p3 + 2] * (double)k2;
+      out[pc] = kc;
+      if (a.dot_partials) dot += (double)u[pc] * (double)kc;
     } else if (EPI == EPI_SMOOTH) {
-      const T u0 = u[p3], u1 = u[p3 + 1], u2 = u[p3 + 2];
-      T o0 = u0 + ((m & 1) ? w * (minv[p3] * (b0 - k0)) : (T)0);
-      T o1 = u1 + ((m & 2) ? w * (minv[p3 + 1] * (b1 - k1)) : (T)0);
-      T o2 = u2 + ((m & 4) ? w * (minv[p3 + 2] * (b2 - k2)) : (T)0);
-      if (dprev) { o0 += c1 * dprev[p3]; o1 += c1 * dprev[p3 + 1]; o2 += c1 * dprev[p3 + 2]; }
-      out[p3] = o0; out[p3 + 1] = o1; out[p3 + 2] = o2;
-      if (dout) { dout[p3] = o0 - u0; dout[p3 + 1] = o1 - u1; dout[p3 + 2] = o2 - u2; }
+      const T u0 = u[pc];
+      T o = u0 + (((m >> c) & 1) ? w * (minv[pc] * (bc - kc)) : (T)0);
+      if (dprev) o += c1 * dprev[pc];
+      out[pc] = o;
+      if (dout) dout[pc] = o - u0;
     } else {
-      out[p3] = b0 - k0; out[p3 + 1] = b1 - k1; out[p3 + 2] = b2 - k2;
+      out[pc] = bc - kc;
     }
   }
   if (EPI == EPI_APPLY && a.dot_partials && ks) reduce_and_finalize(dot, a.dot_partials, ks, a.dot_slot, nullptr);
@@ -570,7 +577,7 @@ template void launch_wide_compress<double, 2>(const Grid&, const double*, const 
 
 template <typename T, typename S, int R>
 void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
-  const int blocks = blocks_for(g.n, 128, 148LL * 16);
+  const int blocks = blocks_for((long long)g.n * WideLayout<S, R>::G, 128, 148LL * 32);
   if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY>, blocks, 128, 0, st, g, a, stc, sqrtd);
   else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH>, blocks, 128, 0, st, g, a, stc, sqrtd);
   else launch_k(k_wide_op<T, S, R, EPI_RESID>, blocks, 128, 0, st, g, a, stc, sqrtd);
@@ -579,7 +586,7 @@ template void launch_wide_op<float, __half, 2>(const Grid&, int, const OpArgs&, 
 template void launch_wide_op<float, float, 2>(const Grid&, int, const OpArgs&, const float*, const float*, cudaStream_t);
 template void launch_wide_op<double, double, 2>(const Grid&, int, const OpArgs&, const double*, const double*,
                                                 cudaStream_t);
-int wide_op_grid_blocks(const Grid& g) { return blocks_for(g.n, 128, 148LL * 16); }
+int wide_op_grid_blocks(const Grid& g) { return blocks_for((long long)g.n * 8, 128, 148LL * 32); }
 
 int wide_dense_assemble(const Grid& c, int R, const double* stencil, const uint8_t* cmask, double* A, int n,
                         cudaStream_t st) {
