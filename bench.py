@@ -393,6 +393,84 @@ def run_batch(args):
     return 0
 
 
+# --------------------------------------------------------------------------- other configurations
+def other_configs(args, local):
+    """One measured solve of each other configuration of the reference's
+    benchmark set, after the headline arm (warm-up call, then one timed call,
+    host clock around the synchronous API call, tol 1e-8):
+      * 192^3 bracket with 16 load cases as one block call;
+      * 64 independent parts, edges in {32..128}, in one batch call;
+      * the 512x256x256 two-material part (steel / ABS, per-voxel nu), 6 levels."""
+    import torch
+    from voxelsim_fea_b200 import generators
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions, solve_batch
+    opts = dict(device=local, check_every=args.check_every, smoother=args.smoother,
+                smoothed_transfers=args.smoothed_transfers)
+    out = {}
+
+    def timed_call(fn):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, r
+
+    # 192^3, k = 16 load cases (generators.load_cases: direction uniform on the
+    # sphere, 1-10 kN on a random 8x8 top patch)
+    w = WORKLOADS["bracket_192"]
+    p = make_problem(w)
+    nx, ny, nz = p["dims"]
+    F = generators.load_cases(p, 16, seed=w["seed"] + 1)
+    m = MGSolver(nx, ny, nz, p["fixed_dofs"], nu=p["nu"], max_levels=w["levels"], options=SolverOptions.fast(**opts))
+    E = mg_modulus(p)
+    dt, _ = timed_call(lambda: m.solve_block(E, F, tol=TOL, max_cg=args.max_it or None))
+    infos = m.last_block_info
+    out["bracket_192_block16"] = {"seconds": dt, "dof_per_case": m.ndof, "cases": 16,
+                                  "mdof_per_s": 16 * m.ndof / dt / 1e6,
+                                  "iterations_max": max(i.iters for i in infos),
+                                  "true_resid_max": max(i.true_resid for i in infos),
+                                  "what": "k = 16 concurrent solves sharing one operator set-up (vf_solve_block)"}
+    m.close()
+    del F
+
+    # 64 uneven parts in one batch call
+    rng = np.random.default_rng(1234)
+    edges = (32, 48, 64, 80, 96, 112, 128)
+    parts, solvers = [], []
+    for i in range(64):
+        sh = tuple(int(rng.choice(edges)) for _ in range(3))
+        q = generators.bracket(shape=sh, seed=5000 + i, sigma=3.0, load_n=2000.0, patch=8)
+        parts.append(q)
+        solvers.append(MGSolver(*sh, q["fixed_dofs"], nu=q["nu"], options=SolverOptions.fast(**opts)))
+    ndof = sum(sv.ndof for sv in solvers)
+    dt, _ = timed_call(lambda: solve_batch(solvers, [mg_modulus(q) for q in parts], [q["f"] for q in parts],
+                                           tol=TOL, max_cg=args.max_it or None))
+    out["batch64_parts_32-128"] = {"seconds": dt, "dof": ndof, "mdof_per_s": ndof / dt / 1e6,
+                                   "iterations_max": max(sv.last_iters for sv in solvers),
+                                   "true_resid_max": max(sv.last_info.true_resid for sv in solvers),
+                                   "what": "independent solvers set up and solved concurrently (vf_solve_batch)"}
+    for sv in solvers:
+        sv.close()
+    del parts, solvers
+
+    # 512 x 256 x 256 two-material part
+    w = WORKLOADS["twomat_512x256x256"]
+    p = make_problem(w)
+    nx, ny, nz = p["dims"]
+    m = MGSolver(nx, ny, nz, p["fixed_dofs"], nu=0.3, max_levels=w["levels"], options=SolverOptions.fast(**opts))
+    E = mg_modulus(p)
+    nu = np.ascontiguousarray(p["nu"], dtype=np.float64)
+    cap = args.max_it or 4000
+    dt, _ = timed_call(lambda: m.solve(E, p["f"], tol=TOL, max_cg=cap, nu_elem=nu))
+    out["twomat_512x256x256"] = {"seconds": dt, "dof": m.ndof, "mdof_per_s": m.ndof / dt / 1e6,
+                                 "iterations": int(m.last_iters), "true_resid": float(m.last_info.true_resid),
+                                 "converged": bool(m.last_converged), "max_cg": cap,
+                                 "setup_ms": float(m.last_info.setup_ms)}
+    m.close()
+    return out
+
+
 # --------------------------------------------------------------------------- B200 arm
 def run_b200(args):
     import torch
@@ -650,6 +728,10 @@ def run_b200(args):
                "ms_per_step": ems, "true_resid": float(fast.last_info.true_resid),
                "u_finite": bool(np.isfinite(u_h).all())}
 
+    others = None
+    if rank == 0 and world == 1 and K == 1 and not args.no_other_configs and args.workload == "bracket_256x128x128":
+        others = other_configs(args, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_record(full=((nx, ny, nz), E_mg, nu_scalar))
@@ -685,6 +767,7 @@ def run_b200(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "other_configs": others,
             "clocks": clocks,
             "gpu_launches": launches,
         }
@@ -713,6 +796,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-errors", action="store_true", help="skip the FP64 reference solve and the error figures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the single-solve figures of the 192^3 block, 64-part batch and 512x256x256 configs")
     ap.add_argument("--nvtx", action="store_true", help="wrap the timed steps in NVTX range vf_timed")
     ap.add_argument("--kernel-profile", choices=("apply", "smooth", "resid", "restrict", "prolong", "vcycle"),
                     help="set up, then run one kernel 3x inside NVTX range vf_kernel and exit")
