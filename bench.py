@@ -807,7 +807,7 @@ def main():
     ap.add_argument("--mixed-mode", choices=("outer64", "reliable", "restart"), default="outer64")
     ap.add_argument("--smoother", choices=("jacobi", "chebyshev"), default="chebyshev",
                     help="V-cycle smoothing of every arm (plain FP64, mixed, learned)")
-    ap.add_argument("--smoothed-transfers", type=int, default=0,
+    ap.add_argument("--smoothed-transfers", type=int, default=2,
                     help="bitmask of transfers l -> l+1 with the smoothed prolongation (2: level 1 -> 2)")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed: residual reduction between FP64 corrections (solver default if unset)")

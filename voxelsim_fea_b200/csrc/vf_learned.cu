@@ -252,6 +252,7 @@ struct NnStage {
   double* part = nullptr;    // sum-of-squares partials
   float* scale = nullptr;
   std::vector<void*> allocs;
+  int* err = nullptr;        // the solver's error flag (expired bounded waits of the convolutions)
 };
 
 namespace {
@@ -351,10 +352,13 @@ void nn_make_input(NnStage* s, const Grid& gL, const T* r, const int* skip, cuda
            s->Y[0], s->Z[0], s->in, skip);
 }
 
+void nn_set_error_flag(NnStage* s, int* err) { s->err = err; }
+
 void nn_forward(NnStage* s, const int* skip, cudaStream_t st) {
   auto conv = [&](int k, int lv, const bf16* in, bf16* out, const bf16* sk, bool relu, float* of32) {
     NnConvArgs a{in, s->w[k], s->b[k], sk, nullptr, out, of32, s->X[lv], s->Y[lv], s->Z[lv], relu ? 1 : 0};
     a.skip_flag = skip;
+    a.err = s->err;
     nn_conv_forward(kCin[k], kCout[k], a, st);
   };
   const long long v1 = (long long)s->X[1] * s->Y[1] * s->Z[1], v0 = v1 * 8, v2 = v1 / 8;

@@ -338,9 +338,11 @@ size_t nn_wgrad_work_bytes(int cin, int cout, int X, int Y, int Z) {
 
 #define VF_NN_PAIRS(F) F(16, 16) F(16, 32) F(32, 16) F(32, 32) F(32, 64) F(64, 32) F(64, 64)
 
+template <int CIN, int COUT> int conv_forward_tc(const NnConvArgs& a, cudaStream_t st);   // vf_nn_tc.cu
+
 int nn_conv_forward(int cin, int cout, const NnConvArgs& a, cudaStream_t st) {
 #define VF_NN_FWD(I, O) \
-  if (cin == I && cout == O) return conv_forward_t<I, O>(a, st);
+  if (cin == I && cout == O) return conv_forward_tc<I, O>(a, st);
   VF_NN_PAIRS(VF_NN_FWD)
 #undef VF_NN_FWD
   return -1;

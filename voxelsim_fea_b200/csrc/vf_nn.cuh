@@ -21,6 +21,7 @@ struct NnConvArgs {
   int X, Y, Z;
   int relu;
   const int* skip_flag = nullptr;   // device flag: the launch is a no-op while *skip_flag != 0
+  int* err = nullptr;               // device flag raised when a bounded wait of the kernel expires
 };
 
 // Supported (cin, cout): (16,16) (16,32) (32,16) (32,32) (32,64) (64,32) (64,64).
@@ -43,6 +44,7 @@ bool nn_has_weights(const NnStage* s);
 void nn_set_features(NnStage* s, const Grid& g0, const double* E0, const double* eref_dev, cudaStream_t st);
 template <typename T> void nn_make_input(NnStage* s, const Grid& gL, const T* r, const int* skip, cudaStream_t st);
 void nn_forward(NnStage* s, const int* skip, cudaStream_t st);
+void nn_set_error_flag(NnStage* s, int* err);
 template <typename T> void nn_make_output(NnStage* s, const Grid& gL, const uint8_t* maskL, T* e, const int* skip,
                                           cudaStream_t st);
 const void* nn_input_buffer(const NnStage* s);

@@ -2321,6 +2321,7 @@ int vf_learned_configure(vf_solver* s, int32_t level, const float* params, int64
     cudaError_t e = cudaSuccess;
     s->nn = vf::nn_create(s->L[level].g, level, s->st, &e);
     if (!s->nn) { s->err = std::string("learned stage: ") + cudaGetErrorString(e); return VF_ERR_NOMEM; }
+    vf::nn_set_error_flag(s->nn, s->d_err);
     s->nn_level = level;
     if (s->have_material) nn_refresh_features(s);
   }

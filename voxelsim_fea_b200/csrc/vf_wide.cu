@@ -216,24 +216,21 @@ __global__ void __launch_bounds__(kSetupThreads) k_rap_b(Grid f, const double* _
 // upper offsets D of reach Rc: one CTA per coarse interior node I, P_s[.][I]
 // of the (2Pr+1)^3 fine nodes around 2I in shared memory, one thread per D.
 constexpr int kRapThreads = 64;
-constexpr int kRapChunk = 5;   // fine nodes whose B rows are staged together
 __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const double* __restrict__ psb, int Pr,
                                                        const double* __restrict__ bsb, Grid c, int Rc,
                                                        double* __restrict__ stc) {
-  extern __shared__ double smem_c[];   // sps [(2Pr+1)^3][9], then sB [kRapChunk][NSB * 9]
+  extern __shared__ double sps[];   // [(2Pr+1)^3][9]
   const int NA = Pr + 1, NS = NA * NA * NA;
   const int NBA = Pr + Rf + 1, NSB = NBA * NBA * NBA;
   const int WI = 2 * Pr + 1, NI = WI * WI * WI;
   const int Wc = wide_w(Rc), NBc = wide_nb(Rc), SC = NBc / 2;
-  double* sps = smem_c;
-  double* sB = smem_c + NI * 9;
   const long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
   const long long nc = c.n;
   for (long long node = blockIdx.x; node < nint; node += gridDim.x) {
     int X, Y, Z;
     interior_xyz(c, node, X, Y, Z);
     const int pI = c.idx(X, Y, Z);
-    __syncthreads();   // the previous node's readers are done with sps / sB
+    __syncthreads();   // the previous node's readers are done with sps
     for (int e = threadIdx.x; e < NI * 9; e += blockDim.x) {
       const int i = e / 9, k = e % 9;
       const int ix = 2 * X + i % WI - Pr, iy = 2 * Y + (i / WI) % WI - Pr, iz = 2 * Z + i / (WI * WI) - Pr;
@@ -244,47 +241,33 @@ __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const dou
       }
       sps[e] = v;
     }
-    // one thread per diagonal / upper offset; the others idle
-    const int u = threadIdx.x;
-    const int s = SC + u;
-    const bool mine = u <= SC;
-    const int Dx = s % Wc - Rc, Dy = (s / Wc) % Wc - Rc, Dz = s / (Wc * Wc) - Rc;
-    const int Jx = X + Dx, Jy = Y + Dy, Jz = Z + Dz;
-    const bool jin = mine && inside(c, Jx, Jy, Jz);
-    double acc[9];
+    __syncthreads();
+    for (int u = threadIdx.x; u <= SC; u += blockDim.x) {
+      const int s = SC + u;   // center and upper offsets
+      const int Dx = s % Wc - Rc, Dy = (s / Wc) % Wc - Rc, Dz = s / (Wc * Wc) - Rc;
+      const int Jx = X + Dx, Jy = Y + Dy, Jz = Z + Dz;
+      double acc[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) acc[k] = 0.0;
-    for (int i0 = 0; i0 < NI; i0 += kRapChunk) {
-      __syncthreads();   // sps staged / the previous chunk's readers are done
-      for (int e = threadIdx.x; e < kRapChunk * NSB * 9; e += blockDim.x) {
-        const int ii = e / (NSB * 9), rem = e % (NSB * 9);
-        const int i = i0 + ii;
-        double v = 0.0;
-        if (i < NI) {
+      for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+      if (inside(c, Jx, Jy, Jz)) {
+        for (int i = 0; i < NI; ++i) {
           const int ix = 2 * X + i % WI - Pr, iy = 2 * Y + (i / WI) % WI - Pr, iz = 2 * Z + i / (WI * WI) - Pr;
-          if (inside(f, ix, iy, iz)) v = bsb[(long long)f.idx(ix, iy, iz) * NSB * 9 + rem];
+          if (!inside(f, ix, iy, iz)) continue;
+          const int bx = Jx - ceil_half(ix - Pr - Rf), by = Jy - ceil_half(iy - Pr - Rf);
+          const int bz = Jz - ceil_half(iz - Pr - Rf);
+          if (bx < 0 || bx >= NBA || by < 0 || by >= NBA || bz < 0 || bz >= NBA) continue;
+          const double* P = sps + i * 9;
+          const double* B = bsb + ((long long)f.idx(ix, iy, iz) * NSB + (bz * NBA + by) * NBA + bx) * 9;
+          double Bv[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) Bv[k] = B[k];
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+              acc[3 * r + cc] += P[r] * Bv[cc] + P[3 + r] * Bv[3 + cc] + P[6 + r] * Bv[6 + cc];
         }
-        sB[e] = v;
       }
-      __syncthreads();
-      if (!jin) continue;
-      for (int ii = 0; ii < kRapChunk && i0 + ii < NI; ++ii) {
-        const int i = i0 + ii;
-        const int ix = 2 * X + i % WI - Pr, iy = 2 * Y + (i / WI) % WI - Pr, iz = 2 * Z + i / (WI * WI) - Pr;
-        if (!inside(f, ix, iy, iz)) continue;
-        const int bx = Jx - ceil_half(ix - Pr - Rf), by = Jy - ceil_half(iy - Pr - Rf);
-        const int bz = Jz - ceil_half(iz - Pr - Rf);
-        if (bx < 0 || bx >= NBA || by < 0 || by >= NBA || bz < 0 || bz >= NBA) continue;
-        const double* P = sps + i * 9;
-        const double* B = sB + ii * NSB * 9 + ((bz * NBA + by) * NBA + bx) * 9;
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-          for (int cc = 0; cc < 3; ++cc)
-            acc[3 * r + cc] += P[r] * B[cc] + P[3 + r] * B[3 + cc] + P[6 + r] * B[6 + cc];
-      }
-    }
-    if (mine) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * nc + pI] = acc[k];
     }
@@ -455,9 +438,8 @@ __device__ __forceinline__ void load_block(const S* __restrict__ stc, long long 
 template <typename S, typename A, typename L, int JJ>
 struct WideBlocks {
   // acc (this node's rows) += own block u = lane + G*JJ applied to the
-  // neighbour at off(s); for an upper block also the transposed upper block
-  // u of the node p - off(s) (lane and slot are the same there).  V(dx, dy,
-  // dz, c): D^1/2 u at the neighbour (dx, dy, dz).
+  // neighbour p + off(s); for an upper block also the transposed upper block
+  // u of the node p - off(s) (lane and slot are the same there).
   template <typename VF>
   __device__ __forceinline__ static void run(const S* __restrict__ stc, const Grid& g, int p, int lane, int x, int y,
                                              int z, A (&acc)[3], VF V) {
@@ -466,11 +448,12 @@ struct WideBlocks {
     if (u < L::NBLK) {
       const int s = (u == L::NU) ? SC : SC + 1 + u;
       const int dx = s % W - R, dy = (s / W) % W - R, dz = s / (W * W) - R;
-      {
-        // own block (zero where the neighbour is outside the level)
+      const long long v = (long long)p * L::G + lane;
+      if (inside(g, x + dx, y + dy, z + dz)) {
+        const int q = g.idx(x + dx, y + dy, z + dz);
         A blk[9];
-        load_block<S, A, L, JJ>(stc, (long long)p * L::G + lane, blk);
-        const A v0 = V(dx, dy, dz, 0), v1 = V(dx, dy, dz, 1), v2 = V(dx, dy, dz, 2);
+        load_block<S, A, L, JJ>(stc, v, blk);
+        const A v0 = V(q, 0), v1 = V(q, 1), v2 = V(q, 2);
 #pragma unroll
         for (int r = 0; r < 3; ++r) acc[r] += blk[3 * r] * v0 + blk[3 * r + 1] * v1 + blk[3 * r + 2] * v2;
       }
@@ -478,7 +461,7 @@ struct WideBlocks {
         const int q = g.idx(x - dx, y - dy, z - dz);
         A blk[9];
         load_block<S, A, L, JJ>(stc, (long long)q * L::G + lane, blk);
-        const A w0 = V(-dx, -dy, -dz, 0), w1 = V(-dx, -dy, -dz, 1), w2 = V(-dx, -dy, -dz, 2);
+        const A w0 = V(q, 0), w1 = V(q, 1), w2 = V(q, 2);
 #pragma unroll
         for (int c = 0; c < 3; ++c) acc[c] += blk[c] * w0 + blk[3 + c] * w1 + blk[6 + c] * w2;
       }
@@ -489,22 +472,16 @@ struct WideBlocks {
 
 // y = mask(D^1/2 A~ D^1/2 u) with the epilogues of the other level kernels
 // (APPLY, SMOOTH with the Chebyshev step fields, RESID; a null rhs reads as
-// zero).  A CTA owns a tile of kWX x kWY x kWZ nodes and stages D^1/2 u of the
-// tile and its reach-R halo in shared memory; G = 8 lanes per node each apply
-// their own blocks and the transposed blocks of the same lane and slot of the
-// lower neighbours, the partial sums meet through warp shuffles, and lanes
-// 0..2 write component 0..2 of the node.
-constexpr int kWX = 8, kWY = 4, kWZ = 2;
-constexpr int kWideThreads = kWX * kWY * kWZ * 8;
+// zero).  G = 8 lanes per node: each lane applies its own blocks and the
+// transposed blocks of the same lane and slot of the lower neighbours, the
+// partial sums meet through warp shuffles, and lanes 0..2 write component
+// 0..2 of the node.
 template <typename T, typename S, int R, int EPI>
-__global__ void __launch_bounds__(kWideThreads) k_wide_op(Grid g, OpArgs a, const S* __restrict__ stc,
-                                                          const T* __restrict__ sqd) {
+__global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __restrict__ stc,
+                                                 const T* __restrict__ sqd) {
   using L = WideLayout<S, R>;
   using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
   constexpr int G = L::G;
-  static_assert(G * kWX * kWY * kWZ == kWideThreads, "one lane group per node of the tile");
-  constexpr int HX = kWX + 2 * R, HY = kWY + 2 * R, HZ = kWZ + 2 * R;
-  __shared__ A vs[HZ][HY][HX][3];
   KrylovState* ks = a.ks;
   if (ks && ks->done) return;
   const T* __restrict__ u = (const T*)a.u;
@@ -516,28 +493,18 @@ __global__ void __launch_bounds__(kWideThreads) k_wide_op(Grid g, OpArgs a, cons
   const T* dprev = (const T*)a.dprev;
   T* dout = (T*)a.dout;
   const T c1 = a.c1_dev ? (T)(*a.c1_dev) : (T)0;
-  const int ntx = (g.lx + kWX) / kWX, nty = (g.ly + kWY) / kWY, ntz = (g.lz + kWZ) / kWZ;
-  const int nl = threadIdx.x / G, lane = threadIdx.x % G;
-  const int lxn = nl % kWX, lyn = (nl / kWX) % kWY, lzn = nl / (kWX * kWY);
+  auto V = [&](int q, int c) -> A { return (A)__ldg(sqd + 3LL * q + c) * (A)__ldg(u + 3LL * q + c); };
   double dot = 0.0;
-  for (int tile = blockIdx.x; tile < ntx * nty * ntz; tile += gridDim.x) {
-    const int X0 = (tile % ntx) * kWX, Y0 = ((tile / ntx) % nty) * kWY, Z0 = (tile / (ntx * nty)) * kWZ;
-    __syncthreads();   // the previous tile's readers are done with vs
-    for (int h = threadIdx.x; h < HX * HY * HZ; h += blockDim.x) {
-      const int hx = h % HX, hy = (h / HX) % HY, hz = h / (HX * HY);
-      const int qx = X0 - R + hx, qy = Y0 - R + hy, qz = Z0 - R + hz;
-      const bool qin = inside(g, qx, qy, qz);
-      const long long q3 = qin ? 3LL * g.idx(qx, qy, qz) : 0;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) vs[hz][hy][hx][c] = qin ? (A)__ldg(sqd + q3 + c) * (A)__ldg(u + q3 + c) : (A)0;
-    }
-    __syncthreads();
-    const int x = X0 + lxn, y = Y0 + lyn, z = Z0 + lzn;
-    const bool in = inside(g, x, y, z);
-    const int p = in ? g.idx(x, y, z) : 0;
+  // whole warps iterate together (the shuffles need every lane)
+  const long long nv = ((long long)g.n * G + 31) / 32 * 32;
+  for (long long vv = blockIdx.x * (long long)blockDim.x + threadIdx.x; vv < nv;
+       vv += (long long)gridDim.x * blockDim.x) {
+    const int p = (int)(vv / G), lane = (int)(vv % G);
+    int x = -1, y = -1, z = -1;
+    if (p < g.n) decode(g, p, x, y, z);
+    const bool in = p < g.n && inside(g, x, y, z);
     const uint8_t m = in ? mask[p] : (uint8_t)0;
     A acc[3] = {(A)0, (A)0, (A)0};
-    auto V = [&](int dx, int dy, int dz, int c) -> A { return vs[lzn + R + dz][lyn + R + dy][lxn + R + dx][c]; };
     if (m) WideBlocks<S, A, L, 0>::run(stc, g, p, lane, x, y, z, acc, V);
 #pragma unroll
     for (int o = 1; o < G; o <<= 1) {
@@ -626,7 +593,7 @@ void launch_wide_galerkin(const Grid& f, const double* stf, int Rf, const uint8_
   launch_k(k_rap_b, (int)std::min<long long>((nintf + ngb - 1) / ngb, 148LL * 64), kSetupThreads, smem_b, st, f, stf,
            Rf, psb, Pr, c, bsb);
   const int WI = 2 * Pr + 1;
-  const size_t smem = sizeof(double) * (WI * WI * WI * 9 + (size_t)kRapChunk * NSB * 9);
+  const size_t smem = sizeof(double) * WI * WI * WI * 9;
   launch_k(k_rap_c, (int)std::min<long long>(nintc, 148LL * 256), kRapThreads, smem, st, f, Rf, psb, Pr, bsb, c, Rc,
            stc);
   launch_k(k_wide_mirror, blocks_for((long long)(wide_nb(Rc) / 2) * nintc, 128), 128, 0, st, c, Rc, stc);
@@ -649,18 +616,15 @@ template void launch_wide_compress<double, 2>(const Grid&, const double*, const 
 template <typename T, typename S, int R>
 void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
   const int blocks = wide_op_grid_blocks(g);
-  if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY>, blocks, kWideThreads, 0, st, g, a, stc, sqrtd);
-  else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH>, blocks, kWideThreads, 0, st, g, a, stc, sqrtd);
-  else launch_k(k_wide_op<T, S, R, EPI_RESID>, blocks, kWideThreads, 0, st, g, a, stc, sqrtd);
+  if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else launch_k(k_wide_op<T, S, R, EPI_RESID>, blocks, 128, 0, st, g, a, stc, sqrtd);
 }
 template void launch_wide_op<float, __half, 2>(const Grid&, int, const OpArgs&, const __half*, const float*, cudaStream_t);
 template void launch_wide_op<float, float, 2>(const Grid&, int, const OpArgs&, const float*, const float*, cudaStream_t);
 template void launch_wide_op<double, double, 2>(const Grid&, int, const OpArgs&, const double*, const double*,
                                                 cudaStream_t);
-int wide_op_grid_blocks(const Grid& g) {
-  const long long tiles = (long long)((g.lx + kWX) / kWX) * ((g.ly + kWY) / kWY) * ((g.lz + kWZ) / kWZ);
-  return (int)std::min<long long>(tiles, 148LL * 4);
-}
+int wide_op_grid_blocks(const Grid& g) { return blocks_for((long long)g.n * 8, 128, 148LL * 32); }
 
 int wide_dense_assemble(const Grid& c, int R, const double* stencil, const uint8_t* cmask, double* A, int n,
                         cudaStream_t st) {

@@ -40,6 +40,16 @@ def _preset_smoother(kw):
     return "chebyshev"
 
 
+def _preset_transfers(kw):
+    """The presets smooth the level 1 -> 2 prolongation (the 125-block coarse
+    space) wherever the options allow it (Galerkin levels, auto damping,
+    symmetric storage): about 1.4x fewer PCG iterations at the price of a
+    heavier set-up and level 2."""
+    if kw.get("coarse_storage") == "full" or kw.get("omega_mode", "auto") != "auto":
+        return 0
+    return 2
+
+
 @dataclasses.dataclass
 class SolverOptions:
     """B200 solver options beyond the reference's keyword arguments."""
@@ -86,7 +96,7 @@ class SolverOptions:
         the CG residual norm of a converging solve on high-contrast geometry is
         not monotone."""
         base = dict(coarse="galerkin", coarsest="cholesky", omega_mode="auto", stall_guard=False,
-                    smoother=_preset_smoother(kw))
+                    smoother=_preset_smoother(kw), smoothed_transfers=_preset_transfers(kw))
         base.update(kw)
         return cls(**base)
 
@@ -95,7 +105,7 @@ class SolverOptions:
         """Galerkin hierarchy, mixed precision: by default FP64 PCG preconditioned by
         the FP32 V-cycle (``mixed_mode="outer64"``)."""
         base = dict(coarse="galerkin", coarsest="cholesky", precision="mixed", omega_mode="auto",
-                    stall_guard=False, smoother=_preset_smoother(kw))
+                    stall_guard=False, smoother=_preset_smoother(kw), smoothed_transfers=_preset_transfers(kw))
         base.update(kw)
         return cls(**base)
 
