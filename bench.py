@@ -570,6 +570,28 @@ def run_b200(args):
         ms = max_over_ranks(ev0.elapsed_time(ev1) / steps, dist, "cuda")
         return ms, res, clocks, int(s1.value - s0.value)
 
+    if args.kernel_profile == "learned":
+        # set-up once, then the learned stage (restriction, the 10 U-Net
+        # convolutions on level 1, prolongation) once inside NVTX range vf_kernel
+        from voxelsim_fea_b200.learned import stage
+        step(fast)
+        stage.enable_default(fast)
+        r = np.random.default_rng(3).standard_normal(ndof)
+        e = np.empty(ndof)
+        _lib.check(L.vf_learned_apply(fast._h, _lib.ptr(r), _lib.ptr(e)), fast._h)   # warm
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("vf_kernel")
+        t0 = time.perf_counter()
+        for _ in range(args.kernel_iters):
+            _lib.check(L.vf_learned_apply(fast._h, _lib.ptr(r), _lib.ptr(e)), fast._h)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / args.kernel_iters
+        torch.cuda.nvtx.range_pop()
+        print(json.dumps({"kernel": "learned", "ms_per_application": dt * 1e3, "workload": args.workload,
+                          "timing": "host clock around vf_learned_apply (host arrays, FP64 transfers)"}), flush=True)
+        fast.close()
+        return 0
+
     if args.kernel_profile:
         # set-up once, then KERNEL alone inside an NVTX range (for ncu --nvtx-include "vf_kernel/")
         kid = {"apply": 0, "smooth": 1, "resid": 2, "restrict": 3, "prolong": 4, "vcycle": 5}[args.kernel_profile]
@@ -645,8 +667,14 @@ def run_b200(args):
     def errors_of(u):
         if ref_fields is None or u is None:
             return None
-        return field_errors(u, von_mises(u), ref_fields[0], ref_fields[1], node_act, elem_act,
-                            apply_k=lambda v: fast._apply(0, v))
+        return field_errors(u, von_mises(u), ref_fields[0], ref_fields[1], node_act, elem_act, apply_k=apply_fp64)
+
+    def apply_fp64(v):
+        """K v with the FP64 fine operator (vf_apply, level 0)."""
+        y = np.empty(ndof)
+        _lib.check(L.vf_apply(fast._h, 0, _lib.VF_PREC_FP64, _lib.ptr(np.ascontiguousarray(v, dtype=np.float64)),
+                              _lib.ptr(y)), fast._h)
+        return y
 
     # learned stage + mixed precision (flexible CG with the U-Net stage after
     # each V-cycle), packaged weights; reported beside the mixed solver
@@ -799,7 +827,7 @@ def main():
     ap.add_argument("--no-other-configs", action="store_true",
                     help="skip the single-solve figures of the 192^3 block, 64-part batch and 512x256x256 configs")
     ap.add_argument("--nvtx", action="store_true", help="wrap the timed steps in NVTX range vf_timed")
-    ap.add_argument("--kernel-profile", choices=("apply", "smooth", "resid", "restrict", "prolong", "vcycle"),
+    ap.add_argument("--kernel-profile", choices=("apply", "smooth", "resid", "restrict", "prolong", "vcycle", "learned"),
                     help="set up, then run one kernel 3x inside NVTX range vf_kernel and exit")
     ap.add_argument("--kernel-precision", choices=("fp32", "fp64"), default="fp32")
     ap.add_argument("--modal-zchunk", type=int, default=0, help="z-planes per CTA of the modal kernel (0 = auto)")
