@@ -182,6 +182,7 @@ __global__ void __launch_bounds__(TX * TY, 2)
 
   P hiPrev[3][4];
   double dot = 0.0;
+  uint8_t mk_next[L];
 
   // false: this step's copies did not arrive in time (every thread agrees)
   auto step = [&](const int s, P (&Fc)[3][4], const P (&Fp)[3][4]) -> bool {
@@ -191,11 +192,15 @@ __global__ void __launch_bounds__(TX * TY, 2)
     // the barrier also marks step s-1 done everywhere: stage (s+2) is free
     if (__syncthreads_or(!arrived)) return false;
     if (leader && s + 2 < nsteps) issue(s + 2);
+    // free-mask bytes: this step's were loaded one step ahead (mk_next),
+    // the next step's are requested now, far from their use
     uint8_t mk[L];
 #pragma unroll
     for (int l = 0; l < L; ++l) {
-      const int zs = z0[l] + s - 1;
-      mk[l] = (s >= 2 && out_col && zs < oend[l]) ? mask[(zs + 1) * sz + colbase] : (uint8_t)0;
+      mk[l] = mk_next[l];
+      const int zs = z0[l] + s;   // output plane of step s + 1
+      mk_next[l] = (s + 1 >= 2 && s + 1 < nsteps && out_col && zs < oend[l]) ? __ldg(mask + (zs + 1) * sz + colbase)
+                                                                             : (uint8_t)0;
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -330,6 +335,8 @@ __global__ void __launch_bounds__(TX * TY, 2)
       issue(0);
       issue(1);
     }
+#pragma unroll
+    for (int l = 0; l < L; ++l) mk_next[l] = 0;   // steps 0 and 1 write no output
 #pragma unroll 1
     for (int s = 0; s < nsteps; ++s) {
       if (!step(s, Fa, Fb)) {

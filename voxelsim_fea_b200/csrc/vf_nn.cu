@@ -1,26 +1,20 @@
 // 3x3x3 convolutions of the learned preconditioner stage: BF16 operands,
-// FP32 accumulation on the tensor cores (mma.m16n8k16), implicit GEMM.
+// FP32 accumulation on the tensor cores, implicit GEMM.
 //
 // Activations are channels-last BF16 tensors [Z][Y][X][C] (C = 16, 32 or 64),
 // zero outside the box (the halo loads fill zeros: "same" padding).  Weights
 // are [27][COUT][CIN] BF16 (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)), so the
-// input-channel axis -- the GEMM K axis -- is contiguous for the B operand.
+// input-channel axis -- the GEMM K axis -- is contiguous.
 //
-// Forward (and backward-data, which is the forward of dY with the weights
-// transposed and the taps mirrored): a CTA computes a 16 x 8 x 2 voxel tile;
-// warp w owns two 16-voxel x-rows (GEMM M = 16 voxels per row) times all
-// COUT output channels (N).  The input halo (18 x 10 x 4 voxels) and the 9
-// weight taps of one dz plane live in shared memory with a channel stride
-// padded by 8 (16 bytes), so every ldmatrix phase reads 8 rows spread over
-// all 32 banks.  K loops over taps and 16-channel chunks.  The epilogue adds
-// the bias and an optional skip tensor, then applies ReLU (forward) or the
-// ReLU gate of the saved activation (backward), and stores BF16 pairs.
+// Forward and backward-data (the forward of dY with the weights transposed
+// and the taps mirrored) run on tcgen05 with TMEM accumulators
+// (vf_nn_tc.cu); this file keeps the dispatch and the weight gradient.
 //
 // Backward-weight: dW[tap][co][ci] = sum_v dY[v][co] X[v + off(tap)][ci] is a
-// GEMM with M = co, N = ci and K = voxels.  A CTA takes a group of taps and
-// a strided set of voxel tiles; both operands come out of shared memory
-// through ldmatrix.trans.  Per-CTA partial sums are reduced in a fixed order
-// (deterministic).
+// GEMM with M = co, N = ci and K = voxels (mma.m16n8k16).  A CTA takes a group
+// of taps and a strided set of voxel tiles; both operands come out of shared
+// memory through ldmatrix.trans.  Per-CTA partial sums are reduced in a fixed
+// order (deterministic).
 #include <cuda_bf16.h>
 
 #include <atomic>
@@ -41,10 +35,6 @@ constexpr int NTHREADS = 256;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void ldsm_x4(unsigned a, unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3) {
-  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
-}
 __device__ __forceinline__ void ldsm_x4_t(unsigned a, unsigned& r0, unsigned& r1, unsigned& r2, unsigned& r3) {
   asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
                : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "r"(a));
@@ -80,125 +70,6 @@ __device__ __forceinline__ void load_halo(bf16* s, const bf16* __restrict__ g, i
 
 __device__ __forceinline__ int halo_index(int hx, int hy, int hz) { return (hz * HTY + hy) * HTX + hx; }
 
-template <int CIN, int COUT>
-constexpr size_t conv_smem_bytes() {
-  return sizeof(bf16) * ((size_t)NHALO * (CIN + 8) + (size_t)9 * COUT * (CIN + 8));
-}
-
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(NTHREADS) k_conv3(NnConvArgs a) {
-  constexpr int CP = CIN + 8;
-  constexpr int NT = COUT / 8;       // n-tiles of 8 output channels
-  if (a.skip_flag && *a.skip_flag) return;
-  extern __shared__ __align__(16) unsigned char smem[];
-  bf16* sIn = reinterpret_cast<bf16*>(smem);
-  bf16* sW = sIn + NHALO * CP;       // [9][COUT][CP]
-  const int X = a.X, Y = a.Y, Z = a.Z;
-  const int tx = (X + OTX - 1) / OTX, ty = (Y + OTY - 1) / OTY;
-  const int X0 = (blockIdx.x % tx) * OTX, Y0 = ((blockIdx.x / tx) % ty) * OTY, Z0 = (blockIdx.x / (tx * ty)) * OTZ;
-  const bf16* __restrict__ in = reinterpret_cast<const bf16*>(a.in);
-  const bf16* __restrict__ w = reinterpret_cast<const bf16*>(a.w);
-  load_halo<CIN, CP>(sIn, in, X, Y, Z, X0, Y0, Z0);
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float acc[2][NT][4];
-#pragma unroll
-  for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int n = 0; n < NT; ++n)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) acc[r][n][k] = 0.f;
-  // ldmatrix row of this lane inside a 16 x 16 A tile: voxel (lane&7) + 8*bit3, k offset 8*bit4
-  const int a_row = (lane & 7) + ((lane >> 3) & 1) * 8;
-  const int a_col = (lane >> 4) * 8;
-  // B: weight row n = (lane&7) + 8*bit4 inside a 16-channel pair, k offset 8*bit3
-  const int b_row = (lane & 7) + ((lane >> 4) & 1) * 8;
-  const int b_col = ((lane >> 3) & 1) * 8;
-  int rowy[2], rowz[2];
-#pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int row = warp * 2 + r;
-    rowy[r] = row % OTY;
-    rowz[r] = row / OTY;
-  }
-
-#pragma unroll 1
-  for (int dz = 0; dz < 3; ++dz) {
-    __syncthreads();   // previous plane's weights consumed (first pass: halo stores ordered)
-    {
-      constexpr int CH = CIN / 8;
-      const bf16* wsrc = w + (long long)dz * 9 * COUT * CIN;
-      for (int i = threadIdx.x; i < 9 * COUT * CH; i += NTHREADS) {
-        const int row = i / CH, c = i - row * CH;
-        *reinterpret_cast<uint4*>(sW + row * CP + c * 8) =
-            __ldg(reinterpret_cast<const uint4*>(wsrc + (long long)row * CIN) + c);
-      }
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int t9 = 0; t9 < 9; ++t9) {
-      const int dy = t9 / 3, dx = t9 % 3;   // halo offsets 0..2 (== d + 1)
-      const bf16* wt = sW + t9 * COUT * CP;
-#pragma unroll
-      for (int kc = 0; kc < CIN / 16; ++kc) {
-        unsigned af[2][4];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          const int hv = halo_index(a_row + dx, rowy[r] + dy, rowz[r] + dz);
-          ldsm_x4(smem_u32(sIn + hv * CP + kc * 16 + a_col), af[r][0], af[r][1], af[r][2], af[r][3]);
-        }
-#pragma unroll
-        for (int np = 0; np < NT / 2; ++np) {
-          unsigned b0, b1, b2, b3;
-          ldsm_x4(smem_u32(wt + (np * 16 + b_row) * CP + kc * 16 + b_col), b0, b1, b2, b3);
-#pragma unroll
-          for (int r = 0; r < 2; ++r) {
-            mma16816(acc[r][2 * np], af[r][0], af[r][1], af[r][2], af[r][3], b0, b1);
-            mma16816(acc[r][2 * np + 1], af[r][0], af[r][1], af[r][2], af[r][3], b2, b3);
-          }
-        }
-      }
-    }
-  }
-
-  // epilogue: thread holds rows g, g+8 (x), channel pair 2*tig (+8*n)
-  const bf16* __restrict__ skip = reinterpret_cast<const bf16*>(a.skip);
-  const bf16* __restrict__ gate = reinterpret_cast<const bf16*>(a.gate);
-  bf16* __restrict__ out = reinterpret_cast<bf16*>(a.out);
-  const int g = lane >> 2, tig = lane & 3;
-#pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int y = Y0 + rowy[r], z = Z0 + rowz[r];
-    if (y >= Y || z >= Z) continue;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int x = X0 + g + 8 * h;
-      if (x >= X) continue;
-      const long long vo = (((long long)z * Y + y) * X + x) * COUT;
-#pragma unroll
-      for (int n = 0; n < NT; ++n) {
-        const int co = n * 8 + 2 * tig;
-        float v0 = acc[r][n][2 * h], v1 = acc[r][n][2 * h + 1];
-        if (a.bias) { v0 += a.bias[co]; v1 += a.bias[co + 1]; }
-        if (skip) {
-          const float2 s2 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(skip + vo + co));
-          v0 += s2.x; v1 += s2.y;
-        }
-        if (a.relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
-        if (gate) {
-          const float2 g2 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(gate + vo + co));
-          v0 = g2.x > 0.f ? v0 : 0.f;
-          v1 = g2.y > 0.f ? v1 : 0.f;
-        }
-        if (a.out_f32) { a.out_f32[vo + co] = v0; a.out_f32[vo + co + 1] = v1; }
-        else *reinterpret_cast<__nv_bfloat162*>(out + vo + co) = __floats2bfloat162_rn(v0, v1);
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// backward-weight
 // ---------------------------------------------------------------------------
 template <int CIN, int COUT>
 struct WgradCfg {
@@ -296,17 +167,6 @@ __global__ void k_reduce_partials(const float* __restrict__ partial, int nparts,
     for (int b = 0; b < nparts; ++b) s += partial[(long long)b * n + i];
     out[i] = accumulate ? out[i] + s : s;
   }
-}
-
-template <int CIN, int COUT>
-int conv_forward_t(const NnConvArgs& a, cudaStream_t st) {
-  constexpr size_t smem = conv_smem_bytes<CIN, COUT>();
-  static std::atomic<int> per_dev[kMaxDevices];
-  kernel_prepare(per_dev, k_conv3<CIN, COUT>, smem, NTHREADS);
-  const long long tiles = (long long)((a.X + OTX - 1) / OTX) * ((a.Y + OTY - 1) / OTY) * ((a.Z + OTZ - 1) / OTZ);
-  if (tiles <= 0) return 0;
-  launch_k(k_conv3<CIN, COUT>, dim3((unsigned)tiles), dim3(NTHREADS), smem, st, a);
-  return 0;
 }
 
 template <int CIN, int COUT>
