@@ -226,10 +226,180 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(NnConvArgs a) {
                  : "memory");
 }
 
+// The same GEMM marching a column of ZC output planes: all 27 weight taps stay
+// resident, the input planes live in a 3-slot ring (plane p in slot p % 3),
+// and each step stages one new plane before its 27 x CIN/16 MMAs.  For the
+// channel pairs whose 27 taps fit in shared memory next to the ring.
+template <int CIN, int COUT>
+struct TczLayout {
+  static constexpr int KC = CIN / 8;
+  static constexpr uint32_t ROW = HCX * 16;
+  static constexpr uint32_t CHUNK_A = HCY * ROW;
+  static constexpr uint32_t PLANE = KC * CHUNK_A;
+  static constexpr uint32_t IN_BYTES = 3 * PLANE;
+  static constexpr uint32_t CHUNK_B = COUT * 16;
+  static constexpr uint32_t TAP_B = KC * CHUNK_B;
+  static constexpr uint32_t W_BYTES = 27 * TAP_B;
+  static constexpr int TCOLS = COUT < 32 ? 32 : COUT;
+  static constexpr size_t smem() { return 1024 + (size_t)IN_BYTES + W_BYTES + 64; }
+  static constexpr bool fits() { return smem() <= 200 * 1024; }
+  static_assert(TCOLS >= 32 && TCOLS <= 512, "TMEM columns");
+};
+constexpr int kZC = 8;   // output planes per CTA
+
+template <int CIN, int COUT>
+__device__ __forceinline__ void stage_plane(unsigned char* sIn, const bf16* __restrict__ in, int X, int Y, int Z,
+                                            int X0, int Y0, int zz) {
+  using L = TczLayout<CIN, COUT>;
+  unsigned char* dst = sIn + ((zz + 3) % 3) * L::PLANE;
+  for (int i = threadIdx.x; i < L::KC * HCY * HCX; i += kTcThreads) {
+    const int v = i % (HCY * HCX), kc = i / (HCY * HCX);
+    const int hx = v % HCX, hy = v / HCX;
+    const int x = X0 - 1 + hx, y = Y0 - 1 + hy;
+    uint4 val = make_uint4(0u, 0u, 0u, 0u);
+    if (x >= 0 && x < X && y >= 0 && y < Y && zz >= 0 && zz < Z)
+      val = __ldg(reinterpret_cast<const uint4*>(in + (((long long)zz * Y + y) * X + x) * CIN) + kc);
+    *reinterpret_cast<uint4*>(dst + kc * L::CHUNK_A + hy * L::ROW + hx * 16) = val;
+  }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kTcThreads) k_conv3_tcz(NnConvArgs a) {
+  using L = TczLayout<CIN, COUT>;
+  static_assert(COUT % 16 == 0 && COUT >= 16 && COUT <= 256, "N of an M = 128 BF16 MMA");
+  static_assert(CIN % 16 == 0, "K steps of 16 channels");
+  if (a.skip_flag && *a.skip_flag) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* sIn = base;
+  unsigned char* sW = base + L::IN_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sW + L::W_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sW + L::W_BYTES + 16);
+
+  const int X = a.X, Y = a.Y, Z = a.Z;
+  const int ntx = (X + TCX - 1) / TCX, nty = (Y + TCY - 1) / TCY;
+  const int X0 = (blockIdx.x % ntx) * TCX, Y0 = ((blockIdx.x / ntx) % nty) * TCY;
+  const int zb = (blockIdx.x / (ntx * nty)) * kZC, ze = min(zb + kZC, Z);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bf16* __restrict__ in = reinterpret_cast<const bf16*>(a.in);
+  const bf16* __restrict__ w = reinterpret_cast<const bf16*>(a.w);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(s32(tslot)),
+                 "r"((uint32_t)L::TCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(s32(bar)), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  // all 27 taps: sW[tap][kc][n][8]
+  for (int i = threadIdx.x; i < 27 * L::KC * COUT; i += kTcThreads) {
+    const int n = i % COUT, rest = i / COUT, kc = rest % L::KC, tap = rest / L::KC;
+    *reinterpret_cast<uint4*>(sW + tap * L::TAP_B + kc * L::CHUNK_B + n * 16) =
+        __ldg(reinterpret_cast<const uint4*>(w + ((long long)tap * COUT + n) * CIN) + kc);
+  }
+  stage_plane<CIN, COUT>(sIn, in, X, Y, Z, X0, Y0, zb - 1);
+  stage_plane<CIN, COUT>(sIn, in, X, Y, Z, X0, Y0, zb);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = *tslot;
+  constexpr uint32_t idesc = idesc_bf16<COUT>();
+  const bf16* __restrict__ skip = reinterpret_cast<const bf16*>(a.skip);
+  const bf16* __restrict__ gate = reinterpret_cast<const bf16*>(a.gate);
+  bf16* __restrict__ out = reinterpret_cast<bf16*>(a.out);
+  const int m = warp * 32 + lane;
+  const int x = X0 + m % TCX, y = Y0 + m / TCX;
+  const bool valid = x < X && y < Y;
+  bool failed = false;
+
+#pragma unroll 1
+  for (int z = zb; z < ze; ++z) {
+    // plane z+1 into the slot of plane z-2 (read by the previous step's MMAs,
+    // which completed before that step's epilogue)
+    stage_plane<CIN, COUT>(sIn, in, X, Y, Z, X0, Y0, z + 1);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (threadIdx.x == 0) {
+      const uint32_t b0 = s32(sW);
+#pragma unroll 1
+      for (int tap = 0; tap < 27; ++tap) {
+        const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+        const uint32_t a0 = s32(sIn) + ((z - 1 + dz + 3) % 3) * L::PLANE;
+#pragma unroll
+        for (int kk = 0; kk < CIN / 16; ++kk) {
+          const uint64_t ad = umma_desc(a0 + dy * L::ROW + dx * 16 + 2 * kk * L::CHUNK_A, L::CHUNK_A, L::ROW);
+          const uint64_t bd = umma_desc(b0 + tap * L::TAP_B + 2 * kk * L::CHUNK_B, L::CHUNK_B, 128);
+          mma_bf16(tmem, ad, bd, idesc, (tap | kk) != 0 ? 1u : 0u);
+        }
+      }
+      mma_commit(bar);
+    }
+    const unsigned par = (unsigned)((z - zb) & 1);
+    const bool ok = mbar_wait_bounded(bar, par);
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      if (threadIdx.x == 0 && a.err) atomicExch(a.err, 1);
+      mbar_wait_bounded(bar, par);   // let the issued MMAs land before TMEM is freed
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const long long vo = (((long long)z * Y + y) * X + x) * COUT;
+#pragma unroll
+    for (int c0 = 0; c0 < COUT; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (!valid) continue;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        float t = v[j];
+        if (a.bias) t += a.bias[c0 + j];
+        if (skip) t += __bfloat162float(skip[vo + c0 + j]);
+        if (a.relu) t = fmaxf(t, 0.f);
+        if (gate) t = __bfloat162float(gate[vo + c0 + j]) > 0.f ? t : 0.f;
+        v[j] = t;
+      }
+      if (a.out_f32) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 4)
+          *reinterpret_cast<float4*>(a.out_f32 + vo + c0 + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+      } else {
+        uint4 pk[2];
+        __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(pk);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        *reinterpret_cast<uint4*>(out + vo + c0) = pk[0];
+        *reinterpret_cast<uint4*>(out + vo + c0 + 8) = pk[1];
+      }
+    }
+    // every lane's TMEM reads of this step are done before the next MMAs overwrite D
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  }
+  (void)failed;
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"((uint32_t)L::TCOLS)
+                 : "memory");
+}
+
 }  // namespace
 
 template <int CIN, int COUT>
 int conv_forward_tc(const NnConvArgs& a, cudaStream_t st) {
+  if constexpr (TczLayout<CIN, COUT>::fits()) {
+    using LZ = TczLayout<CIN, COUT>;
+    static std::atomic<int> per_dev_z[kMaxDevices];
+    kernel_prepare(per_dev_z, k_conv3_tcz<CIN, COUT>, LZ::smem(), kTcThreads);
+    const long long tiles = (long long)((a.X + TCX - 1) / TCX) * ((a.Y + TCY - 1) / TCY) * ((a.Z + kZC - 1) / kZC);
+    if (tiles <= 0) return 0;
+    launch_k(k_conv3_tcz<CIN, COUT>, dim3((unsigned)tiles), dim3(kTcThreads), LZ::smem(), st, a);
+    return 0;
+  }
   using L = TcLayout<CIN, COUT>;
   static std::atomic<int> per_dev[kMaxDevices];
   kernel_prepare(per_dev, k_conv3_tc<CIN, COUT>, L::smem(), kTcThreads);
