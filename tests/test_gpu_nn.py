@@ -60,6 +60,24 @@ def test_conv_forward_and_gradients(gpu, cin, cout):
     assert _rel(dw, dw_ref) < 1e-5
 
 
+@pytest.mark.parametrize("cin,cout", PAIRS)
+def test_conv_forward_z_columns(gpu, cin, cout):
+    """Forward over several columns of output planes (the z-marching form
+    takes 8 planes per CTA): 19 planes = two full columns and one of 3, with
+    the epilogue's skip input and ReLU."""
+    from voxelsim_fea_b200.learned import conv
+    torch.manual_seed(cin * 7 + cout)
+    shape = (19, 13, 10)
+    x = torch.randn(*shape, cin, device="cuda").to(torch.bfloat16)
+    w = (torch.randn(27, cout, cin, device="cuda") / (27 * cin) ** 0.5).to(torch.bfloat16)
+    b = torch.randn(cout, device="cuda")
+    skip = torch.randn(*shape, cout, device="cuda").to(torch.bfloat16)
+    y = conv.conv3d_forward(x, w, bias=b, skip=skip, relu=True, out_f32=True)
+    ref = torch.relu(_from_ncdhw(F.conv3d(_to_ncdhw(x), _w_torch(w), b.cpu().double(), padding=1))
+                     + skip.cpu().double())
+    assert _rel(y, ref) < 1e-5
+
+
 def test_conv_epilogues(gpu):
     """bias + skip + ReLU in the forward epilogue; the ReLU gate in backward."""
     from voxelsim_fea_b200.learned import conv

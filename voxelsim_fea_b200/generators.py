@@ -134,6 +134,41 @@ def two_material_part(shape=(512, 256, 256), seed=0, sigma=4.0, vsize=1e-3,
     return prob
 
 
+def drop_unsupported(prob):
+    """The island step every job of the reference passes through before its
+    solve (``core/solve_worker.py:274-287`` calling ``fea.drop_unsupported_islands``,
+    ``core/fea.py:164-227``): keep only the active voxels joined to a support
+    by a chain of face-adjacent active voxels, seeded by every voxel that
+    touches a fixed node.  Material hanging on by an edge or a corner (the
+    26-connected labelling of ``noise_solid`` keeps it) is a hinge whose
+    rigid rotation only the e_min voids resist; this drops it.  The loads and
+    supports are left as they are, as in the reference.  Returns a new dict
+    with ``active`` restricted and ``islands_removed`` = voxels dropped."""
+    from scipy import ndimage
+    nx, ny, nz = prob["dims"]
+    active = prob["active"].reshape(nx, ny, nz)
+    fixed_nodes = np.unique(np.asarray(prob["fixed_dofs"], dtype=np.int64) // 3)
+    node_fixed = np.zeros((nx + 1) * (ny + 1) * (nz + 1), dtype=bool)
+    node_fixed[fixed_nodes] = True
+    node_fixed = node_fixed.reshape(nz + 1, ny + 1, nx + 1).transpose(2, 1, 0)
+    seed = np.zeros((nx, ny, nz), dtype=bool)
+    for ox in (0, 1):
+        for oy in (0, 1):
+            for oz in (0, 1):
+                seed |= node_fixed[ox:ox + nx, oy:oy + ny, oz:oz + nz]
+    lab, _ = ndimage.label(active)          # default structure: 6-connected
+    keep_labels = np.unique(lab[seed & active])
+    keep_labels = keep_labels[keep_labels > 0]
+    out = dict(prob)
+    if keep_labels.size == 0:
+        out["islands_removed"] = 0
+        return out
+    kept = np.isin(lab, keep_labels)
+    out["active"] = kept.ravel()
+    out["islands_removed"] = int(active.sum() - kept.sum())
+    return out
+
+
 def load_cases(prob, k, seed, patch=8, mag=(1e3, 1e4)):
     """(k, ndof) block of right-hand sides on one geometry: unit direction
     uniform on the sphere, magnitude uniform in ``mag``, each on a random

@@ -42,12 +42,17 @@ def part_spec(seed, sizes=SIZES):
     return shape, float(rng.uniform(3.0, 5.0))
 
 
-def make_part(seed, sizes=SIZES, shape=None):
-    """CPU-only geometry / load generation (runs in worker processes)."""
+def make_part(seed, sizes=SIZES, shape=None, drop_islands=False):
+    """CPU-only geometry / load generation (runs in worker processes).
+    ``drop_islands``: pass the part through the reference's island step
+    (``generators.drop_unsupported``) before placing its load, as every job
+    of the reference is before its solve."""
     from .. import generators
     spec_shape, sigma = part_spec(seed, sizes)
     shape = shape or spec_shape
     prob = generators.two_material_part(shape, seed=seed, sigma=sigma)
+    if drop_islands:
+        prob = generators.drop_unsupported(prob)
     f = generators.load_cases(prob, 1, seed + 1)[0]
     E = np.where(prob["active"], prob["E_stiff"], prob["E_stiff"] * 1e-9)
     return {"seed": seed, "dims": shape, "E": E, "nu": np.asarray(prob["nu"], dtype=float),
@@ -207,17 +212,20 @@ def modes_configs():
             ("learned_outer64", SolverOptions.fast(mixed_mode="outer64"), True))
 
 
-def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None, max_cg=None):
+def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None, max_cg=None,
+             drop_islands=True):
     """Solve held-out parts without and with the learned stage (FP64 and
-    mixed precision); per-part iterations and device times."""
+    mixed precision); per-part iterations and device times.  ``max_cg``
+    None is the reference's cap of 1000 iterations; ``drop_islands`` runs
+    each part through the reference's island step first."""
     from ..multigrid import MGSolver
     from . import stage
     rows = []
     configs = configs or eval_configs()
     for s in seeds:
-        part = make_part(s, shape=shape)
+        part = make_part(s, shape=shape, drop_islands=drop_islands)
         nx, ny, nz = part["dims"]
-        row = {"seed": s}
+        row = {"seed": s, "active_voxels": int(np.count_nonzero(part["E"] > part["E"].max() * 1e-6))}
         for name, opts, use in configs:
             m = MGSolver(nx, ny, nz, part["fixed"], nu=0.3, options=opts)
             m.set_density(part["E"], nu_elem=part["nu"])
@@ -236,6 +244,32 @@ def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None, 
     return rows
 
 
+def summarize(rows, configs):
+    """Per configuration: parts converged, mean / median iterations and
+    device solve time, and the summed solve time."""
+    out = {}
+    for k, _, _ in configs:
+        it = [r[k]["iters"] for r in rows]
+        ms = [r[k]["solve_ms"] for r in rows]
+        out[k] = {"converged": int(sum(r[k]["converged"] for r in rows)), "parts": len(rows),
+                  "iters_mean": float(np.mean(it)), "iters_median": float(np.median(it)),
+                  "solve_ms_mean": float(np.mean(ms)), "solve_ms_median": float(np.median(ms)),
+                  "solve_ms_total": float(np.sum(ms))}
+    return out
+
+
+def _report(rows, configs, args):
+    summary = summarize(rows, configs)
+    print(json.dumps(summary), flush=True)
+    if args.eval_json:
+        with open(args.eval_json, "w") as fh:
+            json.dump({"protocol": {"size": args.eval_size, "parts": args.eval, "tol": 1e-8,
+                                    "max_cg": args.max_cg or 1000,
+                                    "islands": "kept (26-connected)" if args.raw_parts else
+                                    "dropped by the reference's island step"},
+                       "rows": rows, "summary": summary}, fh, indent=1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--parts", type=int, default=2000)
@@ -251,24 +285,21 @@ def main():
     ap.add_argument("--eval-size", type=int, default=192)
     ap.add_argument("--eval-json", type=str, default=None)
     ap.add_argument("--eval-only", action="store_true", help="evaluate the packaged weights, no training")
-    ap.add_argument("--max-cg", type=int, default=3000)
+    ap.add_argument("--max-cg", type=int, default=None, help="iteration cap (default: the reference's 1000)")
+    ap.add_argument("--raw-parts", action="store_true",
+                    help="evaluate the generated parts as they are, without the reference's island step")
     ap.add_argument("--configs", choices=("headline", "modes"), default="headline")
+    ap.add_argument("--weights", type=str, default=None, help="weights to evaluate (default: the packaged ones)")
     args = ap.parse_args()
     from . import stage
     if args.eval_only:
-        params, level = stage.load_weights()
+        params, level = stage.load_weights(args.weights) if args.weights else stage.load_weights()
         seeds = [9_000_000 + 7919 * i for i in range(args.eval)]
         e = args.eval_size
         cfgs = headline_configs() if args.configs == "headline" else modes_configs()
-        rows = evaluate(params, level, seeds, (e, e, e), configs=cfgs, max_cg=args.max_cg)
-        summary = {k: {"iters_mean": float(np.mean([r[k]["iters"] for r in rows])),
-                       "solve_ms_mean": float(np.mean([r[k]["solve_ms"] for r in rows])),
-                       "converged": int(sum(r[k]["converged"] for r in rows))}
-                   for k, _, _ in cfgs}
-        print(json.dumps(summary), flush=True)
-        if args.eval_json:
-            with open(args.eval_json, "w") as fh:
-                json.dump({"rows": rows, "summary": summary}, fh, indent=1)
+        rows = evaluate(params, level, seeds, (e, e, e), configs=cfgs, max_cg=args.max_cg,
+                        drop_islands=not args.raw_parts)
+        _report(rows, cfgs, args)
         return
     sizes = tuple(int(v) for v in args.sizes.split(","))
     snaps = tuple(int(v) for v in args.snapshots.split(","))
@@ -283,10 +314,9 @@ def main():
     if args.eval:
         seeds = [9_000_000 + 7919 * i for i in range(args.eval)]   # disjoint from the training seeds
         e = args.eval_size
-        rows = evaluate(params, args.level, seeds, (e, e, e))
-        if args.eval_json:
-            with open(args.eval_json, "w") as fh:
-                json.dump(rows, fh, indent=1)
+        rows = evaluate(params, args.level, seeds, (e, e, e), max_cg=args.max_cg,
+                        drop_islands=not args.raw_parts)
+        _report(rows, eval_configs(), args)
 
 
 if __name__ == "__main__":
