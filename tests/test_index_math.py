@@ -84,39 +84,3 @@ def test_tma_wait_is_bounded_by_one_second():
     assert limit <= 1_000_000_000
     assert hint * polls <= limit
     assert hint <= 10_000          # a poll sleeps at most 10 us
-
-
-def _ceil_half(v):
-    return -((-v) // 2)
-
-
-def _offset_range(lo, hi, R, x, lmax):
-    return max(lo, -R, -x), min(hi, R, lmax - x)
-
-
-def test_wide_setup_offset_ranges():
-    """The smoothed-transfer set-up kernels (vf_wide.cu) loop only over the
-    neighbour offsets that can contribute; restated here against a scan of all
-    offsets with the kernels' own skip tests, per axis, over every fine
-    position, coarse slot and reach in use: the same offsets, in order."""
-    import itertools as it
-    for (Pr, Rf) in ((2, 1), (1, 2), (1, 1)):
-        for lmax in (6, 9):
-            lc = lmax // 2
-            for x in range(lmax + 1):
-                for J in range(lc + 1):
-                    # k_rap_b: i = x + d with ceil((i - Pr) / 2) in [J - Pr, J], d in [-Rf, Rf], i inside
-                    full = [d for d in range(-Rf, Rf + 1) if 0 <= x + d <= lmax
-                            and 0 <= J - _ceil_half(x + d - Pr) <= Pr]
-                    a, b = _offset_range(2 * J - Pr - 1 - x, 2 * J + Pr - x, Rf, x, lmax)
-                    assert full == list(range(a, b + 1)), (Pr, Rf, x, J)
-                    # k_prolong_blocks: |x + d - 2J| <= 1
-                    full = [d for d in range(-Rf, Rf + 1) if 0 <= x + d <= lmax and abs(x + d - 2 * J) <= 1]
-                    a, b = _offset_range(2 * J - x - 1, 2 * J - x + 1, Rf, x, lmax)
-                    assert full == list(range(a, b + 1)), (Pr, Rf, x, J)
-            for X, J in it.product(range(lc + 1), range(lc + 1)):
-                # k_rap_c: i = 2X + o, |o| <= Pr, ceil((i - Pr - Rf) / 2) in [J - Pr - Rf, J], i inside
-                full = [o for o in range(-Pr, Pr + 1) if 0 <= 2 * X + o <= lmax
-                        and 0 <= J - _ceil_half(2 * X + o - Pr - Rf) <= Pr + Rf]
-                a, b = _offset_range(2 * J - Pr - Rf - 1 - 2 * X, 2 * J + Pr + Rf - 2 * X, Pr, 2 * X, lmax)
-                assert full == list(range(a, b + 1)), (Pr, Rf, X, J)

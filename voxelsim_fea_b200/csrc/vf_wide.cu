@@ -75,15 +75,6 @@ __device__ __forceinline__ void decode(const Grid& g, int p, int& x, int& y, int
   z = t / g.py - 1;
 }
 
-// [lo, hi] clipped to [-R, R] and to the offsets that stay inside [0, lmax]
-// from x: the neighbour offsets of one axis that can contribute.  Loops over
-// these ranges visit the contributing terms in the same order as a loop over
-// all offsets that skips the others, so the sums are bit-identical.
-__device__ __forceinline__ void offset_range(int lo, int hi, int R, int x, int lmax, int& a, int& b) {
-  a = max(max(lo, -R), -x);
-  b = min(min(hi, R), lmax - x);
-}
-
 inline int blocks_for(long long n, int threads, long long cap = 148LL * 64) {
   long long b = (n + threads - 1) / threads;
   if (b > cap) b = cap;
@@ -154,20 +145,13 @@ __global__ void __launch_bounds__(kSetupThreads) k_prolong_blocks(Grid f, const 
 #pragma unroll
         for (int k = 0; k < 9; ++k) acc[k] = 0.0;
         const double* A = sA + (long long)nl * NB * 9;
-        // neighbours i + d with a non-zero trilinear weight: |i + d - 2J| <= 1
-        int x0, x1, y0, y1, z0, z1;
-        offset_range(2 * Jx - x - 1, 2 * Jx - x + 1, Rf, x, f.lx, x0, x1);
-        offset_range(2 * Jy - y - 1, 2 * Jy - y + 1, Rf, y, f.ly, y0, y1);
-        offset_range(2 * Jz - z - 1, 2 * Jz - z + 1, Rf, z, f.lz, z0, z1);
-        for (int dz = z0; dz <= z1; ++dz)
-          for (int dy = y0; dy <= y1; ++dy)
-            for (int dx = x0; dx <= x1; ++dx) {
-              const int s = ((dz + Rf) * W + (dy + Rf)) * W + (dx + Rf);
-              const double wk = tw(x + dx - 2 * Jx) * tw(y + dy - 2 * Jy) * tw(z + dz - 2 * Jz);
-              if (wk == 0.0) continue;
+        for (int s = 0; s < NB; ++s) {
+          const int dx = s % W - Rf, dy = (s / W) % W - Rf, dz = s / (W * W) - Rf;
+          const double wk = tw(x + dx - 2 * Jx) * tw(y + dy - 2 * Jy) * tw(z + dz - 2 * Jz);
+          if (wk == 0.0 || !inside(f, x + dx, y + dy, z + dz)) continue;
 #pragma unroll
-              for (int k = 0; k < 9; ++k) acc[k] += wk * A[s * 9 + k];
-            }
+          for (int k = 0; k < 9; ++k) acc[k] += wk * A[s * 9 + k];
+        }
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           const double mr = minvf[3LL * p + r];
@@ -208,26 +192,19 @@ __global__ void __launch_bounds__(kSetupThreads) k_rap_b(Grid f, const double* _
     for (int k = 0; k < 9; ++k) acc[k] = 0.0;
     if (inside(c, Jx, Jy, Jz)) {
       const double* As = sA + (long long)nl * NB * 9;
-      // neighbours i = k + d whose P_s slots reach J: ceil((i - Pr) / 2) in [J - Pr, J]
-      int x0, x1, y0, y1, z0, z1;
-      offset_range(2 * Jx - Pr - 1 - x, 2 * Jx + Pr - x, Rf, x, f.lx, x0, x1);
-      offset_range(2 * Jy - Pr - 1 - y, 2 * Jy + Pr - y, Rf, y, f.ly, y0, y1);
-      offset_range(2 * Jz - Pr - 1 - z, 2 * Jz + Pr - z, Rf, z, f.lz, z0, z1);
-      for (int dz = z0; dz <= z1; ++dz)
-        for (int dy = y0; dy <= y1; ++dy)
-          for (int dx = x0; dx <= x1; ++dx) {
-            const int s = ((dz + Rf) * W + (dy + Rf)) * W + (dx + Rf);
-            const int ix = x + dx, iy = y + dy, iz = z + dz;
-            const int ax = Jx - ceil_half(ix - Pr), ay = Jy - ceil_half(iy - Pr), az = Jz - ceil_half(iz - Pr);
-            if (ax < 0 || ax > Pr || ay < 0 || ay > Pr || az < 0 || az > Pr) continue;
-            const double* P = psb + ((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9;
-            const double* A = As + s * 9;
+      for (int s = 0; s < NB; ++s) {
+        const int ix = x + s % W - Rf, iy = y + (s / W) % W - Rf, iz = z + s / (W * W) - Rf;
+        if (!inside(f, ix, iy, iz)) continue;
+        const int ax = Jx - ceil_half(ix - Pr), ay = Jy - ceil_half(iy - Pr), az = Jz - ceil_half(iz - Pr);
+        if (ax < 0 || ax > Pr || ay < 0 || ay > Pr || az < 0 || az > Pr) continue;
+        const double* P = psb + ((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9;
+        const double* A = As + s * 9;
 #pragma unroll
-            for (int r = 0; r < 3; ++r)
+        for (int r = 0; r < 3; ++r)
 #pragma unroll
-              for (int cc = 0; cc < 3; ++cc)
-                acc[3 * r + cc] += A[3 * r] * P[cc] + A[3 * r + 1] * P[3 + cc] + A[3 * r + 2] * P[6 + cc];
-          }
+          for (int cc = 0; cc < 3; ++cc)
+            acc[3 * r + cc] += A[3 * r] * P[cc] + A[3 * r + 1] * P[3 + cc] + A[3 * r + 2] * P[6 + cc];
+      }
     }
     double* out = bsb + ((long long)p * NSB + b) * 9;
 #pragma unroll
@@ -273,17 +250,9 @@ __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const dou
 #pragma unroll
       for (int k = 0; k < 9; ++k) acc[k] = 0.0;
       if (inside(c, Jx, Jy, Jz)) {
-        // fine nodes i = 2I + o (|o| <= Pr) whose B slots reach J:
-        // ceil((i - Pr - Rf) / 2) in [J - Pr - Rf, J]
-        int ox0, ox1, oy0, oy1, oz0, oz1;
-        offset_range(2 * Jx - Pr - Rf - 1 - 2 * X, 2 * Jx + Pr + Rf - 2 * X, Pr, 2 * X, f.lx, ox0, ox1);
-        offset_range(2 * Jy - Pr - Rf - 1 - 2 * Y, 2 * Jy + Pr + Rf - 2 * Y, Pr, 2 * Y, f.ly, oy0, oy1);
-        offset_range(2 * Jz - Pr - Rf - 1 - 2 * Z, 2 * Jz + Pr + Rf - 2 * Z, Pr, 2 * Z, f.lz, oz0, oz1);
-        for (int oz = oz0; oz <= oz1; ++oz)
-          for (int oy = oy0; oy <= oy1; ++oy)
-            for (int ox = ox0; ox <= ox1; ++ox) {
-          const int i = ((oz + Pr) * WI + (oy + Pr)) * WI + (ox + Pr);
-          const int ix = 2 * X + ox, iy = 2 * Y + oy, iz = 2 * Z + oz;
+        for (int i = 0; i < NI; ++i) {
+          const int ix = 2 * X + i % WI - Pr, iy = 2 * Y + (i / WI) % WI - Pr, iz = 2 * Z + i / (WI * WI) - Pr;
+          if (!inside(f, ix, iy, iz)) continue;
           const int bx = Jx - ceil_half(ix - Pr - Rf), by = Jy - ceil_half(iy - Pr - Rf);
           const int bz = Jz - ceil_half(iz - Pr - Rf);
           if (bx < 0 || bx >= NBA || by < 0 || by >= NBA || bz < 0 || bz >= NBA) continue;
@@ -297,7 +266,7 @@ __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const dou
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc)
               acc[3 * r + cc] += P[r] * Bv[cc] + P[3 + r] * Bv[3 + cc] + P[6 + r] * Bv[6 + cc];
-            }
+        }
       }
 #pragma unroll
       for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * nc + pI] = acc[k];
