@@ -60,12 +60,15 @@ def test_conv_forward_and_gradients(gpu, cin, cout):
     assert _rel(dw, dw_ref) < 1e-5
 
 
+@pytest.mark.parametrize("form", ["column", "plane"])
 @pytest.mark.parametrize("cin,cout", PAIRS)
-def test_conv_forward_z_columns(gpu, cin, cout):
-    """Forward over several columns of output planes (the z-marching form
-    takes 8 planes per CTA): 19 planes = two full columns and one of 3, with
-    the epilogue's skip input and ReLU."""
+def test_conv_forward_z_columns(gpu, monkeypatch, cin, cout, form):
+    """Both forward forms (VOXFEA_CONV_FORM: one output plane per CTA, or a
+    column of 8 planes marched with the taps resident -- on its own only on
+    boxes large enough to fill the GPU with columns) over 19 planes = two
+    full columns and one of 3, with the epilogue's skip input and ReLU."""
     from voxelsim_fea_b200.learned import conv
+    monkeypatch.setenv("VOXFEA_CONV_FORM", form)
     torch.manual_seed(cin * 7 + cout)
     shape = (19, 13, 10)
     x = torch.randn(*shape, cin, device="cuda").to(torch.bfloat16)

@@ -24,6 +24,8 @@
 #include <cuda_bf16.h>
 
 #include <atomic>
+#include <cstdlib>
+#include <cstring>
 
 #include "vf_common.cuh"
 #include "vf_nn.cuh"
@@ -389,16 +391,33 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tcz(NnConvArgs a) {
 
 }  // namespace
 
+// The z-marching form where its columns still give every SM a few CTAs (its
+// steps are serial inside a CTA: on the U-Net's coarse boxes, 135 columns
+// took 52 us where the one-plane form's 918 CTAs took 20 us); else one plane
+// per CTA.
+// VOXFEA_CONV_FORM=plane|column overrides the choice (the tests run both).
+constexpr long long kTczMinColumns = 3LL * 148;
+
+int conv_form_override() {
+  const char* e = std::getenv("VOXFEA_CONV_FORM");
+  if (!e) return 0;
+  if (!std::strcmp(e, "plane")) return 1;
+  if (!std::strcmp(e, "column")) return 2;
+  return 0;
+}
+
 template <int CIN, int COUT>
 int conv_forward_tc(const NnConvArgs& a, cudaStream_t st) {
   if constexpr (TczLayout<CIN, COUT>::fits()) {
     using LZ = TczLayout<CIN, COUT>;
-    static std::atomic<int> per_dev_z[kMaxDevices];
-    kernel_prepare(per_dev_z, k_conv3_tcz<CIN, COUT>, LZ::smem(), kTcThreads);
-    const long long tiles = (long long)((a.X + TCX - 1) / TCX) * ((a.Y + TCY - 1) / TCY) * ((a.Z + kZC - 1) / kZC);
-    if (tiles <= 0) return 0;
-    launch_k(k_conv3_tcz<CIN, COUT>, dim3((unsigned)tiles), dim3(kTcThreads), LZ::smem(), st, a);
-    return 0;
+    const long long cols = (long long)((a.X + TCX - 1) / TCX) * ((a.Y + TCY - 1) / TCY) * ((a.Z + kZC - 1) / kZC);
+    const int ov = conv_form_override();
+    if (ov == 2 || (ov == 0 && cols >= kTczMinColumns)) {
+      static std::atomic<int> per_dev_z[kMaxDevices];
+      kernel_prepare(per_dev_z, k_conv3_tcz<CIN, COUT>, LZ::smem(), kTcThreads);
+      launch_k(k_conv3_tcz<CIN, COUT>, dim3((unsigned)cols), dim3(kTcThreads), LZ::smem(), st, a);
+      return 0;
+    }
   }
   using L = TcLayout<CIN, COUT>;
   static std::atomic<int> per_dev[kMaxDevices];
