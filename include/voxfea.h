@@ -129,7 +129,12 @@ typedef struct vf_options {
                               two coarse spacings apart (125 blocks).  Bit 1 only (level 1 -> 2):
                               needs VF_COARSE_GALERKIN, VF_OMEGA_AUTO and symmetric storage; 0 =
                               trilinear everywhere (default) */
-  int32_t reserved[2];
+  int32_t learned_watch;   /* learned stage on (vf_learned_configure): when the residual has not
+                              halved over this many iterations, the stage is switched off and the
+                              solve continues as plain PCG from its current iterate, within the
+                              same iteration budget (vf_solve_info.outer_iters = the iteration of
+                              the switch); 0 = never (default 64) */
+  int32_t reserved[1];
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };
@@ -144,7 +149,9 @@ typedef struct vf_solve_info {
   int32_t iters;           /* PCG iterations (all inner iterations for MIXED);
                               MGSolver.last_iters (multigrid.py:515)        */
   int32_t outer_iters;     /* MIXED: residual replacements (RELIABLE) or
-                              refinement steps (RESTART), else 0            */
+                              refinement steps (RESTART); with a learned stage
+                              (FP64 or OUTER64): the iteration after which it
+                              was switched off for stagnating (0: stayed on) */
   int32_t converged;       /* MGSolver.last_converged                       */
   int32_t status;          /* VF_OK, VF_ERR_STALLED, VF_ERR_BREAKDOWN, ...   */
   double  resid_ratio;     /* MGSolver.last_resid_ratio (recurrence, or the

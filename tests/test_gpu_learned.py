@@ -64,6 +64,37 @@ def test_solve_with_learned_stage_converges(gpu):
     assert np.abs(sols[True] - ref).max() < 1e-5 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("fast", [False, True])
+def test_learned_stage_falls_back_to_plain_pcg(gpu, fast):
+    """With the stage on, a residual that stops halving over learned_watch
+    iterations switches the stage off and the solve goes on as plain PCG from
+    its current iterate (FP64 PCG and the FP64-outer / FP32-V-cycle mode): a
+    tiny watch window forces the switch early; the solve converges to the
+    plain solve's displacement and reports the switch iteration."""
+    from voxelsim_fea_b200.learned import stage
+    from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions
+    part = _part(4242)
+    nx, ny, nz = part["dims"]
+    preset = SolverOptions.fast if fast else SolverOptions.robust
+    res = {}
+    for watch, use in ((64, False), (1, True), (0, True)):
+        m = MGSolver(nx, ny, nz, part["fixed"], nu=0.3, options=preset(learned_watch=watch))
+        m.set_density(part["E"], nu_elem=part["nu"])
+        if use:
+            stage.enable_default(m)
+        u = m.solve(part["E"], part["f"], tol=1e-8, nu_elem=part["nu"])
+        res[(watch, use)] = (u, m.last_converged, m.last_info.true_resid, int(m.last_info.outer_iters),
+                             m.last_iters)
+        m.close()
+    ref = res[(64, False)][0]
+    u, conv, tr, switched, iters = res[(1, True)]
+    assert conv and tr < 1e-8
+    assert 0 < switched < iters, (switched, iters)
+    assert np.abs(u - ref).max() < 1e-5 * np.abs(ref).max()
+    assert res[(0, True)][3] == 0          # watch off: the stage stays on to the end
+    assert res[(64, False)][3] == 0
+
+
 def _energy_left(m, c, e, r):
     """A-norm error fraction after the optimal step along c: 1 - cos_A^2(c, e)."""
     Ac = m._apply(0, c)

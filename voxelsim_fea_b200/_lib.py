@@ -73,7 +73,8 @@ class VfOptions(ctypes.Structure):
         ("coarse_storage", ctypes.c_int32), ("mixed_mode", ctypes.c_int32),
         ("flexible", ctypes.c_int32), ("autotune", ctypes.c_int32),
         ("smoother", ctypes.c_int32), ("cheb_ratio", ctypes.c_int32),
-        ("smoothed_transfers", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
+        ("smoothed_transfers", ctypes.c_int32), ("learned_watch", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 

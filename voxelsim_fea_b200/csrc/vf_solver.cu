@@ -163,6 +163,7 @@ struct vf_solver {
   vf::NnStage* nn = nullptr;
   int nn_level = 1;
   bool nn_on = false;
+  bool nn_stagnated = false;    // run_chunks stopped a learned-stage solve that stopped progressing
   double* d_nn_eref = nullptr;  // [0] max voxel modulus, [1..] reduction scratch
   int* d_err = nullptr;         // kernels' error flag (expired bounded waits)
   double* d_omega = nullptr;    // damping per level (read by the smoothers)
@@ -547,6 +548,21 @@ void pcg_iteration_outer64(vf_solver* s) {
 int graph_slot(const vf_solver* s, bool fp32) { return use_mg(s) ? (fp32 ? 1 : 0) : 2; }
 constexpr int kSlotOuter64 = 3;
 
+void drop_graph(vf_solver* s, int slot) {
+  if (s->chunk[slot]) {
+    cudaGraphExecDestroy(s->chunk[slot]);
+    s->chunk[slot] = nullptr;
+  }
+}
+
+// A solve with the learned stage that stopped progressing (run_chunks'
+// watch) or that the stall guard stopped: it is the fallback the stage
+// keeps -- plain PCG, the stage switched off, from the current iterate and
+// residual, with the rest of the iteration budget.
+bool learned_fallback_due(const vf_solver* s) {
+  return s->nn_on && (s->nn_stagnated || s->h_ks->status == KS_STALLED);
+}
+
 // Run PCG chunks of `iteration` until the device says done.  Host callbacks
 // see each new history entry.
 int run_chunks(vf_solver* s, void (*iteration)(vf_solver*), int gslot,
@@ -595,6 +611,17 @@ int run_chunks(vf_solver* s, void (*iteration)(vf_solver*), int gslot,
       seen = it;
     }
     if (s->h_ks->done) break;
+    // learned stage on: a residual that has not halved over the last
+    // learned_watch iterations hands the solve to plain PCG (the caller
+    // switches the stage off and continues from the current iterate)
+    const int W = s->o.learned_watch;
+    if (s->nn_on && W > 0 && it > W) {
+      const int base = s->h_ks->it_base;
+      if (!(s->history[base + it - 1] < 0.5 * s->history[base + it - 1 - W])) {
+        s->nn_stagnated = true;
+        break;
+      }
+    }
   }
   return VF_OK;
 }
@@ -1114,6 +1141,7 @@ void vf_options_default(vf_options* o) {
   o->smoother = VF_SMOOTH_JACOBI;
   o->cheb_ratio = 30;
   o->autotune = 1;
+  o->learned_watch = 64;
 }
 
 int vf_destroy(vf_solver* s) {
@@ -1153,7 +1181,8 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
       o.coarsest < 0 || o.coarsest > 1 || o.n_smooth < 0 || o.max_levels < 1 || o.coarse_sweeps < 0 ||
       o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0 ||
       o.fine_kernel < 0 || o.fine_kernel > 2 || o.modal_zchunk < -1 || o.coarse_storage < 0 ||
-      o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 2 || o.smoother < 0 || o.smoother > 1) {
+      o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 2 || o.smoother < 0 || o.smoother > 1 ||
+      o.learned_watch < 0) {
     g_last_error = "invalid vf_options field";
     return VF_ERR_ARG;
   }
@@ -1563,14 +1592,33 @@ int mixed_outer64(vf_solver* s, bool have_x0, double tol, int max_it, double fno
   launch_dot<float>(g, w[1], w[2], s->d_partials, s->ks, SLOT_RZ_INIT, s->st);
   launch_convert<float, double>(w[2], v[3], 3LL * g.n, s->st);      // p = z
   VF_CHECK_LAUNCH();
+  int switched = 0;
   if (max_it > 0) {
     int rc = run_chunks(s, pcg_iteration_outer64, kSlotOuter64, progress, user, tol);
     if (rc) return rc;
+    if (learned_fallback_due(s)) {
+      s->nn_stagnated = false;
+      switched = s->h_ks->it;
+      s->nn_on = false;
+      drop_graph(s, kSlotOuter64);
+      init_ks(*s->h_ks, tol, max_it - switched, use_mg(s) ? s->o.stall_guard : 0, switched, 1.0);
+      s->h_ks->fnorm = 1.0;
+      VF_TRY(cudaMemcpyAsync(s->ks, s->h_ks, sizeof(KrylovState), cudaMemcpyHostToDevice, s->st));
+      launch_convert<double, float>(v[1], w[1], 3LL * g.n, s->st);   // r (current) -> FP32
+      precondition<float>(s, w[1], w[2], nullptr);
+      launch_dot<float>(g, w[1], w[2], s->d_partials, s->ks, SLOT_RZ_INIT, s->st);
+      launch_convert<float, double>(w[2], v[3], 3LL * g.n, s->st);  // p = z: a restart
+      VF_CHECK_LAUNCH();
+      rc = max_it > switched ? run_chunks(s, pcg_iteration_outer64, kSlotOuter64, progress, user, tol) : VF_OK;
+      s->nn_on = true;
+      drop_graph(s, kSlotOuter64);
+      if (rc) return rc;
+    }
   }
   launch_scale64(g, v[0], v[0], fnorm, s->st);                       // x = ||f|| x~
   VF_CHECK_LAUNCH();
-  inf.iters = s->h_ks->it;
-  inf.outer_iters = 0;
+  inf.iters = switched + s->h_ks->it;
+  inf.outer_iters = switched;
   inf.converged = s->h_ks->status == KS_CONVERGED;
   inf.resid_ratio = s->h_ks->it > 0 ? s->h_ks->resid : std::numeric_limits<double>::quiet_NaN();
   status = map_status(s->h_ks->status);
@@ -1655,7 +1703,20 @@ extern "C" int vf_solve_cb(vf_solver* s, const double* f, const double* x0, doub
     VF_CHECK_LAUNCH();
     int rc = pcg_solve<double>(s, tol, max_it, use_mg(s) ? s->o.stall_guard : 0, 0, 1.0, fnorm, progress, user, tol);
     if (rc) return rc;
-    inf.iters = s->h_ks->it;
+    int switched = 0;
+    if (learned_fallback_due(s)) {
+      s->nn_stagnated = false;
+      switched = s->h_ks->it;
+      s->nn_on = false;
+      drop_graph(s, graph_slot(s, false));
+      rc = pcg_solve<double>(s, tol, max_it - switched, use_mg(s) ? s->o.stall_guard : 0, switched, 1.0, fnorm,
+                             progress, user, tol);
+      s->nn_on = true;
+      drop_graph(s, graph_slot(s, false));
+      if (rc) return rc;
+    }
+    inf.iters = switched + s->h_ks->it;
+    inf.outer_iters = switched;
     inf.converged = s->h_ks->status == KS_CONVERGED;
     inf.resid_ratio = s->h_ks->it > 0 ? s->h_ks->resid : std::numeric_limits<double>::quiet_NaN();
     status = map_status(s->h_ks->status);
