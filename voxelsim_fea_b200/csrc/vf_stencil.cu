@@ -595,24 +595,6 @@ __global__ void __launch_bounds__(SX * SY, 4) k_sym_march(Grid g, OpArgs a, cons
   const int x = X0 + tx, y = Y0 + ty;
   const bool active = (x <= g.lx) && (y <= g.ly);
 
-  // The stencil rows of this CTA's planes are requested into L2 up front, one
-  // bulk prefetch per (row, plane): the kernel is latency-bound on its chunk
-  // loads, and this puts the whole column's DRAM reads in flight at once.  A
-  // row of SX nodes spans one or two 32-node groups of the warp-chunked
-  // layout (GB bytes each, contiguous); nothing waits on a prefetch.
-  {
-    constexpr long long GB = 32LL * 128 * (long long)sizeof(S);
-    const int xl = min(X0 + SX, g.lx + 1) - 1;
-    for (int t = tid; t < SY * (ze - zb); t += NTH) {
-      const int yy = Y0 + t % SY, zz = zb + t / SY;
-      if (yy > g.ly) continue;
-      const long long g0 = (long long)g.idx(X0, yy, zz) >> 5, g1 = (long long)g.idx(xl, yy, zz) >> 5;
-      const S* src = stc + g0 * (GB / (long long)sizeof(S));
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"((unsigned)((g1 - g0 + 1) * GB))
-                   : "memory");
-    }
-  }
-
   // halo elements of this thread: in-plane storage offset (or -1)
   int hoff[NL];
   int hsl[NL];
