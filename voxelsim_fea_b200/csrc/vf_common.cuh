@@ -240,7 +240,7 @@ template <typename S, int R>
 void launch_wide_compress(const Grid& g, const double* st, const uint8_t* mask, S* stc,
                           typename WideLayout<S, R>::Q* sqrtd, cudaStream_t st_);
 template <typename T, typename S, int R>
-void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, T* v4, cudaStream_t st);
+void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st);
 int wide_op_grid_blocks(const Grid& g);
 int wide_dense_assemble(const Grid& c, int R, const double* stencil, const uint8_t* cmask, double* A, int n,
                         cudaStream_t st);

@@ -84,7 +84,6 @@ struct Level {
   double* sym64 = nullptr; double* sq64 = nullptr;
   float* sym32 = nullptr; __half* sym16 = nullptr; float* sq32 = nullptr;
   int reach = 1;             // Galerkin stencil reach: 1 (27 blocks) or 2 (125 blocks, vf_wide.cu)
-  double* v4d = nullptr; float* v4f = nullptr;   // reach 2: D^1/2 u, 4 values per node (apply scratch)
   bool smooth_down = false;  // the transfer to the next level uses the smoothed prolongation
   // x, tmp, resid, rhs, and a second temporary for the smoothed restriction
   double* w64[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -245,14 +244,13 @@ int nlev(const vf_solver* s) { return use_mg(s) ? (int)s->L.size() : 1; }
 // ---------------------------------------------------------------------------
 template <typename T> void level_sym_op(vf_solver* s, Level& l, int epi, const OpArgs& a);
 template <> void level_sym_op<double>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
-  if (l.reach == 2) launch_wide_op<double, double, 2>(l.g, epi, a, l.sym64, l.sq64, l.v4d, s->st);
+  if (l.reach == 2) launch_wide_op<double, double, 2>(l.g, epi, a, l.sym64, l.sq64, s->st);
   else launch_stencil_sym_op<double, double>(l.g, epi, a, l.sym64, l.sq64, l.szchunk, s->st);
 }
 template <> void level_sym_op<float>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
   if (l.reach == 2) {
-    if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
-      launch_wide_op<float, __half, 2>(l.g, epi, a, l.sym16, l.sq32, l.v4f, s->st);
-    else launch_wide_op<float, float, 2>(l.g, epi, a, l.sym32, l.sq32, l.v4f, s->st);
+    if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) launch_wide_op<float, __half, 2>(l.g, epi, a, l.sym16, l.sq32, s->st);
+    else launch_wide_op<float, float, 2>(l.g, epi, a, l.sym32, l.sq32, s->st);
   } else if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) {
     launch_stencil_sym_op<float, __half>(l.g, epi, a, l.sym16, l.sq32, l.szchunk, s->st);
   } else {
@@ -743,10 +741,6 @@ int build_levels(vf_solver* s) {
         VF_ALLOC(l.sym64, c64);
         VF_ALLOC(l.sq64, 3 * n);
         VF_ALLOC(l.sq32, 3 * n);
-        if (wide) {
-          VF_ALLOC(l.v4d, 4 * n);
-          VF_ALLOC(l.v4f, 4 * n);
-        }
         if (s->o.coarse_storage == VF_STENCIL_SYM_HALF) VF_ALLOC(l.sym16, c16);
         else VF_ALLOC(l.sym32, c32);
       }
@@ -2241,10 +2235,6 @@ int make_child(vf_solver* m, vf_solver** out) {
       for (int k = 0; k < (l.smooth_down ? 5 : 4); ++k) {
         VF_ALLOC(l.w64[k], 3 * n);
         VF_ALLOC(l.w32[k], 3 * n);
-      }
-      if (l.reach == 2) {
-        VF_ALLOC(l.v4d, 4 * n);
-        VF_ALLOC(l.v4f, 4 * n);
       }
     }
     const Grid& g0 = s->L[0].g;

@@ -453,8 +453,7 @@ struct WideBlocks {
         const int q = g.idx(x + dx, y + dy, z + dz);
         A blk[9];
         load_block<S, A, L, JJ>(stc, v, blk);
-        A v0, v1, v2;
-        V(q, v0, v1, v2);
+        const A v0 = V(q, 0), v1 = V(q, 1), v2 = V(q, 2);
 #pragma unroll
         for (int r = 0; r < 3; ++r) acc[r] += blk[3 * r] * v0 + blk[3 * r + 1] * v1 + blk[3 * r + 2] * v2;
       }
@@ -462,8 +461,7 @@ struct WideBlocks {
         const int q = g.idx(x - dx, y - dy, z - dz);
         A blk[9];
         load_block<S, A, L, JJ>(stc, (long long)q * L::G + lane, blk);
-        A w0, w1, w2;
-        V(q, w0, w1, w2);
+        const A w0 = V(q, 0), w1 = V(q, 1), w2 = V(q, 2);
 #pragma unroll
         for (int c = 0; c < 3; ++c) acc[c] += blk[c] * w0 + blk[3 + c] * w1 + blk[6 + c] * w2;
       }
@@ -478,27 +476,9 @@ struct WideBlocks {
 // transposed blocks of the same lane and slot of the lower neighbours, the
 // partial sums meet through warp shuffles, and lanes 0..2 write component
 // 0..2 of the node.
-// The scaled vector v = D^1/2 u of the level, 4 values per node (x, y, z, 0),
-// so that each neighbour's three values arrive by one 16-byte (FP64: two)
-// load instead of six scalar ones: the apply is L1-throughput-bound.
-template <typename T>
-__global__ void k_wide_pack(Grid g, const T* __restrict__ u, const T* __restrict__ sqd, T* __restrict__ v4,
-                            const KrylovState* ks) {
-  if (ks && ks->done) return;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < g.n; p += (long long)gridDim.x * blockDim.x) {
-    const T a0 = sqd[3 * p] * u[3 * p], a1 = sqd[3 * p + 1] * u[3 * p + 1], a2 = sqd[3 * p + 2] * u[3 * p + 2];
-    if constexpr (sizeof(T) == 4) {
-      reinterpret_cast<float4*>(v4)[p] = make_float4(a0, a1, a2, 0.f);
-    } else {
-      reinterpret_cast<double2*>(v4)[2 * p] = make_double2(a0, a1);
-      reinterpret_cast<double2*>(v4)[2 * p + 1] = make_double2(a2, 0.0);
-    }
-  }
-}
-
 template <typename T, typename S, int R, int EPI>
 __global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __restrict__ stc,
-                                                 const T* __restrict__ sqd, const T* __restrict__ v4) {
+                                                 const T* __restrict__ sqd) {
   using L = WideLayout<S, R>;
   using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
   constexpr int G = L::G;
@@ -513,16 +493,7 @@ __global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __re
   const T* dprev = (const T*)a.dprev;
   T* dout = (T*)a.dout;
   const T c1 = a.c1_dev ? (T)(*a.c1_dev) : (T)0;
-  auto V = [&](int q, A& v0, A& v1, A& v2) {
-    if constexpr (sizeof(T) == 4) {
-      const float4 t = __ldg(reinterpret_cast<const float4*>(v4) + q);
-      v0 = t.x; v1 = t.y; v2 = t.z;
-    } else {
-      const double2 t0 = __ldg(reinterpret_cast<const double2*>(v4) + 2LL * q);
-      const double2 t1 = __ldg(reinterpret_cast<const double2*>(v4) + 2LL * q + 1);
-      v0 = t0.x; v1 = t0.y; v2 = t1.x;
-    }
-  };
+  auto V = [&](int q, int c) -> A { return (A)__ldg(sqd + 3LL * q + c) * (A)__ldg(u + 3LL * q + c); };
   double dot = 0.0;
   // whole warps iterate together (the shuffles need every lane)
   const long long nv = ((long long)g.n * G + 31) / 32 * 32;
@@ -643,18 +614,15 @@ template void launch_wide_compress<float, 2>(const Grid&, const double*, const u
 template void launch_wide_compress<double, 2>(const Grid&, const double*, const uint8_t*, double*, double*, cudaStream_t);
 
 template <typename T, typename S, int R>
-void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, T* v4, cudaStream_t st) {
-  launch_k(k_wide_pack<T>, blocks_for(g.n, 256), 256, 0, st, g, (const T*)a.u, sqrtd, v4, (const KrylovState*)a.ks);
+void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
   const int blocks = wide_op_grid_blocks(g);
-  if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY>, blocks, 128, 0, st, g, a, stc, sqrtd, (const T*)v4);
-  else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH>, blocks, 128, 0, st, g, a, stc, sqrtd, (const T*)v4);
-  else launch_k(k_wide_op<T, S, R, EPI_RESID>, blocks, 128, 0, st, g, a, stc, sqrtd, (const T*)v4);
+  if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else launch_k(k_wide_op<T, S, R, EPI_RESID>, blocks, 128, 0, st, g, a, stc, sqrtd);
 }
-template void launch_wide_op<float, __half, 2>(const Grid&, int, const OpArgs&, const __half*, const float*, float*,
-                                               cudaStream_t);
-template void launch_wide_op<float, float, 2>(const Grid&, int, const OpArgs&, const float*, const float*, float*,
-                                              cudaStream_t);
-template void launch_wide_op<double, double, 2>(const Grid&, int, const OpArgs&, const double*, const double*, double*,
+template void launch_wide_op<float, __half, 2>(const Grid&, int, const OpArgs&, const __half*, const float*, cudaStream_t);
+template void launch_wide_op<float, float, 2>(const Grid&, int, const OpArgs&, const float*, const float*, cudaStream_t);
+template void launch_wide_op<double, double, 2>(const Grid&, int, const OpArgs&, const double*, const double*,
                                                 cudaStream_t);
 int wide_op_grid_blocks(const Grid& g) { return blocks_for((long long)g.n * 8, 128, 148LL * 32); }
 
