@@ -426,8 +426,12 @@ def other_configs(args, local):
     E = mg_modulus(p)
     dt, _ = timed_call(lambda: m.solve_block(E, F, tol=TOL, max_cg=args.max_it or None))
     infos = m.last_block_info
+    dev_s = max(i.device_ms for i in infos) / 1e3
     out["bracket_192_block16"] = {"seconds": dt, "dof_per_case": m.ndof, "cases": 16,
                                   "mdof_per_s": 16 * m.ndof / dt / 1e6,
+                                  "device_solve_seconds": dev_s,
+                                  "device_timing": "CUDA events on each case's stream around its solve, the "
+                                                   "longest case (the shared set-up excluded)",
                                   "iterations_max": max(i.iters for i in infos),
                                   "true_resid_max": max(i.true_resid for i in infos),
                                   "what": "k = 16 concurrent solves sharing one operator set-up (vf_solve_block)"}
@@ -446,7 +450,11 @@ def other_configs(args, local):
     ndof = sum(sv.ndof for sv in solvers)
     dt, _ = timed_call(lambda: solve_batch(solvers, [mg_modulus(q) for q in parts], [q["f"] for q in parts],
                                            tol=TOL, max_cg=args.max_it or None))
+    dev_s = max(sv.last_info.setup_ms + sv.last_info.device_ms for sv in solvers) / 1e3
     out["batch64_parts_32-128"] = {"seconds": dt, "dof": ndof, "mdof_per_s": ndof / dt / 1e6,
+                                   "device_part_seconds_max": dev_s,
+                                   "device_timing": "CUDA events on each part's stream around its set-up and "
+                                                    "solve, the longest part (the parts run concurrently)",
                                    "iterations_max": max(sv.last_iters for sv in solvers),
                                    "true_resid_max": max(sv.last_info.true_resid for sv in solvers),
                                    "what": "independent solvers set up and solved concurrently (vf_solve_batch)"}
