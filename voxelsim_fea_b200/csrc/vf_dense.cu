@@ -44,7 +44,7 @@ __global__ void k_dense_assemble(Grid c, const double* __restrict__ st, const ui
 // 1024 threads, one per (row t, column c) of the block; the panel solve and
 // the block-row solve of the inverse phase then multiply by linv instead of
 // substituting row by row.
-__global__ void __launch_bounds__(NB * NB) k_potrf_diag(double* A, int n, int k, int nb, int* info, double* linv) {
+__global__ void __launch_bounds__(NB * NB, 1) k_potrf_diag(double* A, int n, int k, int nb, int* info, double* linv) {
   __shared__ double L[NB][NB + 1], X[NB][NB + 1];
   const int c = threadIdx.x % NB, t = threadIdx.x / NB;
   L[t][c] = (t < nb && c <= t) ? A[(long long)(k + t) * n + k + c] : 0.0;
@@ -65,14 +65,18 @@ __global__ void __launch_bounds__(NB * NB) k_potrf_diag(double* A, int n, int k,
     if (t > j && t < nb && c > j && c <= t) L[t][c] -= L[t][j] * L[c][j];
     __syncthreads();
   }
-  // X = L^-1, one row per step (all columns at once): X[r][c] for c <= r
+  // X = L^-1 by right-looking substitution: thread (t, c) keeps X[t][c] in a
+  // register; step r finalises row r and every lower row subtracts its
+  // multiple of it -- one FMA and one barrier per step (a row-by-row dot
+  // product per step made each row a 32-long dependent chain)
+  double xv = (t == c) ? 1.0 : 0.0;
   for (int r = 0; r < nb; ++r) {
     if (t == r) {
-      double v = (r == c) ? 1.0 : 0.0;
-      for (int l = c; l < r; ++l) v -= L[r][l] * X[l][c];
-      X[r][c] = (c <= r) ? v / L[r][r] : 0.0;
+      xv = xv / L[r][r];
+      X[r][c] = xv;
     }
     __syncthreads();
+    if (t > r && t < nb) xv = fma(-L[t][r], X[r][c], xv);
   }
   if (t < nb && c <= t) A[(long long)(k + t) * n + k + c] = L[t][c];
   linv[t * NB + c] = (t < nb && c < nb) ? X[t][c] : 0.0;
