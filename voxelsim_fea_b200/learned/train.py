@@ -236,6 +236,8 @@ def evaluate(params, level, seeds, shape, tol=1e-8, verbose=True, configs=None, 
             inf = m.last_info
             row[name] = {"iters": int(inf.iters), "solve_ms": float(inf.device_ms),
                          "true_resid": float(inf.true_resid), "converged": bool(inf.converged)}
+            if use:   # iteration at which the stage was switched off for stagnating (0: stayed on)
+                row[name]["stage_off_at"] = int(inf.outer_iters)
             m.close()
         rows.append(row)
         if verbose:
@@ -255,6 +257,9 @@ def summarize(rows, configs):
                   "iters_mean": float(np.mean(it)), "iters_median": float(np.median(it)),
                   "solve_ms_mean": float(np.mean(ms)), "solve_ms_median": float(np.median(ms)),
                   "solve_ms_total": float(np.sum(ms))}
+        offs = [r[k]["stage_off_at"] for r in rows if "stage_off_at" in r[k]]
+        if offs:
+            out[k]["stage_switched_off"] = int(sum(1 for v in offs if v > 0))
     return out
 
 
@@ -288,7 +293,9 @@ def main():
     ap.add_argument("--max-cg", type=int, default=None, help="iteration cap (default: the reference's 1000)")
     ap.add_argument("--raw-parts", action="store_true",
                     help="evaluate the generated parts as they are, without the reference's island step")
-    ap.add_argument("--configs", choices=("headline", "modes"), default="headline")
+    ap.add_argument("--configs", choices=("headline", "modes", "learned"), default="headline")
+    ap.add_argument("--learned-watch", type=int, default=None,
+                    help="learned_watch of the configurations with the stage on (default: the option's default)")
     ap.add_argument("--weights", type=str, default=None, help="weights to evaluate (default: the packaged ones)")
     args = ap.parse_args()
     from . import stage
@@ -296,7 +303,12 @@ def main():
         params, level = stage.load_weights(args.weights) if args.weights else stage.load_weights()
         seeds = [9_000_000 + 7919 * i for i in range(args.eval)]
         e = args.eval_size
-        cfgs = headline_configs() if args.configs == "headline" else modes_configs()
+        cfgs = {"headline": headline_configs, "modes": modes_configs,
+                "learned": lambda: tuple(c for c in headline_configs() if c[2])}[args.configs]()
+        if args.learned_watch is not None:
+            for _, opts, use in cfgs:
+                if use:
+                    opts.learned_watch = int(args.learned_watch)
         rows = evaluate(params, level, seeds, (e, e, e), configs=cfgs, max_cg=args.max_cg,
                         drop_islands=not args.raw_parts)
         _report(rows, cfgs, args)
