@@ -84,3 +84,45 @@ def test_tma_wait_is_bounded_by_one_second():
     assert limit <= 1_000_000_000
     assert hint * polls <= limit
     assert hint <= 10_000          # a poll sleeps at most 10 us
+
+
+def _trtri_schedule(n, nb=32):
+    """The level schedule of the coarsest inverse's batched triangular
+    inversion (vf_dense.cu, dense_cholesky_inverse): per level g, the pairs
+    (r0, r1, r2) and the scratch offset of each T = L21 Y11."""
+    nbk = (n + nb - 1) // nb
+    levels = []
+    g = 1
+    while g < nbk:
+        pairs, toff = [], 0
+        for p0 in range(0, nbk, 2 * g):
+            r0, r1, r2 = p0 * nb, min((p0 + g) * nb, n), min((p0 + 2 * g) * nb, n)
+            if r1 >= r2:
+                continue
+            pairs.append((r0, r1, r2, toff))
+            toff += (r2 - r1) * (r1 - r0)
+        levels.append((g, pairs, toff))
+        g *= 2
+    return levels
+
+
+def test_coarsest_triangular_inversion_schedule():
+    """Restated on the host: diagonal 32x32 block inverses, then per level
+    Y21 = -Y22 (L21 Y11) over the pairs, give L^-1; the scratch of each level
+    fits the n^2 / 2 + 32 n doubles the work buffer reserves."""
+    import numpy as np
+    rng = np.random.default_rng(0)
+    for n in (5, 32, 33, 100, 259, 300):
+        L = np.tril(rng.standard_normal((n, n))) + n * np.eye(n)
+        Y = np.zeros((n, n))
+        for k in range(0, n, 32):
+            e = min(k + 32, n)
+            Y[k:e, k:e] = np.linalg.inv(L[k:e, k:e])
+        for g, pairs, _ in _trtri_schedule(n):
+            for r0, r1, r2, _ in pairs:
+                T = L[r1:r2, r0:r1] @ Y[r0:r1, r0:r1]
+                Y[r1:r2, r0:r1] = -Y[r1:r2, r1:r2] @ T
+        np.testing.assert_allclose(Y @ L, np.eye(n), atol=1e-12)
+    for n in (5, 33, 4131, 9999, 16384):
+        for g, pairs, toff in _trtri_schedule(n):
+            assert toff <= n * n // 2 + 32 * n, (n, g, toff)

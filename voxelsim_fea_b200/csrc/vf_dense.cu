@@ -6,6 +6,8 @@
 // the factorization runs once per set_material, outside the iteration.
 // Replaces the reference's 30-sweep Jacobi "coarse solve" (core/multigrid.py:428-429)
 // when VF_COARSEST_CHOLESKY is selected.
+#include <algorithm>
+
 #include "vf_common.cuh"
 
 namespace vf {
@@ -146,61 +148,84 @@ __global__ void __launch_bounds__(256) k_syrk_update(double* A, int n, int k, in
     }
 }
 
-// Diagonal block of Y: Y[k:k+nb, 0:ncol] <- L_kk^{-1} Y[k:k+nb, 0:ncol]
-// (a product with linv; each CTA owns 64 columns, read whole before written).
-__global__ void __launch_bounds__(256) k_trsv_block_rows(const double* linv, double* Y, int n, int k, int nb,
-                                                         int ncol) {
-  __shared__ double Li[NB][NB + 1], Yb[NB][64 + 1];
-  const int tid = threadIdx.x;
-  const int c0 = blockIdx.x * 64;
-  for (int e = tid; e < NB * NB; e += 256) Li[e / NB][e % NB] = linv[e];
-  for (int e = tid; e < NB * 64; e += 256) {
-    const int l = e / 64, c = e % 64;
-    Yb[l][c] = (l < nb && c0 + c < ncol) ? Y[(long long)(k + l) * n + c0 + c] : 0.0;
+// Y = L^-1 by recursive doubling over the 32-row block structure (the
+// blocked triangular inversion): with both halves of a block pair already
+// inverted,
+//     [L11 0; L21 L22]^-1 = [Y11 0; -Y22 L21 Y11  Y22],
+// so each level is two batched products over all pairs of the level:
+// T = L21 Y11, then Y21 = -Y22 T.  8 levels for n = 4,131 (16 launches
+// instead of a 130-step substitution whose products had K = 32).
+struct GemmJob {
+  const double* A; const double* B; double* C;   // C (M x N) = alpha A (M x K) B (K x N), row-major
+  int lda, ldb, ldc, M, N, K;
+};
+constexpr int kMaxJobs = 128;
+struct GemmBatch {
+  GemmJob job[kMaxJobs];
+  int count;
+  double alpha;
+  int a_lower, b_lower;   // A / B lower triangular (square): skip the zero part of the K range
+};
+
+// One 64 x 64 output tile per CTA (blockIdx.x: tile of job blockIdx.y),
+// 4 x 4 register blocks, K in chunks of 32 through shared memory.
+__global__ void __launch_bounds__(256) k_gemm_batched(const __grid_constant__ GemmBatch bt) {
+  const GemmJob& jb = bt.job[blockIdx.y];
+  const int tn = (jb.N + TB - 1) / TB, tm = (jb.M + TB - 1) / TB;
+  if ((int)blockIdx.x >= tn * tm) return;
+  const int i0 = ((int)blockIdx.x / tn) * TB, j0 = ((int)blockIdx.x % tn) * TB;
+  int kb = 0, ke = jb.K;
+  if (bt.b_lower) kb = j0;                        // B[k][j] = 0 for k < j
+  if (bt.a_lower) ke = min(ke, i0 + TB);          // A[i][k] = 0 for k > i
+  constexpr int LC = 32;
+  __shared__ double As[TB][LC + 1], Bs[LC][TB + 1];
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+  double acc[4][4] = {};
+  for (int k0 = kb; k0 < ke; k0 += LC) {
+    for (int e = tid; e < TB * LC; e += 256) {
+      const int r = e / LC, l = e % LC;
+      const int gi = i0 + r, gk = k0 + l;
+      As[r][l] = (gi < jb.M && gk < ke) ? jb.A[(long long)gi * jb.lda + gk] : 0.0;
+      const int lr = e / TB, c = e % TB;
+      const int gk2 = k0 + lr, gj = j0 + c;
+      Bs[lr][c] = (gk2 < ke && gj < jb.N) ? jb.B[(long long)gk2 * jb.ldb + gj] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int l = 0; l < LC; ++l) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) a[q] = As[ty + 16 * q][l];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) b[q] = Bs[l][tx + 16 * q];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) acc[q][w] = fma(a[q], b[w], acc[q][w]);
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  const int c = tid % 64, ir = tid / 64;
-  for (int a = 0; a < NB / 4; ++a) {
-    const int i = ir + 4 * a;
-    double v = 0.0;
-    for (int l = 0; l <= i; ++l) v = fma(Li[i][l], Yb[l][c], v);
-    if (i < nb && c0 + c < ncol) Y[(long long)(k + i) * n + c0 + c] = v;
-  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const int i = i0 + ty + 16 * q, j = j0 + tx + 16 * w;
+      if (i < jb.M && j < jb.N) jb.C[(long long)i * jb.ldc + j] = bt.alpha * acc[q][w];
+    }
 }
 
-// Y[i, 0:ncol] -= sum_l L[i][k+l] Y[k+l, 0:ncol] for i >= k+nb.
-// Grid: (column tiles of 64, row tiles of 64 below the block).
-__global__ void __launch_bounds__(256) k_trsm_update(const double* A, double* Y, int n, int k, int nb, int ncol) {
-  const int i0 = k + nb + blockIdx.y * TB, c0 = blockIdx.x * TB;
-  __shared__ double Li[TB][NB + 1], Yk[NB][TB + 1];
-  const int tid = threadIdx.x;
-  for (int e = tid; e < TB * NB; e += 256) {
-    const int r = e / NB, l = e % NB;
-    Li[r][l] = (i0 + r < n && l < nb) ? A[(long long)(i0 + r) * n + k + l] : 0.0;
-    const int lr = e / TB, c = e % TB;
-    Yk[lr][c] = (lr < nb && c0 + c < ncol) ? Y[(long long)(k + lr) * n + c0 + c] : 0.0;
-  }
-  __syncthreads();
-  const int tx = tid % 16, ty = tid / 16;
-  double acc[4][4] = {};
-  for (int l = 0; l < nb; ++l) {
-    double li[4], yk[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) li[a] = Li[ty + 16 * a][l];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) yk[b] = Yk[l][tx + 16 * b];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = fma(li[a], yk[b], acc[a][b]);
-  }
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = i0 + ty + 16 * a, c = c0 + tx + 16 * b;
-      if (i < n && c < ncol) Y[(long long)i * n + c] -= acc[a][b];
+// Y = 0 with the inverted diagonal blocks L_kk^-1 on the diagonal.
+__global__ void k_y_init(double* Y, int n, const double* linv_all) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / n), j = (int)(e % n);
+    double v = 0.0;
+    if (i / NB == j / NB) {
+      const int k = i / NB;
+      v = linv_all[(size_t)k * NB * NB + (i - k * NB) * NB + (j - k * NB)];
     }
+    Y[e] = v;
+  }
 }
 
 // Ainv = Y^T Y (Y lower triangular): Ainv[i][j] = sum_{l >= max(i,j)} Y[l][i] Y[l][j].
@@ -249,12 +274,6 @@ __global__ void __launch_bounds__(256) k_yty(const double* Y, double* Ainv, int 
         Ainv[(long long)j * n + i] = acc[a][b];
       }
     }
-}
-
-__global__ void k_set_identity(double* Y, int n) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * n;
-       e += (long long)gridDim.x * blockDim.x)
-    Y[e] = (e / n == e % n) ? 1.0 : 0.0;
 }
 
 // x = Ainv b on the coarsest level; b gathered into shared memory in FP64.
@@ -306,7 +325,9 @@ int dense_assemble(const Grid& c, const double* stencil, const uint8_t* cmask, d
 
 // Doubles of the work buffer: Y = L^-1 (n x n) and the inverted diagonal
 // blocks (NB x NB each).
-size_t dense_work_count(int n) { return (size_t)n * n + (size_t)((n + NB - 1) / NB) * NB * NB; }
+size_t dense_work_count(int n) {
+  return (size_t)n * n + (size_t)((n + NB - 1) / NB) * NB * NB + (size_t)n * n / 2 + (size_t)NB * n;
+}
 
 // A (n x n, lower part) is overwritten by L; work (dense_work_count(n))
 // receives Y = L^-1 and the inverted diagonal blocks; A <- Y^T Y = A^-1.
@@ -325,17 +346,36 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
       launch_k(k_syrk_update, dim3(tiles, tiles), 256, 0, st, A, n, k, nb);
     }
   }
-  // Y = L^{-1} into work
-  launch_k(k_set_identity, 148 * 4, 256, 0, st, work, n);
-  for (int k = 0; k < n; k += NB) {
-    const int nb = (n - k < NB) ? (n - k) : NB;
-    const int ncol = k + nb;
-    const double* linv = linv_all + (size_t)(k / NB) * NB * NB;
-    launch_k(k_trsv_block_rows, (ncol + 63) / 64, 256, 0, st, linv, work, n, k, nb, ncol);
-    const int rest = n - k - nb;
-    if (rest > 0) {
-      launch_k(k_trsm_update, dim3((ncol + TB - 1) / TB, (rest + TB - 1) / TB), 256, 0, st, A, work, n, k, nb, ncol);
+  // Y = L^{-1} into work: diagonal blocks from the factorization, then the
+  // off-diagonal blocks level by level (T in the scratch after linv_all)
+  launch_k(k_y_init, 148 * 4, 256, 0, st, work, n, (const double*)linv_all);
+  double* tbuf = linv_all + (size_t)((n + NB - 1) / NB) * NB * NB;
+  const int nbk = (n + NB - 1) / NB;
+  for (int g = 1; g < nbk; g *= 2) {
+    GemmBatch b1{}, b2{};
+    b1.alpha = 1.0; b1.b_lower = 1;     // T = L21 Y11
+    b2.alpha = -1.0; b2.a_lower = 1;    // Y21 = -Y22 T
+    int max_tiles = 0;
+    size_t toff = 0;
+    auto flush = [&]() {
+      if (b1.count == 0) return;
+      launch_k(k_gemm_batched, dim3(max_tiles, b1.count), 256, 0, st, b1);
+      launch_k(k_gemm_batched, dim3(max_tiles, b2.count), 256, 0, st, b2);
+      b1.count = b2.count = 0;
+      max_tiles = 0;
+    };
+    for (int p0 = 0; p0 < nbk; p0 += 2 * g) {
+      const int r0 = p0 * NB, r1 = std::min((p0 + g) * NB, n), r2 = std::min((p0 + 2 * g) * NB, n);
+      if (r1 >= r2) continue;
+      const int m = r2 - r1, h = r1 - r0;
+      double* T = tbuf + toff;   // distinct per pair within a level (sum of m h <= n^2 / 4)
+      toff += (size_t)m * h;
+      b1.job[b1.count++] = GemmJob{A + (size_t)r1 * n + r0, work + (size_t)r0 * n + r0, T, n, n, h, m, h, h};
+      b2.job[b2.count++] = GemmJob{work + (size_t)r1 * n + r1, T, work + (size_t)r1 * n + r0, n, h, n, m, h, m};
+      max_tiles = std::max(max_tiles, ((m + TB - 1) / TB) * ((h + TB - 1) / TB));
+      if (b1.count == kMaxJobs) flush();
     }
+    flush();
   }
   // A <- Y^T Y (lower-triangle tiles, mirrored)
   const int tiles = (n + TB - 1) / TB;
