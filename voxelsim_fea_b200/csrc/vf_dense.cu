@@ -47,40 +47,44 @@ __global__ void k_dense_assemble(Grid c, const double* __restrict__ st, const ui
 // the block-row solve of the inverse phase then multiply by linv instead of
 // substituting row by row.
 __global__ void __launch_bounds__(NB * NB, 1) k_potrf_diag(double* A, int n, int k, int nb, int* info, double* linv) {
-  __shared__ double L[NB][NB + 1], X[NB][NB + 1];
+  // L: the block being reduced (column j is read, columns > j updated in step
+  // j); F: the factor, each entry written once -- so one barrier per column:
+  // every thread takes the pivot's square root itself, and nothing reads
+  // what step j writes until step j + 1
+  __shared__ double L[NB][NB + 1], F[NB][NB + 1], X[NB][NB + 1];
   const int c = threadIdx.x % NB, t = threadIdx.x / NB;
   L[t][c] = (t < nb && c <= t) ? A[(long long)(k + t) * n + k + c] : 0.0;
+  F[t][c] = 0.0;
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
+    const double d = L[j][j];
+    const bool bad = !(d > 0.0);
+    const double piv = bad ? 1.0 : sqrt(d);
+    const double rinv = 1.0 / piv;
     if (t == j && c == j) {
-      const double d = L[j][j];
-      if (!(d > 0.0)) {
-        if (*info == 0) *info = k + j + 1;
-        L[j][j] = 1.0;
-      } else {
-        L[j][j] = sqrt(d);
-      }
+      F[j][j] = piv;
+      if (bad && *info == 0) *info = k + j + 1;
+    }
+    if (t > j && t < nb) {
+      const double lt = L[t][j] * rinv;
+      if (c == j) F[t][j] = lt;
+      else if (c > j && c <= t) L[t][c] -= lt * (L[c][j] * rinv);
     }
     __syncthreads();
-    if (c == j && t > j && t < nb) L[t][j] /= L[j][j];
-    __syncthreads();
-    if (t > j && t < nb && c > j && c <= t) L[t][c] -= L[t][j] * L[c][j];
-    __syncthreads();
   }
-  // X = L^-1 by right-looking substitution: thread (t, c) keeps X[t][c] in a
+  // X = F^-1 by right-looking substitution: thread (t, c) keeps X[t][c] in a
   // register; step r finalises row r and every lower row subtracts its
-  // multiple of it -- one FMA and one barrier per step (a row-by-row dot
-  // product per step made each row a 32-long dependent chain)
+  // multiple of it -- one FMA and one barrier per step
   double xv = (t == c) ? 1.0 : 0.0;
   for (int r = 0; r < nb; ++r) {
     if (t == r) {
-      xv = xv / L[r][r];
+      xv = xv / F[r][r];
       X[r][c] = xv;
     }
     __syncthreads();
-    if (t > r && t < nb) xv = fma(-L[t][r], X[r][c], xv);
+    if (t > r && t < nb) xv = fma(-F[t][r], X[r][c], xv);
   }
-  if (t < nb && c <= t) A[(long long)(k + t) * n + k + c] = L[t][c];
+  if (t < nb && c <= t) A[(long long)(k + t) * n + k + c] = F[t][c];
   linv[t * NB + c] = (t < nb && c < nb) ? X[t][c] : 0.0;
 }
 
