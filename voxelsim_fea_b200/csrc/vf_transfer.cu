@@ -51,13 +51,22 @@ __global__ void __launch_bounds__(256) k_restrict_f(Grid f, const float* __restr
 #pragma unroll
     for (int dz = -1; dz <= 1; ++dz)
 #pragma unroll
-      for (int dy = -1; dy <= 1; ++dy)
+      for (int dy = -1; dy <= 1; ++dy) {
+        // the three fine nodes 2X-1 .. 2X+1 of this row are 9 consecutive
+        // values starting on an 8-byte boundary (storage x = 2X, rows a
+        // multiple of 4 nodes long): four float2 loads and one float
+        const long long q = 3 * (long long)f.idx(2 * X - 1, 2 * Y + dy, 2 * Z + dz);
+        const float2* q2 = reinterpret_cast<const float2*>(rf + q);
+        const float2 v01 = __ldg(q2), v23 = __ldg(q2 + 1), v45 = __ldg(q2 + 2), v67 = __ldg(q2 + 3);
+        const float v8 = __ldg(rf + q + 8);
+        const float r[9] = {v01.x, v01.y, v23.x, v23.y, v45.x, v45.y, v67.x, v67.y, v8};
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
           const float w = (dx ? 0.5f : 1.0f) * (dy ? 0.5f : 1.0f) * (dz ? 0.5f : 1.0f);
-          const long long q = 3 * (long long)f.idx(2 * X + dx, 2 * Y + dy, 2 * Z + dz);
-          a0 += w * rf[q]; a1 += w * rf[q + 1]; a2 += w * rf[q + 2];
+          const int o = 3 * (dx + 1);
+          a0 += w * r[o]; a1 += w * r[o + 1]; a2 += w * r[o + 2];
         }
+      }
     const int p = c.idx(X, Y, Z);
     const uint8_t m = cm[p];
     rc[3 * (long long)p] = (m & 1) ? a0 : 0.0f;
@@ -132,6 +141,12 @@ template <> struct Vec12<double> {
   __device__ __forceinline__ double& at(int i) { return reinterpret_cast<double*>(v)[i]; }
 };
 
+// Four consecutive storage nodes per thread (one 16-byte-aligned group of
+// u): their coarse parents lie in the three coarse columns 2 gx - 1 .. 2 gx + 1
+// of at most two coarse rows and planes, loaded once for the four nodes, and
+// only where a weight is non-zero (an even fine coordinate has one parent on
+// that axis).  The sums keep the order of the 8-corner loop over (kz, ky, kx)
+// with the zero-weight terms left out, which does not change them.
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong_add4(Grid c, const T* __restrict__ ec, Grid f,
                                                       const uint8_t* __restrict__ fm, T* __restrict__ uf,
@@ -150,14 +165,33 @@ __global__ void __launch_bounds__(256) k_prolong_add4(Grid c, const T* __restric
     Vec12<T> u;
     u.load(uf + 3LL * p0);
     const int y0 = y >> 1, z0 = z >> 1;
+    const int ny = (y & 1) ? 2 : 1, nz = (z & 1) ? 2 : 1;
     const T wy[2] = {(y & 1) ? (T)0.5 : (T)1, (y & 1) ? (T)0.5 : (T)0};
     const T wz[2] = {(z & 1) ? (T)0.5 : (T)1, (z & 1) ? (T)0.5 : (T)0};
+    // node j (logical x = 4 gx - 1 + j) uses coarse column ci = (x >> 1) - (2 gx - 1)
+    // and, for odd x, ci + 1: j = 0 -> {0, 1}, 1 -> {1}, 2 -> {1, 2}, 3 -> {2}
+    const bool a0 = (m4 & 0xffu) != 0, a1 = (m4 & 0xff00u) != 0, a2 = (m4 & 0xff0000u) != 0,
+               a3 = (m4 & 0xff000000u) != 0;
+    const bool need[3] = {a0, a0 || a1 || a2, a2 || a3};
+    T cv[2][2][3][3];
+#pragma unroll
+    for (int kz = 0; kz < 2; ++kz)
+#pragma unroll
+      for (int ky = 0; ky < 2; ++ky)
+#pragma unroll
+        for (int ci = 0; ci < 3; ++ci) {
+          const bool ld = kz < nz && ky < ny && need[ci];
+          const long long q = ld ? 3 * (long long)c.idx(2 * gx - 1 + ci, y0 + ky, z0 + kz) : 0;
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) cv[kz][ky][ci][cc] = ld ? __ldg(ec + q + cc) : (T)0;
+        }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const uint8_t m = (uint8_t)(m4 >> (8 * j));
-      const int x = 4 * gx + j - 1;                 // logical x (mask 0 outside [0, lx])
       if (!m) continue;
-      const int x0 = x >> 1;
+      const int x = 4 * gx + j - 1;
+      const int cb = (j + 1) >> 1;                   // coarse column of x >> 1: 0, 1, 1, 2
+      const int nx = (x & 1) ? 2 : 1;
       const T wx[2] = {(x & 1) ? (T)0.5 : (T)1, (x & 1) ? (T)0.5 : (T)0};
       T e0 = 0, e1 = 0, e2 = 0;
 #pragma unroll
@@ -166,9 +200,10 @@ __global__ void __launch_bounds__(256) k_prolong_add4(Grid c, const T* __restric
         for (int ky = 0; ky < 2; ++ky)
 #pragma unroll
           for (int kx = 0; kx < 2; ++kx) {
+            if (kz >= nz || ky >= ny || kx >= nx) continue;
             const T w = wx[kx] * wy[ky] * wz[kz];
-            const long long q = 3 * (long long)c.idx(x0 + kx, y0 + ky, z0 + kz);
-            e0 += w * __ldg(ec + q); e1 += w * __ldg(ec + q + 1); e2 += w * __ldg(ec + q + 2);
+            const T* v = cv[kz][ky][cb + kx];
+            e0 += w * v[0]; e1 += w * v[1]; e2 += w * v[2];
           }
       if (m & 1) u.at(3 * j) += e0;
       if (m & 2) u.at(3 * j + 1) += e1;
