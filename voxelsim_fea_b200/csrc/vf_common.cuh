@@ -256,7 +256,7 @@ template <typename T> void launch_jacobi_from_zero(const Grid& g, const T* b, co
 int dense_assemble(const Grid& c, const double* stencil, const uint8_t* cmask, double* A, int n, cudaStream_t st);
 int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStream_t st);
 size_t dense_work_count(int n);
-template <typename T> void launch_dense_solve(const Grid& c, const double* Ainv, int n, const T* b, T* x, const KrylovState* ks, cudaStream_t st);
+template <typename T, typename M> void launch_dense_solve(const Grid& c, const M* Ainv, int n, const T* b, T* x, const KrylovState* ks, cudaStream_t st);
 
 // vf_krylov.cu -- fused PCG vector kernels with deterministic FP64 reductions
 constexpr int kVecBlocks = 148 * 8;     // grid of the vector kernels (fixed => deterministic)

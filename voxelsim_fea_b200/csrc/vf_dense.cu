@@ -280,9 +280,11 @@ __global__ void __launch_bounds__(256) k_yty(const double* Y, double* Ainv, int 
     }
 }
 
-// x = Ainv b on the coarsest level; b gathered into shared memory in FP64.
-template <typename T>
-__global__ void k_dense_solve(Grid c, const double* __restrict__ Ainv, int n, const T* __restrict__ b,
+// x = Ainv b on the coarsest level; b gathered into shared memory in FP64,
+// products accumulated in FP64 (Ainv in FP64, or its FP32 copy for the FP32
+// V-cycle: half the bytes of the GEMV, which streams n^2 values per call).
+template <typename T, typename M>
+__global__ void k_dense_solve(Grid c, const M* __restrict__ Ainv, int n, const T* __restrict__ b,
                               T* __restrict__ x, const KrylovState* ks) {
   if (ks && ks->done) return;
   extern __shared__ double sb[];
@@ -296,16 +298,16 @@ __global__ void k_dense_solve(Grid c, const double* __restrict__ Ainv, int n, co
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
-    const double* row = Ainv + (long long)i * n;
+    const M* row = Ainv + (long long)i * n;
     // eight independent partial sums keep eight 256-byte row segments in
     // flight per warp (the GEMV streams n^2 doubles per call)
     double part[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int j = lane;
     for (; j + 7 * 32 < n; j += 8 * 32) {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) part[k] += __ldg(row + j + 32 * k) * sb[j + 32 * k];
+      for (int k = 0; k < 8; ++k) part[k] += (double)__ldg(row + j + 32 * k) * sb[j + 32 * k];
     }
-    for (; j < n; j += 32) part[7] += __ldg(row + j) * sb[j];
+    for (; j < n; j += 32) part[7] += (double)__ldg(row + j) * sb[j];
     double s = ((part[0] + part[1]) + (part[2] + part[3])) + ((part[4] + part[5]) + (part[6] + part[7]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -393,17 +395,22 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
 void dense_prepare_smem(int n) {
   (void)n;
   const int bytes = (int)sizeof(double) * 16384;
-  cudaFuncSetAttribute(k_dense_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_dense_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_dense_solve<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_dense_solve<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_dense_solve<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-template <typename T>
-void launch_dense_solve(const Grid& c, const double* Ainv, int n, const T* b, T* x, const KrylovState* ks,
+template <typename T, typename M>
+void launch_dense_solve(const Grid& c, const M* Ainv, int n, const T* b, T* x, const KrylovState* ks,
                         cudaStream_t st) {
   int blocks = (n + 7) / 8;   // one row per warp: every row's stream in flight at once
-  launch_k(k_dense_solve<T>, blocks, 256, sizeof(double) * n, st, c, Ainv, n, b, x, ks);
+  launch_k(k_dense_solve<T, M>, blocks, 256, sizeof(double) * n, st, c, Ainv, n, b, x, ks);
 }
-template void launch_dense_solve<double>(const Grid&, const double*, int, const double*, double*, const KrylovState*, cudaStream_t);
-template void launch_dense_solve<float>(const Grid&, const double*, int, const float*, float*, const KrylovState*, cudaStream_t);
+template void launch_dense_solve<double, double>(const Grid&, const double*, int, const double*, double*,
+                                                 const KrylovState*, cudaStream_t);
+template void launch_dense_solve<float, double>(const Grid&, const double*, int, const float*, float*,
+                                                const KrylovState*, cudaStream_t);
+template void launch_dense_solve<float, float>(const Grid&, const float*, int, const float*, float*,
+                                               const KrylovState*, cudaStream_t);
 
 }  // namespace vf

@@ -133,6 +133,7 @@ struct vf_solver {
   uint8_t* d_allfree = nullptr;
   // coarsest dense factor
   double* d_Ainv = nullptr;
+  float* d_Ainv32 = nullptr;    // FP32 copy of the coarsest inverse for the FP32 V-cycle
   double* d_dense_work = nullptr;
   int dense_n = 0;
   int* d_info = nullptr;
@@ -416,7 +417,12 @@ template <typename T>
 void coarse_solve(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
   Level& l = s->L[li];
   if (s->o.coarsest == VF_COARSEST_CHOLESKY && s->d_Ainv) {
-    launch_dense_solve<T>(l.g, s->d_Ainv, s->dense_n, b, x, ks, s->st);
+    if constexpr (sizeof(T) == 4) {
+      if (s->d_Ainv32) launch_dense_solve<T, float>(l.g, s->d_Ainv32, s->dense_n, b, x, ks, s->st);
+      else launch_dense_solve<T, double>(l.g, s->d_Ainv, s->dense_n, b, x, ks, s->st);
+    } else {
+      launch_dense_solve<T, double>(l.g, s->d_Ainv, s->dense_n, b, x, ks, s->st);
+    }
   } else {
     smooth<T>(s, li, x, Sel<T>::w(l, 1), b, s->o.coarse_sweeps, true, ks);
   }
@@ -796,6 +802,7 @@ int build_levels(vf_solver* s) {
     const int n = 3 * lc.g.nodes_ref();
     if (n <= 16384) {
       VF_ALLOC(s->d_Ainv, (size_t)n * n);
+      VF_ALLOC(s->d_Ainv32, (size_t)n * n);
       VF_ALLOC(s->d_dense_work, dense_work_count(n));
       s->dense_n = n;
       dense_prepare_smem(n);
@@ -1026,6 +1033,7 @@ int build_dense_coarsest(vf_solver* s) {
   }
   if (s->dense_n != n) {
     VF_ALLOC(s->d_Ainv, (size_t)n * n);
+    VF_ALLOC(s->d_Ainv32, (size_t)n * n);
     VF_ALLOC(s->d_dense_work, dense_work_count(n));
     s->dense_n = n;
     dense_prepare_smem(n);
@@ -1041,6 +1049,7 @@ int build_dense_coarsest(vf_solver* s) {
   if (lc.reach > 1) wide_dense_assemble(lc.g, lc.reach, st, lc.mask, s->d_Ainv, n, sd);
   else dense_assemble(lc.g, st, lc.mask, s->d_Ainv, n, sd);
   dense_cholesky_inverse(s->d_Ainv, s->d_dense_work, n, s->d_info, sd);
+  launch_convert<double, float>(s->d_Ainv, s->d_Ainv32, (long long)n * n, sd);
   VF_CHECK_LAUNCH();
   int info = 0;
   VF_TRY(cudaMemcpyAsync(&info, s->d_info, sizeof(int), cudaMemcpyDeviceToHost, sd));
@@ -2196,6 +2205,7 @@ void share_operator(vf_solver* c, const vf_solver* m) {
   c->d_spc = m->d_spc;
   c->d_one = m->d_one;
   c->d_Ainv = m->d_Ainv;
+  c->d_Ainv32 = m->d_Ainv32;
   c->dense_n = m->dense_n;
   c->d_omega = m->d_omega;
   c->d_lambda = m->d_lambda;
