@@ -439,16 +439,13 @@ template <typename S, typename A, typename L, int JJ>
 struct WideBlocks {
   // acc (this node's rows) += own block u = lane + G*JJ applied to the
   // neighbour p + off(s); for an upper block also the transposed upper block
-  // u of the node p - off(s) (lane and slot are the same there).  With the
-  // node's blocks split over SPLIT threads, thread `sub` takes the slots JJ
-  // of its share.
-  template <int SPLIT, typename VF>
-  __device__ __forceinline__ static void run(const S* __restrict__ stc, const Grid& g, int p, int lane, int sub, int x,
-                                             int y, int z, A (&acc)[3], VF V) {
+  // u of the node p - off(s) (lane and slot are the same there).
+  template <typename VF>
+  __device__ __forceinline__ static void run(const S* __restrict__ stc, const Grid& g, int p, int lane, int x, int y,
+                                             int z, A (&acc)[3], VF V) {
     constexpr int R = (L::W - 1) / 2, W = L::W, SC = L::NB / 2;
-    constexpr int PER = (L::NJ + SPLIT - 1) / SPLIT;
     const int u = lane + L::G * JJ;
-    if (u < L::NBLK && JJ / PER == sub) {
+    if (u < L::NBLK) {
       const int s = (u == L::NU) ? SC : SC + 1 + u;
       const int dx = s % W - R, dy = (s / W) % W - R, dz = s / (W * W) - R;
       const long long v = (long long)p * L::G + lane;
@@ -469,7 +466,7 @@ struct WideBlocks {
         for (int c = 0; c < 3; ++c) acc[c] += blk[c] * w0 + blk[3 + c] * w1 + blk[6 + c] * w2;
       }
     }
-    if constexpr (JJ + 1 < L::NJ) WideBlocks<S, A, L, JJ + 1>::template run<SPLIT>(stc, g, p, lane, sub, x, y, z, acc, V);
+    if constexpr (JJ + 1 < L::NJ) WideBlocks<S, A, L, JJ + 1>::run(stc, g, p, lane, x, y, z, acc, V);
   }
 };
 
@@ -478,15 +475,13 @@ struct WideBlocks {
 // zero).  G = 8 lanes per node: each lane applies its own blocks and the
 // transposed blocks of the same lane and slot of the lower neighbours, the
 // partial sums meet through warp shuffles, and lanes 0..2 write component
-// 0..2 of the node.  SPLIT = 2 (small levels, whose G threads per node
-// would leave most SMs idle): two threads per lane, each applying half of
-// the lane's blocks, reduced by one more shuffle step.
-template <typename T, typename S, int R, int EPI, int SPLIT>
+// 0..2 of the node.
+template <typename T, typename S, int R, int EPI>
 __global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __restrict__ stc,
                                                  const T* __restrict__ sqd) {
   using L = WideLayout<S, R>;
   using A = typename std::conditional<sizeof(T) == 8, double, float>::type;
-  constexpr int G = L::G, TG = G * SPLIT;   // threads per node
+  constexpr int G = L::G;
   KrylovState* ks = a.ks;
   if (ks && ks->done) return;
   const T* __restrict__ u = (const T*)a.u;
@@ -501,22 +496,22 @@ __global__ void __launch_bounds__(128) k_wide_op(Grid g, OpArgs a, const S* __re
   auto V = [&](int q, int c) -> A { return (A)__ldg(sqd + 3LL * q + c) * (A)__ldg(u + 3LL * q + c); };
   double dot = 0.0;
   // whole warps iterate together (the shuffles need every lane)
-  const long long nv = ((long long)g.n * TG + 31) / 32 * 32;
+  const long long nv = ((long long)g.n * G + 31) / 32 * 32;
   for (long long vv = blockIdx.x * (long long)blockDim.x + threadIdx.x; vv < nv;
        vv += (long long)gridDim.x * blockDim.x) {
-    const int p = (int)(vv / TG), lane = (int)(vv % G), sub = (int)((vv % TG) / G);
+    const int p = (int)(vv / G), lane = (int)(vv % G);
     int x = -1, y = -1, z = -1;
     if (p < g.n) decode(g, p, x, y, z);
     const bool in = p < g.n && inside(g, x, y, z);
     const uint8_t m = in ? mask[p] : (uint8_t)0;
     A acc[3] = {(A)0, (A)0, (A)0};
-    if (m) WideBlocks<S, A, L, 0>::template run<SPLIT>(stc, g, p, lane, sub, x, y, z, acc, V);
+    if (m) WideBlocks<S, A, L, 0>::run(stc, g, p, lane, x, y, z, acc, V);
 #pragma unroll
-    for (int o = 1; o < TG; o <<= 1) {
+    for (int o = 1; o < G; o <<= 1) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
     }
-    if (!in || sub != 0 || lane >= 3) continue;
+    if (!in || lane >= 3) continue;
     const int c = lane;
     const long long pc = 3LL * p + c;
     const A ac = c == 0 ? acc[0] : (c == 1 ? acc[1] : acc[2]);
@@ -618,30 +613,18 @@ template void launch_wide_compress<__half, 2>(const Grid&, const double*, const 
 template void launch_wide_compress<float, 2>(const Grid&, const double*, const uint8_t*, float*, float*, cudaStream_t);
 template void launch_wide_compress<double, 2>(const Grid&, const double*, const uint8_t*, double*, double*, cudaStream_t);
 
-// Levels whose 8 threads per node give fewer than 8 CTAs per SM take two
-// threads per lane.
-bool wide_split(const Grid& g) { return (long long)g.n * 8 < 148LL * 8 * 128; }
-
-template <typename T, typename S, int R, int SPLIT>
-void launch_wide_op_t(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
-  const int blocks = blocks_for((long long)g.n * 8 * SPLIT, 128, 148LL * 32);
-  if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY, SPLIT>, blocks, 128, 0, st, g, a, stc, sqrtd);
-  else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH, SPLIT>, blocks, 128, 0, st, g, a, stc, sqrtd);
-  else launch_k(k_wide_op<T, S, R, EPI_RESID, SPLIT>, blocks, 128, 0, st, g, a, stc, sqrtd);
-}
-
 template <typename T, typename S, int R>
 void launch_wide_op(const Grid& g, int epi, const OpArgs& a, const S* stc, const T* sqrtd, cudaStream_t st) {
-  if (wide_split(g)) launch_wide_op_t<T, S, R, 2>(g, epi, a, stc, sqrtd, st);
-  else launch_wide_op_t<T, S, R, 1>(g, epi, a, stc, sqrtd, st);
+  const int blocks = wide_op_grid_blocks(g);
+  if (epi == EPI_APPLY) launch_k(k_wide_op<T, S, R, EPI_APPLY>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else if (epi == EPI_SMOOTH) launch_k(k_wide_op<T, S, R, EPI_SMOOTH>, blocks, 128, 0, st, g, a, stc, sqrtd);
+  else launch_k(k_wide_op<T, S, R, EPI_RESID>, blocks, 128, 0, st, g, a, stc, sqrtd);
 }
 template void launch_wide_op<float, __half, 2>(const Grid&, int, const OpArgs&, const __half*, const float*, cudaStream_t);
 template void launch_wide_op<float, float, 2>(const Grid&, int, const OpArgs&, const float*, const float*, cudaStream_t);
 template void launch_wide_op<double, double, 2>(const Grid&, int, const OpArgs&, const double*, const double*,
                                                 cudaStream_t);
-int wide_op_grid_blocks(const Grid& g) {
-  return blocks_for((long long)g.n * 8 * (wide_split(g) ? 2 : 1), 128, 148LL * 32);
-}
+int wide_op_grid_blocks(const Grid& g) { return blocks_for((long long)g.n * 8, 128, 148LL * 32); }
 
 int wide_dense_assemble(const Grid& c, int R, const double* stencil, const uint8_t* cmask, double* A, int n,
                         cudaStream_t st) {
