@@ -217,6 +217,13 @@ def test_dense_coarsest_is_exact_inverse(gpu, dims):
     free[fixed] = False
     r = f * free - hex8.element_apply(u, E, hex8.build_edof(nx, ny, nz), hex8.hex8_ke(1.0, 0.3), ndof) * free
     assert np.linalg.norm(r) < 1e-10 * np.linalg.norm(f)
+    # the FP32 V-cycle applies an FP32 copy of the same inverse (FP64 sums):
+    # still a near-exact preconditioner for the FP64 outer iteration
+    m32 = MGSolver(nx, ny, nz, fixed, nu=0.3, max_levels=1, options=SolverOptions.fast())
+    u32 = m32.solve(E, f, tol=1e-10)
+    assert m32.last_converged and m32.last_iters <= 12, m32.last_iters
+    r32 = f * free - hex8.element_apply(u32, E, hex8.build_edof(nx, ny, nz), hex8.hex8_ke(1.0, 0.3), ndof) * free
+    assert np.linalg.norm(r32) < 1e-10 * np.linalg.norm(f)
 
 
 def test_solve_into_out_buffer(gpu):
