@@ -115,6 +115,12 @@ def field_errors(u, vm, u_ref, vm_ref, node_act, elem_act, apply_k=None):
     return out
 
 
+def level_sweeps_kw(args):
+    """Solver option override for --smoothed-level-sweeps (none: the presets')."""
+    v = getattr(args, "smoothed_level_sweeps", None)
+    return {} if v is None else {"smoothed_level_sweeps": int(v)}
+
+
 # DRAM traffic of the roofline kernel comes from an ncu capture summary under
 # profiles/, which records the bytes per launch and a hash of the kernel's
 # sources; the figure is reported only while the sources still hash the same.
@@ -405,7 +411,7 @@ def other_configs(args, local):
     from voxelsim_fea_b200 import generators
     from voxelsim_fea_b200.multigrid import MGSolver, SolverOptions, solve_batch
     opts = dict(device=local, check_every=args.check_every, smoother=args.smoother,
-                smoothed_transfers=args.smoothed_transfers)
+                smoothed_transfers=args.smoothed_transfers, **level_sweeps_kw(args))
     out = {}
 
     def timed_call(fn):
@@ -513,7 +519,7 @@ def run_b200(args):
                         n_smooth=args.n_smooth)
 
     fkw = dict(device=local, check_every=args.check_every, modal_zchunk=args.modal_zchunk, mixed_mode=args.mixed_mode,
-               smoother=args.smoother, smoothed_transfers=args.smoothed_transfers)
+               smoother=args.smoother, smoothed_transfers=args.smoothed_transfers, **level_sweeps_kw(args))
     if args.inner_tol is not None:
         fkw["inner_tol"] = args.inner_tol
     fast = solver(SolverOptions.fast(**fkw))
@@ -647,7 +653,7 @@ def run_b200(args):
     u_plain = None
     if not args.no_plain or (K == 1 and not args.no_errors):
         ps = solver(SolverOptions.robust(device=local, check_every=args.check_every, smoother=args.smoother,
-                                         smoothed_transfers=args.smoothed_transfers))
+                                         smoothed_transfers=args.smoothed_transfers, **level_sweeps_kw(args)))
         L.vf_get_stream(ps._h, ctypes.byref(stream_ptr))
         ext_plain = torch.cuda.ExternalStream(stream_ptr.value)
         ext_save = ext
@@ -845,6 +851,8 @@ def main():
                     help="V-cycle smoothing of every arm (plain FP64, mixed, learned)")
     ap.add_argument("--smoothed-transfers", type=int, default=2,
                     help="bitmask of transfers l -> l+1 with the smoothed prolongation (2: level 1 -> 2)")
+    ap.add_argument("--smoothed-level-sweeps", type=int, default=None,
+                    help="sweeps on the level above a smoothed transfer (default: the presets' choice)")
     ap.add_argument("--inner-tol", type=float, default=None,
                     help="mixed: residual reduction between FP64 corrections (solver default if unset)")
     args = ap.parse_args()

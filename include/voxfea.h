@@ -134,7 +134,9 @@ typedef struct vf_options {
                               solve continues as plain PCG from its current iterate, within the
                               same iteration budget (vf_solve_info.outer_iters = the iteration of
                               the switch); 0 = never (default 64) */
-  int32_t reserved[1];
+  int32_t smoothed_level_sweeps; /* sweeps before and after the coarse correction on a level whose
+                              transfer to the next level is smoothed (its smoothed restriction and
+                              prolongation already smooth it once each); 0 = n_smooth (default) */
 } vf_options;
 
 enum { VF_OMEGA_FIXED = 0, VF_OMEGA_AUTO = 1 };

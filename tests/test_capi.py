@@ -73,7 +73,8 @@ def test_create_rejects_bad_args(lib):
         setattr(o, field, bad)
         assert lib.vf_create(4, 4, 4, 0.3, ctypes.byref(o), ctypes.byref(h)) == _lib.VF_ERR_ARG, field
     # Chebyshev smoothing needs the lambda estimates, at most 2 sweeps and kernels that take its step
-    for fields in ({}, {"omega_mode": 1, "n_smooth": 3}, {"omega_mode": 1, "fine_kernel": 1},
+    for fields in ({}, {"omega_mode": 1, "n_smooth": 3}, {"omega_mode": 1, "smoothed_level_sweeps": 3},
+                   {"omega_mode": 1, "fine_kernel": 1},
                    {"omega_mode": 1, "coarse_storage": 2}, {"omega_mode": 1, "cheb_ratio": 1}):
         o = _lib.default_options()
         o.smoother = _lib.SMOOTHERS["chebyshev"]

@@ -95,3 +95,21 @@ def test_smoothed_solve(gpu, fast):
     assert c0 and c1 and r1 < 1e-8
     assert it1 < it0, (it1, it0)
     assert np.abs(u1 - u0).max() <= 1e-5 * np.abs(u0).max()
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_smoothed_level_sweeps(gpu, fast):
+    """One sweep before and after the coarse correction on level 1, whose
+    smoothed restriction and prolongation smooth it once each already: the
+    same displacement in about as many iterations as two sweeps."""
+    part = _part(shape=(48, 48, 48), seed=9_015_838)
+    res = {}
+    for sw in (0, 1):
+        m = _solver(part, True, fast=fast, smoothed_level_sweeps=sw)
+        u = m.solve(part["E"], part["f"], tol=1e-8, nu_elem=part["nu"], max_cg=3000)
+        res[sw] = (u, m.last_iters, m.last_converged, m.last_info.true_resid)
+        m.close()
+    (u0, it0, c0, _), (u1, it1, c1, r1) = res[0], res[1]
+    assert c0 and c1 and r1 < 1e-8
+    assert it1 <= int(1.15 * it0) + 3, (it1, it0)
+    assert np.abs(u1 - u0).max() <= 1e-5 * np.abs(u0).max()

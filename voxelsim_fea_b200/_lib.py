@@ -74,7 +74,7 @@ class VfOptions(ctypes.Structure):
         ("flexible", ctypes.c_int32), ("autotune", ctypes.c_int32),
         ("smoother", ctypes.c_int32), ("cheb_ratio", ctypes.c_int32),
         ("smoothed_transfers", ctypes.c_int32), ("learned_watch", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("smoothed_level_sweeps", ctypes.c_int32),
     ]
 
 

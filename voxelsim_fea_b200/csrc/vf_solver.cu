@@ -440,16 +440,19 @@ void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks, int dot_slo
   Level& c = s->L[li + 1];
   T* tmp = Sel<T>::w(l, 1);
   T* res = Sel<T>::w(l, 2);
-  const bool cheb = s->o.smoother == VF_SMOOTH_CHEBYSHEV && s->o.n_smooth > 0;
-  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, s->o.n_smooth, true, ks, -1);
-  else smooth<T>(s, li, x, tmp, b, s->o.n_smooth, true, ks);
+  // a level whose transfer down is smoothed gets one more smoothing step from
+  // each of its smoothed restriction and prolongation
+  const int sweeps = (l.smooth_down && s->o.smoothed_level_sweeps > 0) ? s->o.smoothed_level_sweeps : s->o.n_smooth;
+  const bool cheb = s->o.smoother == VF_SMOOTH_CHEBYSHEV && sweeps > 0;
+  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, sweeps, true, ks, -1);
+  else smooth<T>(s, li, x, tmp, b, sweeps, true, ks);
   level_op<T>(s, li, EPI_RESID, x, res, b, ks, nullptr, 0);
   restrict_level<T>(s, li, res, Sel<T>::w(c, 3), ks);
   vcycle<T>(s, li + 1, Sel<T>::w(c, 3), Sel<T>::w(c, 0), ks);
   prolong_level<T>(s, li, Sel<T>::w(c, 0), x, ks);
   // (res is free again: the post-smoothing's first update goes there)
-  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, s->o.n_smooth, false, ks, dot_slot);
-  else smooth<T>(s, li, x, tmp, b, s->o.n_smooth, false, ks, dot_slot);
+  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, sweeps, false, ks, dot_slot);
+  else smooth<T>(s, li, x, tmp, b, sweeps, false, ks, dot_slot);
 }
 
 template <typename T> T** kvec(vf_solver* s);
@@ -1191,14 +1194,14 @@ int vf_create(int32_t nx, int32_t ny, int32_t nz, double nu, const vf_options* o
       o.omega_mode < 0 || o.omega_mode > 1 || !(o.omega_rel > 0.0 && o.omega_rel < 1.0) || o.power_iters < 0 ||
       o.fine_kernel < 0 || o.fine_kernel > 2 || o.modal_zchunk < -1 || o.coarse_storage < 0 ||
       o.coarse_storage > 2 || o.mixed_mode < 0 || o.mixed_mode > 2 || o.smoother < 0 || o.smoother > 1 ||
-      o.learned_watch < 0) {
+      o.learned_watch < 0 || o.smoothed_level_sweeps < 0) {
     g_last_error = "invalid vf_options field";
     return VF_ERR_ARG;
   }
   if (o.smoother == VF_SMOOTH_CHEBYSHEV &&
-      (o.omega_mode != VF_OMEGA_AUTO || o.n_smooth > 2 || o.cheb_ratio < 2 || o.fine_kernel == VF_FINE_GATHER ||
+      (o.omega_mode != VF_OMEGA_AUTO || o.n_smooth > 2 || o.smoothed_level_sweeps > 2 || o.cheb_ratio < 2 || o.fine_kernel == VF_FINE_GATHER ||
        o.coarse_storage == VF_STENCIL_FULL)) {
-    g_last_error = "Chebyshev smoothing needs omega_mode AUTO, n_smooth <= 2, cheb_ratio >= 2, a modal fine kernel "
+    g_last_error = "Chebyshev smoothing needs omega_mode AUTO, n_smooth and smoothed_level_sweeps <= 2, cheb_ratio >= 2, a modal fine kernel "
                    "and symmetric coarse storage";
     return VF_ERR_ARG;
   }

@@ -81,6 +81,7 @@ class SolverOptions:
     # bit l: the transfer from Galerkin level l to l+1 uses the smoothed
     # prolongation (I - (4/3) D^-1 A_l / lambda_l) P; bit 1 (level 1 -> 2) only
     smoothed_transfers: int = 0
+    smoothed_level_sweeps: int = 0   # sweeps on a level whose transfer down is smoothed (0: n_smooth)
     learned_watch: int = 64          # learned stage: iterations without halving the residual before
                                      # the stage is switched off and plain PCG takes over (0: never)
 
@@ -188,6 +189,7 @@ class MGSolver:
         o.cheb_ratio = int(self.options.cheb_ratio)
         o.smoothed_transfers = int(self.options.smoothed_transfers)
         o.learned_watch = int(self.options.learned_watch)
+        o.smoothed_level_sweeps = int(self.options.smoothed_level_sweeps)
         h = ctypes.c_void_p()
         _lib.check(L.vf_create(int(nx), int(ny), int(nz), float(nu), ctypes.byref(o), ctypes.byref(h)),
                    None, "vf_create")
