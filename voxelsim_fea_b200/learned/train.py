@@ -294,6 +294,8 @@ def main():
     ap.add_argument("--raw-parts", action="store_true",
                     help="evaluate the generated parts as they are, without the reference's island step")
     ap.add_argument("--configs", choices=("headline", "modes", "learned"), default="headline")
+    ap.add_argument("--smoothed-level-sweeps", type=int, default=None,
+                    help="smoothed_level_sweeps of every configuration (default: the presets')")
     ap.add_argument("--learned-watch", type=int, default=None,
                     help="learned_watch of the configurations with the stage on (default: the option's default)")
     ap.add_argument("--weights", type=str, default=None, help="weights to evaluate (default: the packaged ones)")
@@ -309,6 +311,9 @@ def main():
             for _, opts, use in cfgs:
                 if use:
                     opts.learned_watch = int(args.learned_watch)
+        if args.smoothed_level_sweeps is not None:
+            for _, opts, _ in cfgs:
+                opts.smoothed_level_sweeps = int(args.smoothed_level_sweeps)
         rows = evaluate(params, level, seeds, (e, e, e), configs=cfgs, max_cg=args.max_cg,
                         drop_islands=not args.raw_parts)
         _report(rows, cfgs, args)
