@@ -117,3 +117,7 @@ def test_presets_pick_a_supported_smoother():
     assert SolverOptions.fast(coarse_storage="full").smoother == "jacobi"
     assert SolverOptions.robust(omega_mode="fixed").smoother == "jacobi"
     assert SolverOptions.robust(smoother="jacobi").smoother == "jacobi"
+    # one smoothing step on level 1 above the smoothed level 1 -> 2 transfer
+    assert SolverOptions.robust().smoothed_level_sweeps == 1 and SolverOptions.fast().smoothed_level_sweeps == 1
+    assert SolverOptions.fast(smoothed_transfers=0).smoothed_level_sweeps == 0
+    assert SolverOptions().smoothed_level_sweeps == 0

@@ -40,6 +40,16 @@ def _preset_smoother(kw):
     return "chebyshev"
 
 
+def _preset_level_sweeps(kw):
+    """With the level 1 -> 2 transfer smoothed, level 1 is smoothed once more by
+    its smoothed restriction and prolongation: the presets give it one
+    Chebyshev step before and after the coarse correction instead of two
+    (bracket 256x128x128: 158 -> 162 iterations, 3.8 % less time to
+    solution; held-out 192^3 two-material parts: 532 -> 560 iterations, 3 %
+    less time)."""
+    return 1 if _preset_transfers(kw) and kw.get("smoothed_transfers", 2) else 0
+
+
 def _preset_transfers(kw):
     """The presets smooth the level 1 -> 2 prolongation (the 125-block coarse
     space) wherever the options allow it (Galerkin levels, auto damping,
@@ -99,7 +109,8 @@ class SolverOptions:
         the CG residual norm of a converging solve on high-contrast geometry is
         not monotone."""
         base = dict(coarse="galerkin", coarsest="cholesky", omega_mode="auto", stall_guard=False,
-                    smoother=_preset_smoother(kw), smoothed_transfers=_preset_transfers(kw))
+                    smoother=_preset_smoother(kw), smoothed_transfers=_preset_transfers(kw),
+                    smoothed_level_sweeps=_preset_level_sweeps(kw))
         base.update(kw)
         return cls(**base)
 
@@ -108,7 +119,8 @@ class SolverOptions:
         """Galerkin hierarchy, mixed precision: by default FP64 PCG preconditioned by
         the FP32 V-cycle (``mixed_mode="outer64"``)."""
         base = dict(coarse="galerkin", coarsest="cholesky", precision="mixed", omega_mode="auto",
-                    stall_guard=False, smoother=_preset_smoother(kw), smoothed_transfers=_preset_transfers(kw))
+                    stall_guard=False, smoother=_preset_smoother(kw), smoothed_transfers=_preset_transfers(kw),
+                    smoothed_level_sweeps=_preset_level_sweeps(kw))
         base.update(kw)
         return cls(**base)
 
