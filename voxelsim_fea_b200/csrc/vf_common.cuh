@@ -254,9 +254,13 @@ template <typename T> void launch_jacobi_from_zero(const Grid& g, const T* b, co
 
 // vf_dense.cu -- coarsest-level dense FP64 direct solve
 int dense_assemble(const Grid& c, const double* stencil, const uint8_t* cmask, double* A, int n, cudaStream_t st);
-int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStream_t st);
+int dense_cholesky_inverse(double* A, double* work, int n, int bw, int* d_info, cudaStream_t st);
 size_t dense_work_count(int n);
-template <typename T, typename M> void launch_dense_solve(const Grid& c, const M* Ainv, int n, const T* b, T* x, const KrylovState* ks, cudaStream_t st);
+int dense_ld32(int n);   // row stride (floats) of the padded FP32 inverse
+void launch_dense_perm(const Grid& c, int* perm, int n, cudaStream_t st);
+void launch_dense_convert_pad(const double* A, float* B, int n, cudaStream_t st);
+template <typename T> void launch_dense_solve(const double* Ainv, int n, const int* perm, const T* b, T* x, const KrylovState* ks, cudaStream_t st);
+void launch_dense_solve_f32(const float* Ainv32, int n, const int* perm, const float* b, float* x, const KrylovState* ks, cudaStream_t st);
 
 // vf_krylov.cu -- fused PCG vector kernels with deterministic FP64 reductions
 constexpr int kVecBlocks = 148 * 8;     // grid of the vector kernels (fixed => deterministic)

@@ -169,6 +169,9 @@ struct GemmBatch {
   int count;
   double alpha;
   int a_lower, b_lower;   // A / B lower triangular (square): skip the zero part of the K range
+  // a_bw > 0: A is a block L21 of a band matrix, its row 0 K rows below its
+  // column 0, so A[i][k] = 0 for k < i + K - a_bw
+  int a_bw;
 };
 
 // One 64 x 64 output tile per CTA (blockIdx.x: tile of job blockIdx.y),
@@ -181,6 +184,7 @@ __global__ void __launch_bounds__(256) k_gemm_batched(const __grid_constant__ Ge
   int kb = 0, ke = jb.K;
   if (bt.b_lower) kb = j0;                        // B[k][j] = 0 for k < j
   if (bt.a_lower) ke = min(ke, i0 + TB);          // A[i][k] = 0 for k > i
+  if (bt.a_bw > 0) kb = max(kb, i0 + jb.K - bt.a_bw);
   constexpr int LC = 32;
   __shared__ double As[TB][LC + 1], Bs[LC][TB + 1];
   const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
@@ -280,42 +284,97 @@ __global__ void __launch_bounds__(256) k_yty(const double* Y, double* Ainv, int 
     }
 }
 
+// Padded-storage vector index of each coarsest DOF (reference node order,
+// DOF 3 * node + c): the GEMVs gather b and scatter x through it instead of
+// decoding node coordinates in every CTA.
+__global__ void k_dense_perm(Grid c, int* __restrict__ perm, int n) {
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int r = i / 3, comp = i - 3 * r;
+    const int xx = r % nx1, rr = r / nx1, yy = rr % ny1, zz = rr / ny1;
+    perm[i] = 3 * c.idx(xx, yy, zz) + comp;
+  }
+}
+
+// FP32 copy of the FP64 inverse with rows padded to ld (a multiple of 4)
+// floats, the padding zero: every row starts on a 16-byte boundary.
+__global__ void k_convert_pad(const double* __restrict__ A, float* __restrict__ B, int n, int ld) {
+  const long long total = (long long)n * ld;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / ld), j = (int)(e - (long long)i * ld);
+    B[e] = j < n ? (float)A[(long long)i * n + j] : 0.0f;
+  }
+}
+
 // x = Ainv b on the coarsest level; b gathered into shared memory in FP64,
-// products accumulated in FP64 (Ainv in FP64, or its FP32 copy for the FP32
-// V-cycle: half the bytes of the GEMV, which streams n^2 values per call).
-template <typename T, typename M>
-__global__ void k_dense_solve(Grid c, const M* __restrict__ Ainv, int n, const T* __restrict__ b,
-                              T* __restrict__ x, const KrylovState* ks) {
+// products accumulated in FP64 (Ainv in FP64; the FP32 V-cycle reads the
+// padded FP32 copy in k_dense_solve_f32).
+template <typename T>
+__global__ void k_dense_solve(const double* __restrict__ Ainv, int n, const int* __restrict__ perm,
+                              const T* __restrict__ b, T* __restrict__ x, const KrylovState* ks) {
   if (ks && ks->done) return;
   extern __shared__ double sb[];
-  const int nx1 = c.lx + 1, ny1 = c.ly + 1;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const int r = i / 3, comp = i % 3;
-    const int xx = r % nx1, rr = r / nx1, yy = rr % ny1, zz = rr / ny1;
-    sb[i] = (double)b[3 * (long long)c.idx(xx, yy, zz) + comp];
-  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sb[i] = (double)b[__ldg(perm + i)];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
-    const M* row = Ainv + (long long)i * n;
+    const double* row = Ainv + (long long)i * n;
     // eight independent partial sums keep eight 256-byte row segments in
     // flight per warp (the GEMV streams n^2 doubles per call)
     double part[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int j = lane;
     for (; j + 7 * 32 < n; j += 8 * 32) {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) part[k] += (double)__ldg(row + j + 32 * k) * sb[j + 32 * k];
+      for (int k = 0; k < 8; ++k) part[k] += __ldg(row + j + 32 * k) * sb[j + 32 * k];
     }
-    for (; j < n; j += 32) part[7] += (double)__ldg(row + j) * sb[j];
+    for (; j < n; j += 32) part[7] += __ldg(row + j) * sb[j];
     double s = ((part[0] + part[1]) + (part[2] + part[3])) + ((part[4] + part[5]) + (part[6] + part[7]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-      const int r = i / 3, comp = i % 3;
-      const int xx = r % nx1, rr = r / nx1, yy = rr % ny1, zz = rr / ny1;
-      x[3 * (long long)c.idx(xx, yy, zz) + comp] = (T)s;
+    if (lane == 0) x[__ldg(perm + i)] = (T)s;
+  }
+}
+
+// The FP32 V-cycle's coarsest GEMV: rows of ld floats (16-byte aligned,
+// zero-padded past n), each lane streaming float4s, eight in flight per lane
+// (4 KB per warp: enough bytes in flight to approach the HBM rate with one
+// row per warp), products accumulated in FP64.
+template <typename T>
+__global__ void k_dense_solve_f32(const float* __restrict__ Ainv, int n, int ld, const int* __restrict__ perm,
+                                  const T* __restrict__ b, T* __restrict__ x, const KrylovState* ks) {
+  if (ks && ks->done) return;
+  extern __shared__ double sb[];   // ld values, zero past n
+  for (int i = threadIdx.x; i < ld; i += blockDim.x) sb[i] = i < n ? (double)b[__ldg(perm + i)] : 0.0;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const int n4 = ld >> 2;
+  for (int i = blockIdx.x * wpb + warp; i < n; i += gridDim.x * wpb) {
+    const float4* row = reinterpret_cast<const float4*>(Ainv + (long long)i * ld);
+    double part[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int j = lane;
+    for (; j + 7 * 32 < n4; j += 8 * 32) {
+      float4 v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = __ldg(row + j + 32 * k);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const double* bb = sb + 4 * (j + 32 * k);
+        part[k] += (double)v[k].x * bb[0] + (double)v[k].y * bb[1] + (double)v[k].z * bb[2] +
+                   (double)v[k].w * bb[3];
+      }
     }
+    for (; j < n4; j += 32) {
+      const float4 v = __ldg(row + j);
+      const double* bb = sb + 4 * j;
+      part[7] += (double)v.x * bb[0] + (double)v.y * bb[1] + (double)v.z * bb[2] + (double)v.w * bb[3];
+    }
+    double s = ((part[0] + part[1]) + (part[2] + part[3])) + ((part[4] + part[5]) + (part[6] + part[7]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[__ldg(perm + i)] = (T)s;
   }
 }
 
@@ -337,15 +396,21 @@ size_t dense_work_count(int n) {
 
 // A (n x n, lower part) is overwritten by L; work (dense_work_count(n))
 // receives Y = L^-1 and the inverted diagonal blocks; A <- Y^T Y = A^-1.
-// d_info > 0 flags a non-positive pivot.
-int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStream_t st) {
+// d_info > 0 flags a non-positive pivot.  bw: A[i][j] == 0 for |i - j| > bw
+// (a stencil operator in lexicographic node order is banded).  A Cholesky
+// factor keeps the band, so the panel solve and the trailing update of block
+// column k only touch the rows below it that lie within the band: the rows
+// they skip would receive exact zeros (the factor is the same bit for bit).
+int dense_cholesky_inverse(double* A, double* work, int n, int bw, int* d_info, cudaStream_t st) {
   cudaMemsetAsync(d_info, 0, sizeof(int), st);
   double* linv_all = work + (size_t)n * n;
+  if (bw < 0 || bw > n) bw = n;
   for (int k = 0; k < n; k += NB) {
     const int nb = (n - k < NB) ? (n - k) : NB;
     double* linv = linv_all + (size_t)(k / NB) * NB * NB;
     launch_k(k_potrf_diag, 1, NB * NB, 0, st, A, n, k, nb, d_info, linv);
-    const int rest = n - k - nb;
+    // rows > k + nb - 1 + bw of columns k .. k + nb - 1 are zero
+    const int rest = std::min(n, k + nb + bw) - (k + nb);
     if (rest > 0) {
       launch_k(k_trsm_panel, (rest + 63) / 64, 256, 0, st, A, n, k, nb, (const double*)linv);
       const int tiles = (rest + TB - 1) / TB;
@@ -360,6 +425,7 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
   for (int g = 1; g < nbk; g *= 2) {
     GemmBatch b1{}, b2{};
     b1.alpha = 1.0; b1.b_lower = 1;     // T = L21 Y11
+    b1.a_bw = bw;
     b2.alpha = -1.0; b2.a_lower = 1;    // Y21 = -Y22 T
     int max_tiles = 0;
     size_t toff = 0;
@@ -376,8 +442,11 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
       const int m = r2 - r1, h = r1 - r0;
       double* T = tbuf + toff;   // distinct per pair within a level (sum of m h <= n^2 / 4)
       toff += (size_t)m * h;
-      b1.job[b1.count++] = GemmJob{A + (size_t)r1 * n + r0, work + (size_t)r0 * n + r0, T, n, n, h, m, h, h};
-      b2.job[b2.count++] = GemmJob{work + (size_t)r1 * n + r1, T, work + (size_t)r1 * n + r0, n, h, n, m, h, m};
+      // L21 = L[r1:r2, r0:r1] is zero below its row bw (the band), and so
+      // is T: only its first mb rows are formed, and only they enter Y21
+      const int mb = std::min(m, bw);
+      b1.job[b1.count++] = GemmJob{A + (size_t)r1 * n + r0, work + (size_t)r0 * n + r0, T, n, n, h, mb, h, h};
+      b2.job[b2.count++] = GemmJob{work + (size_t)r1 * n + r1, T, work + (size_t)r1 * n + r0, n, h, n, m, h, mb};
       max_tiles = std::max(max_tiles, ((m + TB - 1) / TB) * ((h + TB - 1) / TB));
       if (b1.count == kMaxJobs) flush();
     }
@@ -395,22 +464,39 @@ int dense_cholesky_inverse(double* A, double* work, int n, int* d_info, cudaStre
 void dense_prepare_smem(int n) {
   (void)n;
   const int bytes = (int)sizeof(double) * 16384;
-  cudaFuncSetAttribute(k_dense_solve<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_dense_solve<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_dense_solve<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_dense_solve<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_dense_solve<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_dense_solve_f32<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-template <typename T, typename M>
-void launch_dense_solve(const Grid& c, const M* Ainv, int n, const T* b, T* x, const KrylovState* ks,
-                        cudaStream_t st) {
-  int blocks = (n + 7) / 8;   // one row per warp: every row's stream in flight at once
-  launch_k(k_dense_solve<T, M>, blocks, 256, sizeof(double) * n, st, c, Ainv, n, b, x, ks);
+int dense_ld32(int n) { return (n + 3) / 4 * 4; }
+
+void launch_dense_perm(const Grid& c, int* perm, int n, cudaStream_t st) {
+  launch_k(k_dense_perm, (n + 255) / 256, 256, 0, st, c, perm, n);
 }
-template void launch_dense_solve<double, double>(const Grid&, const double*, int, const double*, double*,
-                                                 const KrylovState*, cudaStream_t);
-template void launch_dense_solve<float, double>(const Grid&, const double*, int, const float*, float*,
-                                                const KrylovState*, cudaStream_t);
-template void launch_dense_solve<float, float>(const Grid&, const float*, int, const float*, float*,
-                                               const KrylovState*, cudaStream_t);
+
+void launch_dense_convert_pad(const double* A, float* B, int n, cudaStream_t st) {
+  const int ld = dense_ld32(n);
+  const long long total = (long long)n * ld;
+  launch_k(k_convert_pad, (int)std::min<long long>((total + 255) / 256, 148LL * 32), 256, 0, st, A, B, n, ld);
+}
+
+template <typename T>
+void launch_dense_solve(const double* Ainv, int n, const int* perm, const T* b, T* x, const KrylovState* ks,
+                        cudaStream_t st) {
+  const int blocks = (n + 7) / 8;   // one row per warp: every row's stream in flight at once
+  launch_k(k_dense_solve<T>, blocks, 256, sizeof(double) * n, st, Ainv, n, perm, b, x, ks);
+}
+template void launch_dense_solve<double>(const double*, int, const int*, const double*, double*,
+                                         const KrylovState*, cudaStream_t);
+template void launch_dense_solve<float>(const double*, int, const int*, const float*, float*,
+                                        const KrylovState*, cudaStream_t);
+
+void launch_dense_solve_f32(const float* Ainv32, int n, const int* perm, const float* b, float* x,
+                            const KrylovState* ks, cudaStream_t st) {
+  const int ld = dense_ld32(n);
+  const int blocks = (n + 7) / 8;
+  launch_k(k_dense_solve_f32<float>, blocks, 256, sizeof(double) * ld, st, Ainv32, n, ld, perm, b, x, ks);
+}
 
 }  // namespace vf

@@ -83,6 +83,10 @@ struct Level {
   // (reach 2: WideLayout, 568 values per node)
   double* sym64 = nullptr; double* sq64 = nullptr;
   float* sym32 = nullptr; __half* sym16 = nullptr; float* sq32 = nullptr;
+  // sym64 / sq64 hold the current stencil: built at set-up for an FP64
+  // solver, on the first FP64 use otherwise (a mixed or FP32 solve never
+  // applies an FP64 coarse operator)
+  bool sym64_ok = false;
   int reach = 1;             // Galerkin stencil reach: 1 (27 blocks) or 2 (125 blocks, vf_wide.cu)
   bool smooth_down = false;  // the transfer to the next level uses the smoothed prolongation
   // x, tmp, resid, rhs, and a second temporary for the smoothed restriction
@@ -133,7 +137,8 @@ struct vf_solver {
   uint8_t* d_allfree = nullptr;
   // coarsest dense factor
   double* d_Ainv = nullptr;
-  float* d_Ainv32 = nullptr;    // FP32 copy of the coarsest inverse for the FP32 V-cycle
+  float* d_Ainv32 = nullptr;    // FP32 copy of the coarsest inverse for the FP32 V-cycle (rows of dense_ld32(n))
+  int* d_dense_perm = nullptr;  // padded-vector index of each coarsest DOF
   double* d_dense_work = nullptr;
   int dense_n = 0;
   int* d_info = nullptr;
@@ -244,7 +249,13 @@ int nlev(const vf_solver* s) { return use_mg(s) ? (int)s->L.size() : 1; }
 // operator dispatch on one level
 // ---------------------------------------------------------------------------
 template <typename T> void level_sym_op(vf_solver* s, Level& l, int epi, const OpArgs& a);
+void compress_sym64(vf_solver* s, Level& l) {
+  if (l.reach == 2) launch_wide_compress<double, 2>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+  else launch_stencil_compress<double>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+  l.sym64_ok = true;
+}
 template <> void level_sym_op<double>(vf_solver* s, Level& l, int epi, const OpArgs& a) {
+  if (!l.sym64_ok) compress_sym64(s, l);
   if (l.reach == 2) launch_wide_op<double, double, 2>(l.g, epi, a, l.sym64, l.sq64, s->st);
   else launch_stencil_sym_op<double, double>(l.g, epi, a, l.sym64, l.sq64, l.szchunk, s->st);
 }
@@ -418,10 +429,10 @@ void coarse_solve(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
   Level& l = s->L[li];
   if (s->o.coarsest == VF_COARSEST_CHOLESKY && s->d_Ainv) {
     if constexpr (sizeof(T) == 4) {
-      if (s->d_Ainv32) launch_dense_solve<T, float>(l.g, s->d_Ainv32, s->dense_n, b, x, ks, s->st);
-      else launch_dense_solve<T, double>(l.g, s->d_Ainv, s->dense_n, b, x, ks, s->st);
+      if (s->d_Ainv32) launch_dense_solve_f32(s->d_Ainv32, s->dense_n, s->d_dense_perm, b, x, ks, s->st);
+      else launch_dense_solve<T>(s->d_Ainv, s->dense_n, s->d_dense_perm, b, x, ks, s->st);
     } else {
-      launch_dense_solve<T, double>(l.g, s->d_Ainv, s->dense_n, b, x, ks, s->st);
+      launch_dense_solve<T>(s->d_Ainv, s->dense_n, s->d_dense_perm, b, x, ks, s->st);
     }
   } else {
     smooth<T>(s, li, x, Sel<T>::w(l, 1), b, s->o.coarse_sweeps, true, ks);
@@ -805,10 +816,12 @@ int build_levels(vf_solver* s) {
     const int n = 3 * lc.g.nodes_ref();
     if (n <= 16384) {
       VF_ALLOC(s->d_Ainv, (size_t)n * n);
-      VF_ALLOC(s->d_Ainv32, (size_t)n * n);
+      VF_ALLOC(s->d_Ainv32, (size_t)n * dense_ld32(n));
+      VF_ALLOC(s->d_dense_perm, (size_t)n);
       VF_ALLOC(s->d_dense_work, dense_work_count(n));
       s->dense_n = n;
       dense_prepare_smem(n);
+      launch_dense_perm(lc.g, s->d_dense_perm, n, s->st);
       if (!lc.galerkin && !lc.st64) VF_ALLOC(lc.st64, 243 * (size_t)lc.g.n);
     }
   }
@@ -1036,10 +1049,12 @@ int build_dense_coarsest(vf_solver* s) {
   }
   if (s->dense_n != n) {
     VF_ALLOC(s->d_Ainv, (size_t)n * n);
-    VF_ALLOC(s->d_Ainv32, (size_t)n * n);
+    VF_ALLOC(s->d_Ainv32, (size_t)n * dense_ld32(n));
+    VF_ALLOC(s->d_dense_perm, (size_t)n);
     VF_ALLOC(s->d_dense_work, dense_work_count(n));
     s->dense_n = n;
     dense_prepare_smem(n);
+    launch_dense_perm(lc.g, s->d_dense_perm, n, s->st);   // after its zeroing on st; read on st
   }
   double* st = lc.st64;
   if (!lc.galerkin) {
@@ -1051,8 +1066,11 @@ int build_dense_coarsest(vf_solver* s) {
   }
   if (lc.reach > 1) wide_dense_assemble(lc.g, lc.reach, st, lc.mask, s->d_Ainv, n, sd);
   else dense_assemble(lc.g, st, lc.mask, s->d_Ainv, n, sd);
-  dense_cholesky_inverse(s->d_Ainv, s->d_dense_work, n, s->d_info, sd);
-  launch_convert<double, float>(s->d_Ainv, s->d_Ainv32, (long long)n * n, sd);
+  // DOF bandwidth of the reach-R stencil in reference node order
+  const long long nx1 = lc.g.lx + 1, ny1 = lc.g.ly + 1;
+  const long long bw = 3LL * std::max(lc.reach, 1) * (1 + nx1 + nx1 * ny1) + 2;
+  dense_cholesky_inverse(s->d_Ainv, s->d_dense_work, n, (int)std::min<long long>(bw, n), s->d_info, sd);
+  launch_dense_convert_pad(s->d_Ainv, s->d_Ainv32, n, sd);
   VF_CHECK_LAUNCH();
   int info = 0;
   VF_TRY(cudaMemcpyAsync(&info, s->d_info, sizeof(int), cudaMemcpyDeviceToHost, sd));
@@ -1360,13 +1378,15 @@ int vf_set_material(vf_solver* s, const double* E, const double* nu_elem, uint32
     } else if (s->o.coarse_storage == VF_STENCIL_FULL) {
       launch_convert<double, float>(l.st64, l.st32, 243 * n, s->st);
     } else if (l.reach == 2) {
-      launch_wide_compress<double, 2>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+      l.sym64_ok = false;
+      if (s->o.precision == VF_PREC_FP64) compress_sym64(s, l);
       if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
         launch_wide_compress<__half, 2>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
       else
         launch_wide_compress<float, 2>(l.g, l.st64, l.mask, l.sym32, l.sq32, s->st);
     } else {
-      launch_stencil_compress<double>(l.g, l.st64, l.mask, l.sym64, l.sq64, s->st);
+      l.sym64_ok = false;
+      if (s->o.precision == VF_PREC_FP64) compress_sym64(s, l);
       if (s->o.coarse_storage == VF_STENCIL_SYM_HALF)
         launch_stencil_compress<__half>(l.g, l.st64, l.mask, l.sym16, l.sq32, s->st);
       else
@@ -2203,12 +2223,13 @@ void share_operator(vf_solver* c, const vf_solver* m) {
     d.E64 = sl.E64; d.mu64 = sl.mu64; d.minv64 = sl.minv64; d.st64 = sl.st64;
     d.E32 = sl.E32; d.mu32 = sl.mu32; d.minv32 = sl.minv32; d.st32 = sl.st32;
     d.sym64 = sl.sym64; d.sq64 = sl.sq64; d.sym32 = sl.sym32; d.sym16 = sl.sym16; d.sq32 = sl.sq32;
-    d.reach = sl.reach; d.smooth_down = sl.smooth_down;
+    d.reach = sl.reach; d.smooth_down = sl.smooth_down; d.sym64_ok = sl.sym64_ok;
   }
   c->d_spc = m->d_spc;
   c->d_one = m->d_one;
   c->d_Ainv = m->d_Ainv;
   c->d_Ainv32 = m->d_Ainv32;
+  c->d_dense_perm = m->d_dense_perm;
   c->dense_n = m->dense_n;
   c->d_omega = m->d_omega;
   c->d_lambda = m->d_lambda;

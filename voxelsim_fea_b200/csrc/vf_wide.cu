@@ -274,6 +274,275 @@ __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const dou
   }
 }
 
+// ---- set-up products with the reaches fixed at compile time ------------------
+// The hierarchies this library builds use two (R_l, Pr) pairs: (1, 2) for the
+// smoothed transfer from a 27-block level and (2, 1) for the trilinear
+// transfer below a 125-block level, both giving R_{l+1} = 2.  The kernels
+// below compute exactly the sums of k_prolong_blocks / k_rap_b / k_rap_c (the
+// same terms, added in the same order) but with W, NB and the slot counts as
+// constants and the contributing offsets found per axis instead of by testing
+// all NB of them: the generic kernels spend most of their time on runtime
+// divisions and range tests, not on the FP64 products.
+
+// Padded-storage index and interior coordinates of the interior nodes
+// [n0, n0 + NG) of grid f (-1 past the end), for a CTA's staging.
+template <int NG>
+__device__ __forceinline__ void node_table(const Grid& f, long long n0, long long nint, int* sp) {
+  if (threadIdx.x < NG) {
+    int v = -1;
+    if (n0 + threadIdx.x < nint) {
+      int x, y, z;
+      interior_xyz(f, n0 + threadIdx.x, x, y, z);
+      v = f.idx(x, y, z);
+    }
+    sp[threadIdx.x] = v;
+  }
+}
+
+template <int RF, int PR, bool SMOOTHED>
+__global__ void __launch_bounds__(kSetupThreads) k_prolong_blocks_t(Grid f, const double* __restrict__ stf,
+                                                                    const uint8_t* __restrict__ fm,
+                                                                    const double* __restrict__ minvf,
+                                                                    const double* __restrict__ cdev, Grid c,
+                                                                    double* __restrict__ psb) {
+  constexpr int NA = PR + 1, NS = NA * NA * NA, NG = kSetupThreads / NS;
+  constexpr int W = 2 * RF + 1, NB = W * W * W;
+  __shared__ double sA[SMOOTHED ? NG * NB * 9 : 1];
+  __shared__ int sp[NG];
+  const long long nint = (long long)(f.lx + 1) * (f.ly + 1) * (f.lz + 1);
+  const long long nf = f.n;
+  const double cc = SMOOTHED ? *cdev : 0.0;
+  const int sxy = f.px * f.py;
+  for (long long n0 = (long long)blockIdx.x * NG; n0 < nint; n0 += (long long)gridDim.x * NG) {
+    __syncthreads();   // the previous group's readers are done with sA / sp
+    node_table<NG>(f, n0, nint, sp);
+    __syncthreads();
+    if (SMOOTHED) {
+      for (int e = threadIdx.x; e < NG * NB * 9; e += blockDim.x) {
+        const int nl = e / (NB * 9), rem = e - nl * (NB * 9);
+        const int p = sp[nl];
+        sA[e] = p >= 0 ? stf[(long long)rem * nf + p] : 0.0;
+      }
+      __syncthreads();
+    }
+    const int nl = threadIdx.x / NS, slot = threadIdx.x - nl * NS;
+    if (nl >= NG) continue;
+    const int p = sp[nl];
+    if (p < 0) continue;
+    const int z = p / sxy - 1, rxy = p - (z + 1) * sxy, y = rxy / f.px - 1, x = rxy - (y + 1) * f.px - 1;
+    const int ax = slot % NA, ay = (slot / NA) % NA, az = slot / (NA * NA);
+    const int Jx = ceil_half(x - PR) + ax, Jy = ceil_half(y - PR) + ay, Jz = ceil_half(z - PR) + az;
+    double blk[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) blk[k] = 0.0;
+    if (inside(c, Jx, Jy, Jz)) {
+      const uint8_t m = fm[p];
+      const double w = tw(x - 2 * Jx) * tw(y - 2 * Jy) * tw(z - 2 * Jz);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        if ((m >> r) & 1) blk[4 * r] = w;
+      if (SMOOTHED && cc != 0.0 && m) {
+        double wx[W], wy[W], wz[W];
+#pragma unroll
+        for (int d = 0; d < W; ++d) {
+          const int ix = x + d - RF, iy = y + d - RF, iz = z + d - RF;
+          wx[d] = (ix >= 0 && ix <= f.lx) ? tw(ix - 2 * Jx) : 0.0;
+          wy[d] = (iy >= 0 && iy <= f.ly) ? tw(iy - 2 * Jy) : 0.0;
+          wz[d] = (iz >= 0 && iz <= f.lz) ? tw(iz - 2 * Jz) : 0.0;
+        }
+        double acc[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+        const double* A = sA + nl * NB * 9;
+#pragma unroll
+        for (int dz = 0; dz < W; ++dz) {
+          if (wz[dz] == 0.0) continue;
+#pragma unroll
+          for (int dy = 0; dy < W; ++dy) {
+            if (wy[dy] == 0.0) continue;
+#pragma unroll
+            for (int dx = 0; dx < W; ++dx) {
+              if (wx[dx] == 0.0) continue;
+              const double wk = wx[dx] * wy[dy] * wz[dz];
+              const double* As = A + ((dz * W + dy) * W + dx) * 9;
+#pragma unroll
+              for (int k = 0; k < 9; ++k) acc[k] += wk * As[k];
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          const double mr = minvf[3LL * p + r];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) blk[3 * r + k] -= cc * mr * acc[3 * r + k];
+        }
+      }
+    }
+    double* out = psb + ((long long)p * NS + slot) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[k] = blk[k];
+  }
+}
+
+template <int RF, int PR>
+__global__ void __launch_bounds__(kSetupThreads, 4) k_rap_b_t(Grid f, const double* __restrict__ stf,
+                                                           const double* __restrict__ psb, Grid c,
+                                                           double* __restrict__ bsb) {
+  constexpr int NA = PR + 1, NS = NA * NA * NA;
+  constexpr int NBA = PR + RF + 1, NSB = NBA * NBA * NBA, NG = kSetupThreads / NSB;
+  constexpr int W = 2 * RF + 1, NB = W * W * W;
+  __shared__ double sA[NG * NB * 9];
+  __shared__ int sp[NG];
+  const long long nint = (long long)(f.lx + 1) * (f.ly + 1) * (f.lz + 1);
+  const long long nf = f.n;
+  const int sxy = f.px * f.py;
+  for (long long n0 = (long long)blockIdx.x * NG; n0 < nint; n0 += (long long)gridDim.x * NG) {
+    __syncthreads();
+    node_table<NG>(f, n0, nint, sp);
+    __syncthreads();
+    for (int e = threadIdx.x; e < NG * NB * 9; e += blockDim.x) {
+      const int nl = e / (NB * 9), rem = e - nl * (NB * 9);
+      const int p = sp[nl];
+      sA[e] = p >= 0 ? stf[(long long)rem * nf + p] : 0.0;
+    }
+    __syncthreads();
+    const int nl = threadIdx.x / NSB, b = threadIdx.x - nl * NSB;
+    if (nl >= NG) continue;
+    const int p = sp[nl];
+    if (p < 0) continue;
+    const int z = p / sxy - 1, rxy = p - (z + 1) * sxy, y = rxy / f.px - 1, x = rxy - (y + 1) * f.px - 1;
+    const int Jx = ceil_half(x - PR - RF) + b % NBA, Jy = ceil_half(y - PR - RF) + (b / NBA) % NBA;
+    const int Jz = ceil_half(z - PR - RF) + b / (NBA * NBA);
+    double acc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+    if (inside(c, Jx, Jy, Jz)) {
+      // per axis: slot of J in the P_s row of fine node x + d - RF (-1: none)
+      int sx[W], sy[W], sz[W];
+#pragma unroll
+      for (int d = 0; d < W; ++d) {
+        const int ix = x + d - RF, iy = y + d - RF, iz = z + d - RF;
+        const int ax = Jx - ceil_half(ix - PR), ay = Jy - ceil_half(iy - PR), az = Jz - ceil_half(iz - PR);
+        sx[d] = (ix >= 0 && ix <= f.lx && ax >= 0 && ax <= PR) ? ax : -1;
+        sy[d] = (iy >= 0 && iy <= f.ly && ay >= 0 && ay <= PR) ? ay : -1;
+        sz[d] = (iz >= 0 && iz <= f.lz && az >= 0 && az <= PR) ? az : -1;
+      }
+      const double* As = sA + nl * NB * 9;
+#pragma unroll
+      for (int dz = 0; dz < W; ++dz) {
+        if (sz[dz] < 0) continue;
+#pragma unroll
+        for (int dy = 0; dy < W; ++dy) {
+          if (sy[dy] < 0) continue;
+#pragma unroll
+          for (int dx = 0; dx < W; ++dx) {
+            if (sx[dx] < 0) continue;
+            const int q = p + (dx - RF) + f.px * ((dy - RF) + f.py * (dz - RF));
+            const double* P = psb + ((long long)q * NS + (sz[dz] * NA + sy[dy]) * NA + sx[dx]) * 9;
+            const double* A = As + ((dz * W + dy) * W + dx) * 9;
+            double Pv[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Pv[k] = __ldg(P + k);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+              for (int cc = 0; cc < 3; ++cc)
+                acc[3 * r + cc] += A[3 * r] * Pv[cc] + A[3 * r + 1] * Pv[3 + cc] + A[3 * r + 2] * Pv[6 + cc];
+          }
+        }
+      }
+    }
+    double* out = bsb + ((long long)p * NSB + b) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[k] = acc[k];
+  }
+}
+
+template <int RF, int PR, int RC>
+__global__ void __launch_bounds__(kRapThreads, 16) k_rap_c_t(Grid f, const double* __restrict__ psb,
+                                                         const double* __restrict__ bsb, Grid c,
+                                                         double* __restrict__ stc) {
+  constexpr int NA = PR + 1, NS = NA * NA * NA;
+  constexpr int NBA = PR + RF + 1, NSB = NBA * NBA * NBA;
+  constexpr int WI = 2 * PR + 1, NI = WI * WI * WI;
+  constexpr int Wc = 2 * RC + 1, NBc = Wc * Wc * Wc, SC = NBc / 2;
+  __shared__ double sps[NI * 9];
+  const long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
+  const long long nc = c.n;
+  // this thread's offset D (fixed over the nodes): for fine node 2X + a - PR
+  // the slot of X + D in its B row is D - ceil((a - 2 PR - RF) / 2) per axis
+  const int u = threadIdx.x;
+  const bool has = u <= SC;
+  const int s = SC + (has ? u : 0);
+  const int Dx = s % Wc - RC, Dy = (s / Wc) % Wc - RC, Dz = s / (Wc * Wc) - RC;
+  int bx[WI], by[WI], bz[WI];
+#pragma unroll
+  for (int a = 0; a < WI; ++a) {
+    const int h = ceil_half(a - 2 * PR - RF);
+    bx[a] = Dx - h;
+    by[a] = Dy - h;
+    bz[a] = Dz - h;
+    bx[a] = (bx[a] >= 0 && bx[a] < NBA) ? bx[a] : -1;
+    by[a] = (by[a] >= 0 && by[a] < NBA) ? by[a] : -1;
+    bz[a] = (bz[a] >= 0 && bz[a] < NBA) ? bz[a] : -1;
+  }
+  for (long long node = blockIdx.x; node < nint; node += gridDim.x) {
+    int X, Y, Z;
+    interior_xyz(c, node, X, Y, Z);
+    const int pI = c.idx(X, Y, Z);
+    const int x0 = 2 * X - PR, y0 = 2 * Y - PR, z0 = 2 * Z - PR;
+    __syncthreads();   // the previous node's readers are done with sps
+    for (int e = threadIdx.x; e < NI * 9; e += blockDim.x) {
+      const int i = e / 9, k = e - 9 * i;
+      const int a = i % WI, bb = (i / WI) % WI, cz = i / (WI * WI);
+      const int ix = x0 + a, iy = y0 + bb, iz = z0 + cz;
+      double v = 0.0;
+      if (inside(f, ix, iy, iz)) {
+        const int ax = X - ceil_half(ix - PR), ay = Y - ceil_half(iy - PR), az = Z - ceil_half(iz - PR);
+        v = psb[((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9 + k];
+      }
+      sps[e] = v;
+    }
+    __syncthreads();
+    if (!has) continue;
+    const int Jx = X + Dx, Jy = Y + Dy, Jz = Z + Dz;
+    double acc[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+    if (inside(c, Jx, Jy, Jz)) {
+      const int pf0 = f.idx(x0, y0, z0);
+#pragma unroll
+      for (int az = 0; az < WI; ++az) {
+        const int iz = z0 + az;
+        if (bz[az] < 0 || iz < 0 || iz > f.lz) continue;
+#pragma unroll
+        for (int ay = 0; ay < WI; ++ay) {
+          const int iy = y0 + ay;
+          if (by[ay] < 0 || iy < 0 || iy > f.ly) continue;
+#pragma unroll
+          for (int ax = 0; ax < WI; ++ax) {
+            const int ix = x0 + ax;
+            if (bx[ax] < 0 || ix < 0 || ix > f.lx) continue;
+            const double* P = sps + ((az * WI + ay) * WI + ax) * 9;
+            const int q = pf0 + ax + f.px * (ay + f.py * az);
+            const double* B = bsb + ((long long)q * NSB + (bz[az] * NBA + by[ay]) * NBA + bx[ax]) * 9;
+            double Bv[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Bv[k] = __ldg(B + k);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+              for (int cc = 0; cc < 3; ++cc)
+                acc[3 * r + cc] += P[r] * Bv[cc] + P[3 + r] * Bv[3 + cc] + P[6 + r] * Bv[6 + cc];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * nc + pI] = acc[k];
+  }
+}
+
 // Lower offsets from the upper ones: block (s, p)[r][c] = block (NB-1-s, p + off(s))[c][r].
 __global__ void k_wide_mirror(Grid c, int R, double* __restrict__ stc) {
   const int W = wide_w(R), NB = wide_nb(R), SC = NB / 2;
@@ -586,6 +855,21 @@ void launch_wide_galerkin(const Grid& f, const double* stf, int Rf, const uint8_
   const long long nintc = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
   const int NS = (Pr + 1) * (Pr + 1) * (Pr + 1), NBA = Pr + Rf + 1, NSB = NBA * NBA * NBA;
   const int ngp = kSetupThreads / NS, ngb = kSetupThreads / NSB;
+  const int gp = (int)std::min<long long>((nintf + ngp - 1) / ngp, 148LL * 64);
+  const int gb = (int)std::min<long long>((nintf + ngb - 1) / ngb, 148LL * 64);
+  const int gc = (int)std::min<long long>(nintc, 148LL * 256);
+  // the two pairs the hierarchy builds (see k_prolong_blocks_t)
+#define VF_WIDE_FIXED(RF_, PR_, SM_)                                                                          \
+  do {                                                                                                        \
+    launch_k(k_prolong_blocks_t<RF_, PR_, SM_>, gp, kSetupThreads, 0, st, f, stf, fmask, minvf, cdev, c, psb); \
+    launch_k(k_rap_b_t<RF_, PR_>, gb, kSetupThreads, 0, st, f, stf, (const double*)psb, c, bsb);             \
+    launch_k(k_rap_c_t<RF_, PR_, 2>, gc, kRapThreads, 0, st, f, (const double*)psb, (const double*)bsb, c, stc); \
+    launch_k(k_wide_mirror, blocks_for((long long)(wide_nb(Rc) / 2) * nintc, 128), 128, 0, st, c, Rc, stc);    \
+    return;                                                                                                   \
+  } while (0)
+  if (Rf == 1 && Pr == 2 && Rc == 2 && cdev) VF_WIDE_FIXED(1, 2, true);
+  if (Rf == 2 && Pr == 1 && Rc == 2 && !cdev) VF_WIDE_FIXED(2, 1, false);
+#undef VF_WIDE_FIXED
   const size_t smem_p = cdev ? sizeof(double) * ngp * wide_nb(Rf) * 9 : 0;
   const size_t smem_b = sizeof(double) * ngb * wide_nb(Rf) * 9;
   launch_k(k_prolong_blocks, (int)std::min<long long>((nintf + ngp - 1) / ngp, 148LL * 64), kSetupThreads, smem_p, st,
