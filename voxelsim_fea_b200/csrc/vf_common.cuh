@@ -250,6 +250,8 @@ void launch_stencil_mask_and_diag(const Grid& c, double* stencil, uint8_t* cmask
 // vf_transfer.cu -- restriction / prolongation / first sweep
 template <typename T> void launch_restrict(const Grid& f, const T* rf, const Grid& c, const uint8_t* cmask, T* rc, const KrylovState* ks, cudaStream_t st);
 template <typename T> void launch_prolong_add(const Grid& c, const T* ec, const Grid& f, const uint8_t* fmask, T* uf, const KrylovState* ks, cudaStream_t st);
+// restriction + the coarse level's first smoothing step from zero: uc = w (Minv rc), w = *wdev
+template <typename T> void launch_restrict_first(const Grid& f, const T* rf, const Grid& c, const uint8_t* cmask, T* rc, const T* minvc, const double* wdev, T* uc, const KrylovState* ks, cudaStream_t st);
 template <typename T> void launch_jacobi_from_zero(const Grid& g, const T* b, const T* minv3, const uint8_t* mask, double omega, const double* omega_dev, T* u, const KrylovState* ks, cudaStream_t st);
 
 // vf_dense.cu -- coarsest-level dense FP64 direct solve

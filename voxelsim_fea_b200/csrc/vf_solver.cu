@@ -321,7 +321,7 @@ void level_op(vf_solver* s, int li, int epi, const T* u, T* out, const T* b, Kry
 // is x itself), step 1 adds c1 times that update (k_cheb_coefs).
 template <typename T>
 void smooth_cheb(vf_solver* s, int li, T* x, T* tmp, T* dbuf, const T* b, int sweeps, bool from_zero,
-                 KrylovState* ks, int dot_slot) {
+                 KrylovState* ks, int dot_slot, bool first_ready = false) {
   Level& l = s->L[li];
   const double* c = s->d_cheb + 4 * li;
   T* cur = x;
@@ -330,8 +330,8 @@ void smooth_cheb(vf_solver* s, int li, T* x, T* tmp, T* dbuf, const T* b, int sw
   s1.omega_dev = c + 3;
   s1.c1_dev = c + 2;
   if (from_zero) {
-    T* first = (sweeps % 2 == 1) ? x : tmp;
-    launch_jacobi_from_zero<T>(l.g, b, Sel<T>::minv(l), l.mask, 0.0, c + 1, first, ks, s->st);
+    T* first = (sweeps % 2 == 1) ? x : tmp;   // (cheb_first_target)
+    if (!first_ready) launch_jacobi_from_zero<T>(l.g, b, Sel<T>::minv(l), l.mask, 0.0, c + 1, first, ks, s->st);
     cur = first;
     s1.dprev = first;
   } else {
@@ -391,19 +391,29 @@ void smooth(vf_solver* s, int li, T* x, T* tmp, const T* b, int sweeps, bool fro
 // trilinear prolongation into a temporary followed by one sweep of the level
 // operator with a zero rhs, weight c and the step field (dprev = x, c1 = 1).
 // Temporaries: w[1] and w[4] of level li (free outside the smoothing).
+// first != nullptr: the restriction also makes the coarse level's first
+// smoothing step from zero, first = (*wfirst) Minv_c rc
 template <typename T>
-void restrict_level(vf_solver* s, int li, const T* r, T* rc, KrylovState* ks) {
+void restrict_to(vf_solver* s, const Level& l, const T* r, Level& c, T* rc, KrylovState* ks, T* first,
+                 const double* wfirst) {
+  if (first) launch_restrict_first<T>(l.g, r, c.g, c.mask, rc, Sel<T>::minv(c), wfirst, first, ks, s->st);
+  else launch_restrict<T>(l.g, r, c.g, c.mask, rc, ks, s->st);
+}
+
+template <typename T>
+void restrict_level(vf_solver* s, int li, const T* r, T* rc, KrylovState* ks, T* first = nullptr,
+                    const double* wfirst = nullptr) {
   Level& l = s->L[li];
   Level& c = s->L[li + 1];
   if (!l.smooth_down) {
-    launch_restrict<T>(l.g, r, c.g, c.mask, rc, ks, s->st);
+    restrict_to<T>(s, l, r, c, rc, ks, first, wfirst);
     return;
   }
   T* z = Sel<T>::w(l, 1);
   T* rs = Sel<T>::w(l, 4);
   launch_jacobi_from_zero<T>(l.g, r, Sel<T>::minv(l), l.mask, 0.0, s->d_spc + li, z, ks, s->st);
   level_op<T>(s, li, EPI_RESID, z, rs, r, ks, nullptr, 0);
-  launch_restrict<T>(l.g, rs, c.g, c.mask, rc, ks, s->st);
+  restrict_to<T>(s, l, rs, c, rc, ks, first, wfirst);
 }
 
 template <typename T>
@@ -439,10 +449,23 @@ void coarse_solve(vf_solver* s, int li, const T* b, T* x, KrylovState* ks) {
   }
 }
 
+// pre/post smoothing steps on level li, and whether they are Chebyshev steps
+int level_sweeps(const vf_solver* s, int li) {
+  const Level& l = s->L[li];
+  // a level whose transfer down is smoothed gets one more smoothing step from
+  // each of its smoothed restriction and prolongation
+  return (l.smooth_down && s->o.smoothed_level_sweeps > 0) ? s->o.smoothed_level_sweeps : s->o.n_smooth;
+}
+bool level_cheb(const vf_solver* s, int li) {
+  return s->o.smoother == VF_SMOOTH_CHEBYSHEV && level_sweeps(s, li) > 0 && li < (int)s->L.size() - 1;
+}
+
 // x = V-cycle(b) on level li (core/multigrid.py:426-436); dot_slot >= 0: the
 // last sweep on this level also reduces b.x (r.z of the PCG) into that slot.
+// first_ready: the restriction into this level already made the first
+// Chebyshev step from zero (level_cheb(li))
 template <typename T>
-void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks, int dot_slot = -1) {
+void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks, int dot_slot = -1, bool first_ready = false) {
   Level& l = s->L[li];
   if (li == (int)s->L.size() - 1) {
     coarse_solve<T>(s, li, b, x, ks);
@@ -451,15 +474,17 @@ void vcycle(vf_solver* s, int li, const T* b, T* x, KrylovState* ks, int dot_slo
   Level& c = s->L[li + 1];
   T* tmp = Sel<T>::w(l, 1);
   T* res = Sel<T>::w(l, 2);
-  // a level whose transfer down is smoothed gets one more smoothing step from
-  // each of its smoothed restriction and prolongation
-  const int sweeps = (l.smooth_down && s->o.smoothed_level_sweeps > 0) ? s->o.smoothed_level_sweeps : s->o.n_smooth;
-  const bool cheb = s->o.smoother == VF_SMOOTH_CHEBYSHEV && sweeps > 0;
-  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, sweeps, true, ks, -1);
+  const int sweeps = level_sweeps(s, li);
+  const bool cheb = level_cheb(s, li);
+  if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, sweeps, true, ks, -1, first_ready);
   else smooth<T>(s, li, x, tmp, b, sweeps, true, ks);
   level_op<T>(s, li, EPI_RESID, x, res, b, ks, nullptr, 0);
-  restrict_level<T>(s, li, res, Sel<T>::w(c, 3), ks);
-  vcycle<T>(s, li + 1, Sel<T>::w(c, 3), Sel<T>::w(c, 0), ks);
+  // the next level's first Chebyshev step from zero rides on the restriction
+  // (its target: the next level's x for an odd step count, else its tmp)
+  const bool fuse = level_cheb(s, li + 1);
+  T* first = fuse ? ((level_sweeps(s, li + 1) % 2 == 1) ? Sel<T>::w(c, 0) : Sel<T>::w(c, 1)) : nullptr;
+  restrict_level<T>(s, li, res, Sel<T>::w(c, 3), ks, first, fuse ? s->d_cheb + 4 * (li + 1) + 1 : nullptr);
+  vcycle<T>(s, li + 1, Sel<T>::w(c, 3), Sel<T>::w(c, 0), ks, -1, fuse);
   prolong_level<T>(s, li, Sel<T>::w(c, 0), x, ks);
   // (res is free again: the post-smoothing's first update goes there)
   if (cheb) smooth_cheb<T>(s, li, x, tmp, res, b, sweeps, false, ks, dot_slot);

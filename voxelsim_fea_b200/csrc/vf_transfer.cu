@@ -75,6 +75,61 @@ __global__ void __launch_bounds__(256) k_restrict_f(Grid f, const float* __restr
   }
 }
 
+// Restriction fused with the coarse level's first smoothing step from zero:
+// the restricted residual rc (kept: the coarse level's right-hand side) and
+// uc = w * (Minv rc), the same sums and products as k_restrict_* followed by
+// k_jacobi_from_zero (ghost entries of uc stay untouched: they hold zeros).
+template <typename T>
+__global__ void __launch_bounds__(256) k_restrict_first(Grid f, const T* __restrict__ rf, Grid c,
+                                                        const uint8_t* __restrict__ cm, T* __restrict__ rc,
+                                                        const T* __restrict__ minvc, const double* __restrict__ wdev,
+                                                        T* __restrict__ uc, const KrylovState* ks) {
+  if (ks && ks->done) return;
+  const T w = (T)(*wdev);
+  const int nx1 = c.lx + 1, ny1 = c.ly + 1, nint = nx1 * ny1 * (c.lz + 1);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += gridDim.x * blockDim.x) {
+    const int X = t % nx1, rr = t / nx1, Y = rr % ny1, Z = rr / ny1;
+    T a0 = 0, a1 = 0, a2 = 0;
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          const long long q = 3 * (long long)f.idx(2 * X - 1, 2 * Y + dy, 2 * Z + dz);
+          const float2* q2 = reinterpret_cast<const float2*>(rf + q);
+          const float2 v01 = __ldg(q2), v23 = __ldg(q2 + 1), v45 = __ldg(q2 + 2), v67 = __ldg(q2 + 3);
+          const float v8 = __ldg(rf + q + 8);
+          const float r[9] = {v01.x, v01.y, v23.x, v23.y, v45.x, v45.y, v67.x, v67.y, v8};
+#pragma unroll
+          for (int dx = -1; dx <= 1; ++dx) {
+            const float wt = (dx ? 0.5f : 1.0f) * (dy ? 0.5f : 1.0f) * (dz ? 0.5f : 1.0f);
+            const int o = 3 * (dx + 1);
+            a0 += wt * r[o]; a1 += wt * r[o + 1]; a2 += wt * r[o + 2];
+          }
+        }
+    } else {
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+          for (int dx = -1; dx <= 1; ++dx) {
+            const double wt = (dx ? 0.5 : 1.0) * (dy ? 0.5 : 1.0) * (dz ? 0.5 : 1.0);
+            const long long q = 3 * (long long)f.idx(2 * X + dx, 2 * Y + dy, 2 * Z + dz);
+            a0 += wt * rf[q]; a1 += wt * rf[q + 1]; a2 += wt * rf[q + 2];
+          }
+    }
+    const int p = c.idx(X, Y, Z);
+    const uint8_t m = cm[p];
+    const long long p3 = 3 * (long long)p;
+    const T b0 = (m & 1) ? a0 : (T)0, b1 = (m & 2) ? a1 : (T)0, b2 = (m & 4) ? a2 : (T)0;
+    rc[p3] = b0; rc[p3 + 1] = b1; rc[p3 + 2] = b2;
+    uc[p3] = (m & 1) ? w * (minvc[p3] * b0) : (T)0;
+    uc[p3 + 1] = (m & 2) ? w * (minvc[p3 + 1] * b1) : (T)0;
+    uc[p3 + 2] = (m & 4) ? w * (minvc[p3 + 2] * b2) : (T)0;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_prolong_add(Grid c, const T* __restrict__ ec, Grid f,
                                                      const uint8_t* __restrict__ fm, T* __restrict__ uf,
@@ -246,6 +301,17 @@ void launch_restrict<float>(const Grid& f, const float* rf, const Grid& c, const
                             const KrylovState* ks, cudaStream_t st) {
   launch_k(k_restrict_f, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c, cmask, rc, ks);
 }
+
+template <typename T>
+void launch_restrict_first(const Grid& f, const T* rf, const Grid& c, const uint8_t* cmask, T* rc, const T* minvc,
+                           const double* wdev, T* uc, const KrylovState* ks, cudaStream_t st) {
+  launch_k(k_restrict_first<T>, blocks_for((long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1)), 256, 0, st, f, rf, c,
+           cmask, rc, minvc, wdev, uc, ks);
+}
+template void launch_restrict_first<float>(const Grid&, const float*, const Grid&, const uint8_t*, float*,
+                                           const float*, const double*, float*, const KrylovState*, cudaStream_t);
+template void launch_restrict_first<double>(const Grid&, const double*, const Grid&, const uint8_t*, double*,
+                                            const double*, const double*, double*, const KrylovState*, cudaStream_t);
 
 template <typename T>
 void launch_prolong_add(const Grid& c, const T* ec, const Grid& f, const uint8_t* fmask, T* uf,

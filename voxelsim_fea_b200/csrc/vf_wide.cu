@@ -278,11 +278,14 @@ __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const dou
 // The hierarchies this library builds use two (R_l, Pr) pairs: (1, 2) for the
 // smoothed transfer from a 27-block level and (2, 1) for the trilinear
 // transfer below a 125-block level, both giving R_{l+1} = 2.  The kernels
-// below compute exactly the sums of k_prolong_blocks / k_rap_b / k_rap_c (the
-// same terms, added in the same order) but with W, NB and the slot counts as
+// below compute exactly the sums of k_prolong_blocks / k_rap_b (the same
+// terms, added in the same order) but with W, NB and the slot counts as
 // constants and the contributing offsets found per axis instead of by testing
 // all NB of them: the generic kernels spend most of their time on runtime
-// divisions and range tests, not on the FP64 products.
+// divisions and range tests, not on the FP64 products.  (The coarse product
+// stays generic: a compile-time version held twice the registers and ran
+// slower; so did a B product that staged the neighbours' P_s rows in shared
+// memory.)
 
 // Padded-storage index and interior coordinates of the interior nodes
 // [n0, n0 + NG) of grid f (-1 past the end), for a CTA's staging.
@@ -455,91 +458,6 @@ __global__ void __launch_bounds__(kSetupThreads, 4) k_rap_b_t(Grid f, const doub
     double* out = bsb + ((long long)p * NSB + b) * 9;
 #pragma unroll
     for (int k = 0; k < 9; ++k) out[k] = acc[k];
-  }
-}
-
-template <int RF, int PR, int RC>
-__global__ void __launch_bounds__(kRapThreads, 16) k_rap_c_t(Grid f, const double* __restrict__ psb,
-                                                         const double* __restrict__ bsb, Grid c,
-                                                         double* __restrict__ stc) {
-  constexpr int NA = PR + 1, NS = NA * NA * NA;
-  constexpr int NBA = PR + RF + 1, NSB = NBA * NBA * NBA;
-  constexpr int WI = 2 * PR + 1, NI = WI * WI * WI;
-  constexpr int Wc = 2 * RC + 1, NBc = Wc * Wc * Wc, SC = NBc / 2;
-  __shared__ double sps[NI * 9];
-  const long long nint = (long long)(c.lx + 1) * (c.ly + 1) * (c.lz + 1);
-  const long long nc = c.n;
-  // this thread's offset D (fixed over the nodes): for fine node 2X + a - PR
-  // the slot of X + D in its B row is D - ceil((a - 2 PR - RF) / 2) per axis
-  const int u = threadIdx.x;
-  const bool has = u <= SC;
-  const int s = SC + (has ? u : 0);
-  const int Dx = s % Wc - RC, Dy = (s / Wc) % Wc - RC, Dz = s / (Wc * Wc) - RC;
-  int bx[WI], by[WI], bz[WI];
-#pragma unroll
-  for (int a = 0; a < WI; ++a) {
-    const int h = ceil_half(a - 2 * PR - RF);
-    bx[a] = Dx - h;
-    by[a] = Dy - h;
-    bz[a] = Dz - h;
-    bx[a] = (bx[a] >= 0 && bx[a] < NBA) ? bx[a] : -1;
-    by[a] = (by[a] >= 0 && by[a] < NBA) ? by[a] : -1;
-    bz[a] = (bz[a] >= 0 && bz[a] < NBA) ? bz[a] : -1;
-  }
-  for (long long node = blockIdx.x; node < nint; node += gridDim.x) {
-    int X, Y, Z;
-    interior_xyz(c, node, X, Y, Z);
-    const int pI = c.idx(X, Y, Z);
-    const int x0 = 2 * X - PR, y0 = 2 * Y - PR, z0 = 2 * Z - PR;
-    __syncthreads();   // the previous node's readers are done with sps
-    for (int e = threadIdx.x; e < NI * 9; e += blockDim.x) {
-      const int i = e / 9, k = e - 9 * i;
-      const int a = i % WI, bb = (i / WI) % WI, cz = i / (WI * WI);
-      const int ix = x0 + a, iy = y0 + bb, iz = z0 + cz;
-      double v = 0.0;
-      if (inside(f, ix, iy, iz)) {
-        const int ax = X - ceil_half(ix - PR), ay = Y - ceil_half(iy - PR), az = Z - ceil_half(iz - PR);
-        v = psb[((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9 + k];
-      }
-      sps[e] = v;
-    }
-    __syncthreads();
-    if (!has) continue;
-    const int Jx = X + Dx, Jy = Y + Dy, Jz = Z + Dz;
-    double acc[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) acc[k] = 0.0;
-    if (inside(c, Jx, Jy, Jz)) {
-      const int pf0 = f.idx(x0, y0, z0);
-#pragma unroll
-      for (int az = 0; az < WI; ++az) {
-        const int iz = z0 + az;
-        if (bz[az] < 0 || iz < 0 || iz > f.lz) continue;
-#pragma unroll
-        for (int ay = 0; ay < WI; ++ay) {
-          const int iy = y0 + ay;
-          if (by[ay] < 0 || iy < 0 || iy > f.ly) continue;
-#pragma unroll
-          for (int ax = 0; ax < WI; ++ax) {
-            const int ix = x0 + ax;
-            if (bx[ax] < 0 || ix < 0 || ix > f.lx) continue;
-            const double* P = sps + ((az * WI + ay) * WI + ax) * 9;
-            const int q = pf0 + ax + f.px * (ay + f.py * az);
-            const double* B = bsb + ((long long)q * NSB + (bz[az] * NBA + by[ay]) * NBA + bx[ax]) * 9;
-            double Bv[9];
-#pragma unroll
-            for (int k = 0; k < 9; ++k) Bv[k] = __ldg(B + k);
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-              for (int cc = 0; cc < 3; ++cc)
-                acc[3 * r + cc] += P[r] * Bv[cc] + P[3 + r] * Bv[3 + cc] + P[6 + r] * Bv[6 + cc];
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) stc[((long long)s * 9 + k) * nc + pI] = acc[k];
   }
 }
 
@@ -858,12 +776,13 @@ void launch_wide_galerkin(const Grid& f, const double* stf, int Rf, const uint8_
   const int gp = (int)std::min<long long>((nintf + ngp - 1) / ngp, 148LL * 64);
   const int gb = (int)std::min<long long>((nintf + ngb - 1) / ngb, 148LL * 64);
   const int gc = (int)std::min<long long>(nintc, 148LL * 256);
+  const size_t smem_c = sizeof(double) * (2 * Pr + 1) * (2 * Pr + 1) * (2 * Pr + 1) * 9;   // k_rap_c
   // the two pairs the hierarchy builds (see k_prolong_blocks_t)
 #define VF_WIDE_FIXED(RF_, PR_, SM_)                                                                          \
   do {                                                                                                        \
     launch_k(k_prolong_blocks_t<RF_, PR_, SM_>, gp, kSetupThreads, 0, st, f, stf, fmask, minvf, cdev, c, psb); \
     launch_k(k_rap_b_t<RF_, PR_>, gb, kSetupThreads, 0, st, f, stf, (const double*)psb, c, bsb);             \
-    launch_k(k_rap_c_t<RF_, PR_, 2>, gc, kRapThreads, 0, st, f, (const double*)psb, (const double*)bsb, c, stc); \
+    launch_k(k_rap_c, gc, kRapThreads, smem_c, st, f, Rf, (const double*)psb, Pr, (const double*)bsb, c, Rc, stc); \
     launch_k(k_wide_mirror, blocks_for((long long)(wide_nb(Rc) / 2) * nintc, 128), 128, 0, st, c, Rc, stc);    \
     return;                                                                                                   \
   } while (0)
