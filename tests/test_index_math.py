@@ -126,3 +126,58 @@ def test_coarsest_triangular_inversion_schedule():
     for n in (5, 33, 4131, 9999, 16384):
         for g, pairs, toff in _trtri_schedule(n):
             assert toff <= n * n // 2 + 32 * n, (n, g, toff)
+
+
+def _stencil_matrix(nx1, ny1, nz1, R, rng):
+    """SPD matrix with the coupling pattern of a reach-R 3x3-block stencil in
+    the reference node order r = x + nx1 (y + ny1 z), DOF 3 r + c (the dense
+    coarsest operator of vf_dense.cu / vf_wide.cu)."""
+    import numpy as np
+    n = 3 * nx1 * ny1 * nz1
+    A = np.zeros((n, n))
+    coords = [(x, y, z) for z in range(nz1) for y in range(ny1) for x in range(nx1)]
+    for r, (x, y, z) in enumerate(coords):
+        for dz in range(-R, R + 1):
+            for dy in range(-R, R + 1):
+                for dx in range(-R, R + 1):
+                    X, Y, Z = x + dx, y + dy, z + dz
+                    if 0 <= X < nx1 and 0 <= Y < ny1 and 0 <= Z < nz1:
+                        q = X + nx1 * (Y + ny1 * Z)
+                        if q >= r:
+                            B = rng.standard_normal((3, 3))
+                            A[3 * r:3 * r + 3, 3 * q:3 * q + 3] = B
+                            A[3 * q:3 * q + 3, 3 * r:3 * r + 3] = B.T
+    # diagonal dominance makes it SPD without changing the pattern
+    A += np.diag(np.abs(A).sum(axis=1) + 1.0)
+    return A
+
+
+def test_coarsest_band_limits():
+    """The band the coarsest factorization relies on (vf_solver.cu,
+    build_dense_coarsest; vf_dense.cu, dense_cholesky_inverse): with
+    bw = 3 R (1 + nx1 + nx1 ny1) + 2, a reach-R stencil operator has no entry
+    beyond bw; its Cholesky factor has none either (so the panel solve and the
+    trailing update of a block column touch only the rows within the band);
+    and each L21 block of the triangular inversion's levels, and its product
+    T = L21 Y11, is zero below row bw (the rows the batched products skip)."""
+    import numpy as np
+    rng = np.random.default_rng(1)
+    for (nx1, ny1, nz1, R) in [(5, 4, 6, 1), (4, 3, 7, 2), (6, 2, 5, 2)]:
+        A = _stencil_matrix(nx1, ny1, nz1, R, rng)
+        n = A.shape[0]
+        bw = min(3 * R * (1 + nx1 + nx1 * ny1) + 2, n)
+        i, j = np.indices(A.shape)
+        assert not A[np.abs(i - j) > bw].any()
+        Lf = np.linalg.cholesky(A)
+        assert not Lf[(i - j) > bw].any()
+        Y = np.linalg.inv(Lf)
+        for g, pairs, _ in _trtri_schedule(n, nb=8):
+            for r0, r1, r2, _ in pairs:
+                L21 = Lf[r1:r2, r0:r1]
+                assert not L21[bw:].any(), (nx1, ny1, nz1, R, g)
+                # the skipped K range of each row tile: L21[a][b] == 0 for b < a + h - bw
+                h = r1 - r0
+                a, b = np.indices(L21.shape)
+                assert not L21[b < a + h - bw].any()
+                T = L21 @ Y[r0:r1, r0:r1]
+                assert not T[bw:].any()
