@@ -17,8 +17,9 @@
 // residual and sweep kernels.
 //
 // Set-up (FP64, once per set_material), for the transfer l -> l+1:
-//   k_prolong_blocks  the 3x3 blocks P_s[i][J] of every fine node i (AoS,
-//                     (Pr+1)^3 coarse slots per node; Pr = 1 + R_l when
+//   k_prolong_blocks  the 3x3 blocks P_s[i][J] of every fine node i
+//                     ((Pr+1)^3 coarse slots per node, stored entry-major
+//                     and slot-fastest per node; Pr = 1 + R_l when
 //                     smoothed, 1 for the trilinear P);
 //   k_rap_b           B = A_l P_s, (Pr+R_l+1)^3 coarse slots per fine node;
 //   k_rap_c           the diagonal and upper blocks of A_{l+1} = P_s^T B, one
@@ -105,7 +106,8 @@ __device__ __forceinline__ void stage_blocks(const Grid& f, const double* __rest
 }
 
 // P_s[i][J] per fine interior node i and coarse slot (ax, ay, az), J = jlo(i) + a,
-// jlo = ceil((i - Pr) / 2) per axis; psb[(p * NS + slot) * 9 + 3r + c].
+// jlo = ceil((i - Pr) / 2) per axis; psb[(p * 9 + 3r + c) * NS + slot] (slot fastest:
+// the consecutive slots a warp reads or writes are consecutive words).
 // smoothed: *cdev != 0 (the blocks of A staged); else the trilinear D P.
 __global__ void __launch_bounds__(kSetupThreads) k_prolong_blocks(Grid f, const double* __restrict__ stf, int Rf,
                                                                   const uint8_t* __restrict__ fm,
@@ -160,14 +162,14 @@ __global__ void __launch_bounds__(kSetupThreads) k_prolong_blocks(Grid f, const 
         }
       }
     }
-    double* out = psb + ((long long)p * NS + slot) * 9;
+    double* out = psb + (long long)p * NS * 9 + slot;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) out[k] = blk[k];
+    for (int k = 0; k < 9; ++k) out[k * NS] = blk[k];
   }
 }
 
 // B[k][J] = sum_d A[k][d] P_s[k + d][J] per fine interior node k and coarse
-// slot b, J = ceil((k - Pr - Rf) / 2) + b per axis; bsb[(p * NSB + b) * 9 + 3r + c].
+// slot b, J = ceil((k - Pr - Rf) / 2) + b per axis; bsb[(p * 9 + 3r + c) * NSB + b].
 __global__ void __launch_bounds__(kSetupThreads) k_rap_b(Grid f, const double* __restrict__ stf, int Rf,
                                                          const double* __restrict__ psb, int Pr, Grid c,
                                                          double* __restrict__ bsb) {
@@ -197,18 +199,21 @@ __global__ void __launch_bounds__(kSetupThreads) k_rap_b(Grid f, const double* _
         if (!inside(f, ix, iy, iz)) continue;
         const int ax = Jx - ceil_half(ix - Pr), ay = Jy - ceil_half(iy - Pr), az = Jz - ceil_half(iz - Pr);
         if (ax < 0 || ax > Pr || ay < 0 || ay > Pr || az < 0 || az > Pr) continue;
-        const double* P = psb + ((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9;
+        const double* P = psb + (long long)f.idx(ix, iy, iz) * NS * 9 + (az * NA + ay) * NA + ax;
         const double* A = As + s * 9;
+        double Pv[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Pv[k] = P[k * NS];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
           for (int cc = 0; cc < 3; ++cc)
-            acc[3 * r + cc] += A[3 * r] * P[cc] + A[3 * r + 1] * P[3 + cc] + A[3 * r + 2] * P[6 + cc];
+            acc[3 * r + cc] += A[3 * r] * Pv[cc] + A[3 * r + 1] * Pv[3 + cc] + A[3 * r + 2] * Pv[6 + cc];
       }
     }
-    double* out = bsb + ((long long)p * NSB + b) * 9;
+    double* out = bsb + (long long)p * NSB * 9 + b;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) out[k] = acc[k];
+    for (int k = 0; k < 9; ++k) out[k * NSB] = acc[k];
   }
 }
 
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const dou
       double v = 0.0;
       if (inside(f, ix, iy, iz)) {
         const int ax = X - ceil_half(ix - Pr), ay = Y - ceil_half(iy - Pr), az = Z - ceil_half(iz - Pr);
-        v = psb[((long long)f.idx(ix, iy, iz) * NS + (az * NA + ay) * NA + ax) * 9 + k];
+        v = psb[((long long)f.idx(ix, iy, iz) * 9 + k) * NS + (az * NA + ay) * NA + ax];
       }
       sps[e] = v;
     }
@@ -257,10 +262,10 @@ __global__ void __launch_bounds__(kRapThreads) k_rap_c(Grid f, int Rf, const dou
           const int bz = Jz - ceil_half(iz - Pr - Rf);
           if (bx < 0 || bx >= NBA || by < 0 || by >= NBA || bz < 0 || bz >= NBA) continue;
           const double* P = sps + i * 9;
-          const double* B = bsb + ((long long)f.idx(ix, iy, iz) * NSB + (bz * NBA + by) * NBA + bx) * 9;
+          const double* B = bsb + (long long)f.idx(ix, iy, iz) * NSB * 9 + (bz * NBA + by) * NBA + bx;
           double Bv[9];
 #pragma unroll
-          for (int k = 0; k < 9; ++k) Bv[k] = B[k];
+          for (int k = 0; k < 9; ++k) Bv[k] = B[k * NSB];
 #pragma unroll
           for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -381,9 +386,9 @@ __global__ void __launch_bounds__(kSetupThreads) k_prolong_blocks_t(Grid f, cons
         }
       }
     }
-    double* out = psb + ((long long)p * NS + slot) * 9;
+    double* out = psb + (long long)p * NS * 9 + slot;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) out[k] = blk[k];
+    for (int k = 0; k < 9; ++k) out[k * NS] = blk[k];
   }
 }
 
@@ -441,11 +446,11 @@ __global__ void __launch_bounds__(kSetupThreads, 4) k_rap_b_t(Grid f, const doub
           for (int dx = 0; dx < W; ++dx) {
             if (sx[dx] < 0) continue;
             const int q = p + (dx - RF) + f.px * ((dy - RF) + f.py * (dz - RF));
-            const double* P = psb + ((long long)q * NS + (sz[dz] * NA + sy[dy]) * NA + sx[dx]) * 9;
+            const double* P = psb + (long long)q * NS * 9 + (sz[dz] * NA + sy[dy]) * NA + sx[dx];
             const double* A = As + ((dz * W + dy) * W + dx) * 9;
             double Pv[9];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) Pv[k] = __ldg(P + k);
+            for (int k = 0; k < 9; ++k) Pv[k] = __ldg(P + k * NS);
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -455,9 +460,9 @@ __global__ void __launch_bounds__(kSetupThreads, 4) k_rap_b_t(Grid f, const doub
         }
       }
     }
-    double* out = bsb + ((long long)p * NSB + b) * 9;
+    double* out = bsb + (long long)p * NSB * 9 + b;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) out[k] = acc[k];
+    for (int k = 0; k < 9; ++k) out[k * NSB] = acc[k];
   }
 }
 
