@@ -181,3 +181,83 @@ def test_coarsest_band_limits():
                 assert not L21[b < a + h - bw].any()
                 T = L21 @ Y[r0:r1, r0:r1]
                 assert not T[bw:].any()
+
+
+def _ceil_half(v):
+    return (v + 1) // 2 if v >= 0 else -((-v) // 2)
+
+
+def _tw(d):
+    return 1.0 if d == 0 else (0.5 if d in (1, -1) else 0.0)
+
+
+def test_fixed_reach_setup_tables():
+    """The compile-time set-up products (vf_wide.cu, k_prolong_blocks_t and
+    k_rap_b_t) find the contributing neighbour offsets from per-axis tables;
+    restated on the host, they give the same (offset, slot, weight) terms in
+    the same order as the generic kernels' scan over all (2R+1)^3 offsets,
+    for both reach pairs the hierarchy builds ((R_l, Pr) = (1, 2), (2, 1)),
+    at every node of small fine grids (edges and interior)."""
+    import itertools
+    for RF, PR in [(1, 2), (2, 1)]:
+        W, NA, NBA = 2 * RF + 1, PR + 1, PR + RF + 1
+        for (lx, ly, lz) in [(6, 4, 4), (5, 3, 7)]:
+            cx, cy, cz = lx // 2, ly // 2, lz // 2   # coarse voxels (the grid test uses even and odd)
+
+            def inside_f(x, y, z):
+                return 0 <= x <= lx and 0 <= y <= ly and 0 <= z <= lz
+
+            def inside_c(x, y, z):
+                return 0 <= x <= cx and 0 <= y <= cy and 0 <= z <= cz
+
+            for x, y, z in itertools.product(range(lx + 1), range(ly + 1), range(lz + 1)):
+                # B = A P_s: generic scan (k_rap_b) against the per-axis tables (k_rap_b_t)
+                for b in range(NBA ** 3):
+                    J = (_ceil_half(x - PR - RF) + b % NBA, _ceil_half(y - PR - RF) + (b // NBA) % NBA,
+                         _ceil_half(z - PR - RF) + b // (NBA * NBA))
+                    if not inside_c(*J):
+                        continue
+                    generic = []
+                    for s in range(W ** 3):
+                        ix, iy, iz = x + s % W - RF, y + (s // W) % W - RF, z + s // (W * W) - RF
+                        if not inside_f(ix, iy, iz):
+                            continue
+                        a = (J[0] - _ceil_half(ix - PR), J[1] - _ceil_half(iy - PR), J[2] - _ceil_half(iz - PR))
+                        if min(a) < 0 or max(a) > PR:
+                            continue
+                        generic.append((s, (a[2] * NA + a[1]) * NA + a[0]))
+                    tab = []
+                    for axis, (v, hi) in enumerate([(x, lx), (y, ly), (z, lz)]):
+                        col = []
+                        for d in range(W):
+                            iv = v + d - RF
+                            av = J[axis] - _ceil_half(iv - PR)
+                            col.append(av if (0 <= iv <= hi and 0 <= av <= PR) else -1)
+                        tab.append(col)
+                    fixed = [(((dz * W) + dy) * W + dx, (tab[2][dz] * NA + tab[1][dy]) * NA + tab[0][dx])
+                             for dz in range(W) if tab[2][dz] >= 0
+                             for dy in range(W) if tab[1][dy] >= 0
+                             for dx in range(W) if tab[0][dx] >= 0]
+                    assert fixed == generic, (RF, PR, x, y, z, b)
+                # P_s blocks: generic weights (k_prolong_blocks) against per-axis weights
+                for slot in range(NA ** 3):
+                    J = (_ceil_half(x - PR) + slot % NA, _ceil_half(y - PR) + (slot // NA) % NA,
+                         _ceil_half(z - PR) + slot // (NA * NA))
+                    if not inside_c(*J):
+                        continue
+                    generic = []
+                    for s in range(W ** 3):
+                        dx, dy, dz = s % W - RF, (s // W) % W - RF, s // (W * W) - RF
+                        wk = _tw(x + dx - 2 * J[0]) * _tw(y + dy - 2 * J[1]) * _tw(z + dz - 2 * J[2])
+                        if wk == 0.0 or not inside_f(x + dx, y + dy, z + dz):
+                            continue
+                        generic.append((s, wk))
+                    wts = []
+                    for axis, (v, hi) in enumerate([(x, lx), (y, ly), (z, lz)]):
+                        wts.append([(_tw(v + d - RF - 2 * J[axis]) if 0 <= v + d - RF <= hi else 0.0)
+                                    for d in range(W)])
+                    fixed = [(((dz * W) + dy) * W + dx, wts[0][dx] * wts[1][dy] * wts[2][dz])
+                             for dz in range(W) if wts[2][dz] != 0.0
+                             for dy in range(W) if wts[1][dy] != 0.0
+                             for dx in range(W) if wts[0][dx] != 0.0]
+                    assert fixed == generic, (RF, PR, x, y, z, slot)
